@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Decode throughput benchmark (one JSON line on rank 0).
+
+Default workload -- byte-RLE + RLE v2 plain decode: a 256 MiB uint8 column of
+runs (geometric mean-20 run length, 16 byte values with Zipf(1.2)
+frequencies) in the brle container with 256 KiB chunks, and a 256 MiB int64
+column of 512-value segments (DELTA / SHORT_REPEAT / DIRECT / PATCHED_BASE
+data) in the RLE v2 transposed container with 256 KiB chunks, READ_UNIT 32.
+A step decodes both columns from HBM to HBM.  Synthetic seeded data stands in
+for the reference's datasets, which are not available.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload brle_rlev2|rlev1|lzss|deflate]
+
+Multi-GPU (torchrun, one process per GPU): every rank decodes its own copy of
+the workload (independent chunks, no exchange step), weak scaling, time = max
+over ranks.  --impl reference times the reference's CPU decoders on the host
+cores (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+MiB = 1 << 20
+GiB = 1 << 30
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+# workloads
+# --------------------------------------------------------------------------
+
+def make_workload(name: str, scale: float = 1.0):
+    """Returns (label, [(codec_name, Encoded, raw_bytes_view)], config dict)."""
+    import compression_b200.codecs as cc
+    if name == "brle_rlev2":
+        n = int(256 * MiB * scale)
+        a = cc.gen_brle_bytes(0xB0, n)
+        e1 = cc.brle_encode(a, 256 * 1024)
+        v = cc.gen_rlev2_ints(0xB1, n // 8)
+        e2 = cc.rlev2_encode(v, 256 * 1024, 32)
+        cfg = {"workload": "byte-RLE 256 MiB uint8 + RLE v2 256 MiB int64, 256 KiB chunks, READ_UNIT 32",
+               "columns": 2}
+        return [("brle", e1, a), ("rlev2", e2, v.view(np.uint8))], cfg
+    if name == "rlev1":
+        v = cc.gen_rlev1_ints(0xA0, int(64 * MiB * scale) // 4)
+        e = cc.rlev1_encode(v, 128 * 1024, 128, 4)
+        return [("rlev1", e, v.view(np.uint8))], {"workload": "RLE v1 64 MiB int32, 128 KiB chunks, COMP_COL_LEN 128"}
+    if name == "lzss":
+        a = cc.gen_markov_copy(0xC0, int(GiB * scale), 4096)
+        e = cc.lzss_encode(a, 64 * 1024)
+        return [("lzss", e, a)], {"workload": "LZSS 1 GiB Markov+copy bytes, 64 KiB chunks"}
+    if name == "deflate":
+        total = int(GiB * scale)
+        a = cc.gen_markov_copy(0xD0, total, 32768)
+        sizes = cc.loguniform_sizes(0xD1, 8192, 4096, MiB, total)
+        oo = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+        rng = np.random.default_rng(0xD2)
+        mode = np.zeros(8192, np.uint8)
+        r = rng.random(8192)
+        mode[r < 0.015] = 1
+        mode[(r >= 0.015) & (r < 0.03)] = 2
+        e = cc.deflate_encode(a, oo, 6, mode, 1)
+        return [("deflate", e, a)], {"workload": "Deflate/zlib 1 GiB in 8192 chunks log-uniform 4 KiB-1 MiB, level 6"}
+    raise ValueError(name)
+
+
+# --------------------------------------------------------------------------
+# clocks sampler
+# --------------------------------------------------------------------------
+
+class Clocks:
+    def __init__(self, gpu_index: int):
+        self.samples = []
+        self.stop_flag = False
+        self.idx = gpu_index
+        self.th = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        while not self.stop_flag:
+            try:
+                r = subprocess.run(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}", "--format=csv,noheader,nounits"],
+                                   capture_output=True, text=True, timeout=5)
+                parts = [x.strip() for x in r.stdout.strip().split(",")]
+                if len(parts) >= 6:
+                    self.samples.append(parts)
+            except Exception:
+                pass
+            time.sleep(0.2)
+
+    def __enter__(self):
+        self.th = threading.Thread(target=self._run, daemon=True)
+        self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop_flag = True
+        if self.th:
+            self.th.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace('.', '', 1).isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace('.', '', 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# --------------------------------------------------------------------------
+# CPU baselines (oracle restatement or the reference's own code)
+# --------------------------------------------------------------------------
+
+def cpu_decode_sample(cols, threads: int, budget_s: float = 10.0):
+    """Decode a bounded prefix of each column on the host cores with the
+    oracle (the checker), in parallel over chunks.  Returns (GB/s of
+    decompressed bytes, description)."""
+    import concurrent.futures as cf
+    import copy
+    import oracle
+    # one sub-container per chunk range; ctypes releases the GIL
+    out_bytes = 0
+    t_total = 0.0
+    descr = []
+    for name, enc, raw in cols:
+        nch = enc.n_chunks
+        # sample size: start with 8 chunks per thread, grow until ~budget/len(cols)
+        take = min(nch, max(threads, 8))
+        per = budget_s / len(cols)
+        while True:
+            parts = _split(enc, take, threads)
+            t0 = time.perf_counter()
+            with cf.ThreadPoolExecutor(threads) as ex:
+                rcs = list(ex.map(lambda e: oracle.decode(e)[0], parts))
+            dt = time.perf_counter() - t0
+            if any(rcs):
+                raise RuntimeError(f"oracle failed on {name}")
+            if dt > per / 4 or take >= nch:
+                break
+            take = min(nch, take * 4)
+        nb = sum(p.n_out for p in parts)
+        out_bytes += nb
+        t_total += dt
+        descr.append(f"{name}: {take}/{nch} chunks ({nb / MiB:.0f} MiB out)")
+    return out_bytes / t_total / 1e9, "; ".join(descr)
+
+
+def _split(enc, take, threads):
+    """Sub-containers of the first `take` chunks, split into `threads` parts."""
+    import compression_b200.codecs as cc
+    res = []
+    bounds = np.linspace(0, take, threads + 1).astype(int)
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        if b <= a:
+            continue
+        res.append(_sub(enc, int(a), int(b)))
+    return res
+
+
+def _sub(enc, a, b):
+    import compression_b200.codecs as cc
+    m = enc.meta
+    cs = enc.chunk_size
+    if enc.codec == "brle":
+        p = m["ptr"]
+        data = enc.data[int(p[a]):int(p[b])]
+        ptr = (p[a:b + 1] - p[a]).astype(np.uint64)
+        n_out = min(enc.n_out, b * cs) - a * cs
+        return cc.Encoded("brle", data, n_out, b - a, cs, {"ptr": ptr})
+    if enc.codec in ("rlev1", "rlev2", "lzss"):
+        bo = m["blk_off"]
+        data = enc.data[int(bo[a]):int(bo[b])]
+        meta = {"blk_off": (bo[a:b + 1] - bo[a]).astype(np.uint64), "col_len": m["col_len"][32 * a:32 * b]}
+        if "col_map" in m:
+            meta["col_map"] = m["col_map"][32 * a:32 * b]
+        n_out = min(enc.n_out, b * cs) - a * cs
+        return cc.Encoded(enc.codec, data, n_out, b - a, cs, meta, dict(enc.params))
+    if enc.codec == "deflate":
+        co, cl, oo = m["comp_off"], m["comp_len"], m["out_off"]
+        data = enc.data[int(co[a]):int(co[b])]
+        meta = {"comp_off": (co[a:b + 1] - co[a]).astype(np.uint64), "comp_len": cl[a:b],
+                "out_off": (oo[a:b + 1] - oo[a]).astype(np.uint64)}
+        return cc.Encoded("deflate", data, int(oo[b] - oo[a]), b - a, 0, meta, dict(enc.params))
+    raise ValueError(enc.codec)
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import compression_b200.codecs as cc
+    import compression_b200 as cb
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    cols, cfg = make_workload(args.workload, args.scale)
+    jobs = [cc.DeviceJob(e, dev) for _, e, _ in cols]
+    stream = torch.cuda.current_stream(dev)
+
+    # parity check of the benchmarked data (bit-exact vs the original column)
+    for (name, e, raw), j in zip(cols, jobs):
+        j.launch()
+        torch.cuda.synchronize()
+        if not (j.status() == 0).all() or not np.array_equal(j.output(), raw):
+            raise RuntimeError(f"{name}: GPU output differs from the input column")
+
+    flush = torch.empty(256 * MiB, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def step(evs=None):
+        for i, j in enumerate(jobs):
+            if evs is not None:
+                evs[i][0].record(stream)
+            j.launch(stream)
+            if evs is not None:
+                evs[i][1].record(stream)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    K = args.steps
+    evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in jobs] for _ in range(K)]
+    torch.cuda.synchronize()
+    with Clocks(local_rank) as clk:
+        for k in range(K):
+            flush.zero_()     # L2 flushed between timed steps, outside the events
+            step(evs[k])
+        torch.cuda.synchronize()
+    per_kernel = [[evs[k][i][0].elapsed_time(evs[k][i][1]) for k in range(K)] for i in range(len(jobs))]
+    step_ms = [sum(per_kernel[i][k] for i in range(len(jobs))) for k in range(K)]
+    ms = statistics.mean(step_ms)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    out_bytes = sum(e.n_out for _, e, _ in cols)
+    value = out_bytes * world / (ms / 1e3) / 1e9
+
+    # roofline of the dominant kernel: algorithmic bytes = compressed payload
+    # + metadata read + decompressed bytes written, per launch
+    peak, peak_kind = peaks()
+    kern = []
+    for i, (name, e, _) in enumerate(cols):
+        kms = statistics.mean(per_kernel[i])
+        alg = e.comp_bytes + e.meta_bytes + e.n_out
+        kern.append({"kernel": name, "ms": round(kms, 4), "alg_bytes": alg,
+                     "gbs": round(alg / (kms / 1e3) / 1e9, 1),
+                     "decomp_gbs": round(e.n_out / (kms / 1e3) / 1e9, 1),
+                     "ratio": round(e.comp_bytes / max(e.n_out, 1), 4)})
+    dom = max(kern, key=lambda k: k["ms"])
+
+    # e2e: the reference-shaped host call (host buffers; H2D + decode + D2H inside)
+    e2e = None
+    if not args.no_e2e:
+        import ctypes
+        tot_h2d = sum(e.comp_bytes + e.meta_bytes for _, e, _ in cols)
+        for _ in range(2):
+            for _, e, _ in cols:
+                cc.decode_host_pinned(e)
+        ts = []
+        for _ in range(max(3, min(K, 5))):
+            t0 = time.perf_counter()
+            for _, e, _ in cols:
+                cc.decode_host_pinned(e)
+            ts.append(time.perf_counter() - t0)
+        e2e_s = statistics.median(ts)
+        e2e = {"value": round(out_bytes * world / e2e_s / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": int(tot_h2d), "d2h_bytes_per_step": int(out_bytes),
+               "path": "gd_*_decompress host C-ABI calls (pinned host buffers)"}
+
+    line = {
+        "metric": "decompressed GB/s (byte-RLE + RLE v2 columns)" if args.workload == "brle_rlev2"
+        else f"decompressed GB/s ({args.workload})",
+        "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8/int64" if args.workload == "brle_rlev2" else "u8", "data": "synthetic (seeded generators)",
+        "config": dict(cfg, l2="flushed between timed steps (256 MiB write)", parallelism=f"replicas x{world}"),
+        "roofline": {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["gbs"], "peak": peak,
+                     "unit": "GB/s", "frac": round(dom["gbs"] / peak, 4), "peak_source": peak_kind,
+                     "traffic": None},
+        "kernels": kern,
+        "gpu_launches": len(jobs) * K,
+        "clocks": clk.summary(),
+        "e2e": e2e,
+    }
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        gbs, sample = cpu_decode_sample(cols, threads)
+        line["cpu_baseline"] = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                                "sample": sample}
+    return line
+
+
+def run_reference(args):
+    """The reference's CPU decoders (oracle restatement where the reference
+    has none that builds here) on all host cores."""
+    cols, cfg = make_workload(args.workload, args.scale)
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(args.warmup):
+        cpu_decode_sample(cols, threads, budget_s=2.0)
+    for _ in range(args.steps):
+        gbs, sample = cpu_decode_sample(cols, threads, budget_s=6.0)
+        vals.append(gbs)
+    v = statistics.median(vals)
+    return {"impl": "reference", "metric": "decompressed GB/s (byte-RLE + RLE v2 columns)"
+            if args.workload == "brle_rlev2" else f"decompressed GB/s ({args.workload})",
+            "value": round(v, 3), "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "config": cfg,
+            "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="brle_rlev2", choices=["brle_rlev2", "rlev1", "lzss", "deflate"])
+    ap.add_argument("--scale", type=float, default=1.0, help="workload size factor (1.0 = full size)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return 0
+
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    line = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

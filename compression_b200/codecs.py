@@ -1,0 +1,333 @@
+"""Host-side mirror of the reference's codec interface over the C ABI.
+
+Each codec has an encoder (host, produces the reference container) and a
+device job that owns the device copies of the container and launches the
+sm_100a decoder through the C ABI.  torch provides device memory and streams
+only; all decoding happens in libgd.so.
+
+Reference interfaces mirrored (ZaidQureshi/compression):
+  brle::compress_gpu / decompress_gpu          include/brle/brle.h:251-342
+  rle_v1::compress_gpu / decompress_gpu        include/rle_v1/rlev1.h:25-199
+  rlev2::compress_gpu_transpose / decompress_gpu
+                                               include/rlev2/encoder_trans.h:428-537,
+                                               include/rlev2/decoder_trans.h:615-681
+  lzss::compress_gpu / decompress_gpu          include/lzss/lzss_gpu2.h:1915-2314
+  deflate::decompress_gpu (+ Python producer)  include/zlib/zlib.h:966-1082,
+                                               orig_compressor.py:44-126
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import lib
+
+BRLE_CHUNK = 256 * 1024  # include/brle/brle.h:8
+
+
+class DecodeError(RuntimeError):
+    def __init__(self, status: int, where: str = ""):
+        s = lib().gd_status_string(int(status)).decode()
+        super().__init__(f"{where}: {s} ({status})")
+        self.status = int(status)
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def check(rc: int, where: str) -> None:
+    if rc != 0:
+        raise DecodeError(rc, where)
+
+
+# --------------------------------------------------------------------------
+# generators
+# --------------------------------------------------------------------------
+
+def gen_rlev1_ints(seed: int, n: int) -> np.ndarray:
+    a = np.empty(n, dtype=np.int32)
+    lib().gd_gen_rlev1_ints(seed, n, _p(a))
+    return a
+
+
+def gen_brle_bytes(seed: int, n: int) -> np.ndarray:
+    a = np.empty(n, dtype=np.uint8)
+    lib().gd_gen_brle_bytes(seed, n, _p(a))
+    return a
+
+
+def gen_rlev2_ints(seed: int, n: int) -> np.ndarray:
+    a = np.empty(n, dtype=np.int64)
+    lib().gd_gen_rlev2_ints(seed, n, _p(a))
+    return a
+
+
+def gen_markov_copy(seed: int, n: int, max_dist: int) -> np.ndarray:
+    a = np.empty(n, dtype=np.uint8)
+    lib().gd_gen_markov_copy(seed, n, max_dist, _p(a))
+    return a
+
+
+def loguniform_sizes(seed: int, n: int, lo: int, hi: int, total: int, granule: int = 1) -> np.ndarray:
+    a = np.empty(n, dtype=np.uint64)
+    check(lib().gd_gen_loguniform_sizes(seed, n, lo, hi, total, granule, _p(a)), "loguniform_sizes")
+    return a
+
+
+# --------------------------------------------------------------------------
+# encoded containers
+# --------------------------------------------------------------------------
+
+@dataclass
+class Encoded:
+    """One compressed column: payload bytes plus its metadata arrays."""
+    codec: str
+    data: np.ndarray                  # uint8 payload (blocks / chunk streams)
+    n_out: int                        # decompressed bytes
+    n_chunks: int
+    chunk_size: int = 0
+    meta: dict = field(default_factory=dict)   # named uint64/uint8 arrays
+    params: dict = field(default_factory=dict)
+
+    @property
+    def comp_bytes(self) -> int:
+        return int(self.data.nbytes)
+
+    @property
+    def meta_bytes(self) -> int:
+        return int(sum(v.nbytes for v in self.meta.values()))
+
+
+def _as_u8(raw) -> np.ndarray:
+    a = np.ascontiguousarray(raw)
+    return a.view(np.uint8).reshape(-1)
+
+
+def brle_encode(raw, chunk_size: int = BRLE_CHUNK) -> Encoded:
+    """brle::compress_gpu: container [u32 n_ptr][u64 ptr[n_ptr]][u64 total][data]."""
+    b = _as_u8(raw)
+    L = lib()
+    cap = L.gd_brle_max_encoded_bytes(b.size, chunk_size)
+    out = np.empty(cap, dtype=np.uint8)
+    n = L.gd_brle_encode(_p(b), b.size, chunk_size, _p(out))
+    if n == 0:
+        raise ValueError("brle encode failed")
+    cont = out[:n].copy()
+    n_ptr = int(cont[:4].view(np.uint32)[0])
+    ptr = cont[4:4 + 8 * n_ptr].copy().view(np.uint64)
+    hdr = 4 + 8 * n_ptr + 8
+    return Encoded("brle", cont[hdr:].copy(), b.size, n_ptr - 1, chunk_size, {"ptr": ptr}, {"container": cont})
+
+
+def brle_container(enc: Encoded) -> np.ndarray:
+    return enc.params["container"]
+
+
+def rlev1_encode(raw, chunk_size: int = 128 * 1024, comp_col_len: int = 128, elem_bytes: int = 4) -> Encoded:
+    """rle_v1::compress_gpu (32-lane interleaved blocks + col_len + blk_offset)."""
+    b = _as_u8(raw)
+    L = lib()
+    nc = (b.size + chunk_size - 1) // chunk_size
+    cap = L.gd_rlev1_max_encoded_bytes(b.size, chunk_size)
+    data = np.empty(cap, dtype=np.uint8)
+    blk = np.empty(nc + 1, dtype=np.uint64)
+    col = np.empty(32 * nc, dtype=np.uint64)
+    n = L.gd_rlev1_encode(_p(b), b.size, chunk_size, comp_col_len, elem_bytes, _p(data), _p(blk), _p(col))
+    if n == 0:
+        raise ValueError("rlev1 encode failed")
+    return Encoded("rlev1", data[:n].copy(), b.size, nc, chunk_size, {"blk_off": blk, "col_len": col},
+                   {"comp_col_len": comp_col_len, "elem_bytes": elem_bytes})
+
+
+def rlev2_encode(raw, chunk_size: int = 256 * 1024, read_unit: int = 32) -> Encoded:
+    """rlev2::compress_gpu_transpose (8-byte values)."""
+    b = _as_u8(raw)
+    L = lib()
+    nc = (b.size + chunk_size - 1) // chunk_size
+    cap = L.gd_rlev2_max_encoded_bytes(b.size, chunk_size)
+    data = np.empty(cap, dtype=np.uint8)
+    blk = np.empty(nc + 1, dtype=np.uint64)
+    col = np.empty(32 * nc, dtype=np.uint64)
+    n = L.gd_rlev2_encode(_p(b), b.size, chunk_size, read_unit, _p(data), _p(blk), _p(col))
+    if n == 0:
+        raise ValueError("rlev2 encode failed")
+    return Encoded("rlev2", data[:n].copy(), b.size, nc, chunk_size, {"blk_off": blk, "col_len": col},
+                   {"read_unit": read_unit})
+
+
+def lzss_encode(raw, chunk_size: int = 64 * 1024) -> Encoded:
+    """lzss::compress_gpu (32-column interleaved blocks + .meta arrays)."""
+    b = _as_u8(raw)
+    L = lib()
+    nc = (b.size + chunk_size - 1) // chunk_size
+    cap = L.gd_lzss_max_encoded_bytes(b.size, chunk_size)
+    data = np.empty(cap, dtype=np.uint8)
+    blk = np.empty(nc + 1, dtype=np.uint64)
+    col = np.empty(32 * nc, dtype=np.uint64)
+    cmap = np.empty(32 * nc, dtype=np.uint8)
+    n = L.gd_lzss_encode(_p(b), b.size, chunk_size, _p(data), _p(blk), _p(col), _p(cmap))
+    if n == 0:
+        raise ValueError("lzss encode failed")
+    return Encoded("lzss", data[:n].copy(), b.size, nc, chunk_size,
+                   {"blk_off": blk, "col_len": col, "col_map": cmap}, {})
+
+
+def deflate_encode(raw, out_off: np.ndarray, level: int = 6, mode: np.ndarray | None = None,
+                   zlib_header: int = 1) -> Encoded:
+    """Per-chunk zlib streams padded to 8 bytes (orig_compressor.py:44-126).
+
+    out_off[n+1]: chunk c covers raw[out_off[c]:out_off[c+1]].  mode[c]:
+    0 default strategy, 1 fixed Huffman (Z_FIXED), 2 stored (level 0)."""
+    b = _as_u8(raw)
+    L = lib()
+    oo = np.ascontiguousarray(out_off, dtype=np.uint64)
+    n = oo.size - 1
+    cap = L.gd_deflate_max_encoded_bytes(_p(oo), n)
+    data = np.empty(cap, dtype=np.uint8)
+    coff = np.empty(n + 1, dtype=np.uint64)
+    clen = np.empty(n, dtype=np.uint64)
+    m = None if mode is None else np.ascontiguousarray(mode, dtype=np.uint8)
+    got = L.gd_deflate_encode(_p(b), _p(oo), n, level, None if m is None else _p(m), zlib_header, _p(data),
+                              _p(coff), _p(clen))
+    if got == 0:
+        raise ValueError("deflate encode failed")
+    return Encoded("deflate", data[:got].copy(), int(oo[-1]), n, 0,
+                   {"comp_off": coff, "comp_len": clen, "out_off": oo}, {"zlib_header": zlib_header})
+
+
+# --------------------------------------------------------------------------
+# device jobs
+# --------------------------------------------------------------------------
+
+class DeviceJob:
+    """Device-resident copy of an Encoded container plus its output buffer.
+
+    ``launch(stream)`` enqueues the decoder; ``status()`` returns the per-chunk
+    status array.  torch is used for allocation and streams only.
+    """
+
+    def __init__(self, enc: Encoded, device="cuda", out=None):
+        import torch
+        self.torch = torch
+        self.enc = enc
+        self.dev = torch.device(device)
+        # payload padded to 16 bytes (the inflate reader fetches aligned words)
+        pad = (-enc.data.size) % 16 + 16
+        d = np.concatenate([enc.data, np.zeros(pad, dtype=np.uint8)])
+        self.d_data = torch.from_numpy(d).to(self.dev)
+        self.d_meta = {k: torch.from_numpy(np.ascontiguousarray(v)).to(self.dev) for k, v in enc.meta.items()}
+        if enc.codec in ("rlev1", "rlev2", "lzss"):
+            # the device API bounds the last block by blk_off[n]
+            pass
+        out_n = enc.n_out
+        if enc.codec == "lzss":
+            out_n = enc.n_chunks * enc.chunk_size
+        self.out_n = out_n
+        self.d_out = out if out is not None else torch.empty(max(out_n, 16), dtype=torch.uint8, device=self.dev)
+        self.d_status = torch.zeros(max(enc.n_chunks, 1), dtype=torch.int32, device=self.dev)
+
+    def launch(self, stream=None) -> None:
+        L = lib()
+        e = self.enc
+        s = C.c_void_p(stream.cuda_stream if stream is not None else
+                       self.torch.cuda.current_stream(self.dev).cuda_stream)
+        m = self.d_meta
+        ptr = lambda t: C.c_void_p(t.data_ptr())
+        if e.codec == "brle":
+            rc = L.gd_brle_decode(ptr(self.d_data), ptr(m["ptr"]), e.n_chunks, e.chunk_size, ptr(self.d_out),
+                                  e.n_out, ptr(self.d_status), s)
+        elif e.codec == "rlev1":
+            rc = L.gd_rlev1_decode(ptr(self.d_data), ptr(m["col_len"]), ptr(m["blk_off"]), e.n_chunks,
+                                   e.chunk_size, e.params["comp_col_len"], e.params["elem_bytes"],
+                                   ptr(self.d_out), e.n_out, ptr(self.d_status), s)
+        elif e.codec == "rlev2":
+            rc = L.gd_rlev2_decode(ptr(self.d_data), ptr(m["col_len"]), ptr(m["blk_off"]), e.n_chunks,
+                                   e.chunk_size, e.params["read_unit"], ptr(self.d_out), e.n_out,
+                                   ptr(self.d_status), s)
+        elif e.codec == "lzss":
+            rc = L.gd_lzss_decode(ptr(self.d_data), ptr(m["blk_off"]), ptr(m["col_len"]), ptr(m["col_map"]),
+                                  e.n_chunks, e.chunk_size, ptr(self.d_out), self.out_n, ptr(self.d_status), s)
+        elif e.codec == "deflate":
+            rc = L.gd_inflate(ptr(self.d_data), ptr(m["comp_off"]), ptr(m["comp_len"]), ptr(m["out_off"]),
+                              e.n_chunks, e.params["zlib_header"], ptr(self.d_out), ptr(self.d_status), s)
+        else:
+            raise ValueError(e.codec)
+        check(rc, f"{e.codec} launch")
+
+    def status(self) -> np.ndarray:
+        return self.d_status.cpu().numpy().astype(np.uint32)
+
+    def output(self) -> np.ndarray:
+        return self.d_out[: self.enc.n_out].cpu().numpy()
+
+
+def _pinned_copy(a: np.ndarray) -> np.ndarray:
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    arr = t.numpy()
+    arr._keep = t  # noqa: keep the pinned tensor alive with the view  # type: ignore[attr-defined]
+    return arr
+
+
+def decode_host_pinned(enc: Encoded) -> np.ndarray:
+    """decode_host with the container held in page-locked host memory (the
+    pinned copies are made once and cached on `enc`)."""
+    if "_pinned" not in enc.params:
+        pm = {k: _pinned_copy(v) for k, v in enc.meta.items()}
+        pd = _pinned_copy(enc.data)
+        pc = _pinned_copy(enc.params["container"]) if "container" in enc.params else None
+        enc.params["_pinned"] = (pd, pm, pc)
+    pd, pm, pc = enc.params["_pinned"]
+    view = Encoded(enc.codec, pd, enc.n_out, enc.n_chunks, enc.chunk_size, pm,
+                   {k: v for k, v in enc.params.items() if k not in ("_pinned", "container")})
+    if pc is not None:
+        view.params["container"] = pc
+    return decode_host(view, keep=False)
+
+
+def decode_host(enc: Encoded, keep: bool = True) -> np.ndarray:
+    """Reference-shaped synchronous host call (H2D, decode, D2H) via the C ABI.
+
+    keep=False returns None after releasing the library's output buffer (used
+    for timing the call itself)."""
+    L = lib()
+    out = C.c_void_p()
+    n = C.c_uint64()
+    m = enc.meta
+    if enc.codec == "brle":
+        cont = enc.params["container"]
+        rc = L.gd_brle_decompress(_p(cont), cont.size, C.byref(out), C.byref(n))
+    elif enc.codec == "rlev1":
+        buf = np.concatenate([np.array([enc.n_out], dtype=np.uint64).view(np.uint8), enc.data])
+        rc = L.gd_rlev1_decompress(_p(buf), buf.size, _p(m["col_len"]), m["col_len"].nbytes, _p(m["blk_off"]),
+                                   m["blk_off"].nbytes, enc.params["comp_col_len"], enc.params["elem_bytes"],
+                                   enc.chunk_size, C.byref(out), C.byref(n))
+    elif enc.codec == "rlev2":
+        blk = m["blk_off"].copy()
+        blk[-1] = enc.n_out  # the reference stores the decompressed size there
+        rc = L.gd_rlev2_decompress(_p(enc.data), enc.data.size, enc.n_chunks, _p(blk), _p(m["col_len"]),
+                                   enc.params["read_unit"], enc.chunk_size, C.byref(out), C.byref(n))
+    elif enc.codec == "lzss":
+        cs = np.array([enc.chunk_size], dtype=np.uint64)
+        arrs = [cs, m["blk_off"], m["col_len"], m["col_map"]]
+        ptrs = (C.c_void_p * 4)(*[_p(a) for a in arrs])
+        lens = np.array([a.nbytes for a in arrs], dtype=np.uint64)
+        rc = L.gd_lzss_decompress(_p(enc.data), enc.data.size, ptrs, _p(lens), 4, C.byref(out), C.byref(n))
+    elif enc.codec == "deflate":
+        # reference triple: blk_offset = [total][0][cumulative], col_len = padded lengths
+        blk = np.concatenate([np.array([enc.n_out], dtype=np.uint64), m["comp_off"]])
+        cs = int(m["out_off"][1] - m["out_off"][0]) if enc.n_chunks > 0 else 1
+        rc = L.gd_deflate_decompress(_p(enc.data), enc.data.size, _p(m["comp_len"]), m["comp_len"].nbytes,
+                                     _p(blk), blk.nbytes, cs, C.byref(out), C.byref(n))
+    else:
+        raise ValueError(enc.codec)
+    check(rc, f"{enc.codec} host decompress")
+    res = None
+    if keep:
+        res = np.ctypeslib.as_array(C.cast(out, C.POINTER(C.c_uint8)), shape=(n.value,)).copy() if n.value else \
+            np.empty(0, np.uint8)
+    L.gd_free(out)
+    return res

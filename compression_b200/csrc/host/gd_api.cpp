@@ -1,0 +1,357 @@
+// gd_api.cpp -- host side of the C ABI: status strings, the reference-shaped
+// synchronous host API (H2D copy, device decode, D2H copy, malloc'd output),
+// and the per-thread device staging pool behind it.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "../../../include/gd.h"
+
+namespace {
+
+// Grow-only device buffers, one set per host thread.  Slots are reused
+// across calls so the host API does not pay cudaMalloc on every call.
+struct Pool {
+    struct Slot {
+        void* p = nullptr;
+        size_t cap = 0;
+        int dev = -1;
+    };
+    Slot s[8];
+    ~Pool() {
+        for (auto& x : s)
+            if (x.p) cudaFree(x.p);  // may fail harmlessly at process teardown
+    }
+    void* get(int i, size_t n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        Slot& x = s[i];
+        if (n == 0) n = 16;
+        if (x.p && x.cap >= n && x.dev == dev) return x.p;
+        if (x.p) {
+            int cur = dev;
+            cudaSetDevice(x.dev);
+            cudaFree(x.p);
+            cudaSetDevice(cur);
+        }
+        x.p = nullptr;
+        x.cap = 0;
+        size_t cap = (n + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1);
+        if (cudaMalloc(&x.p, cap) != cudaSuccess) {
+            cudaGetLastError();
+            x.p = nullptr;
+            return nullptr;
+        }
+        x.cap = cap;
+        x.dev = dev;
+        return x.p;
+    }
+};
+thread_local Pool g_pool;
+
+// Output buffers of the host API are page-locked so the device-to-host copy
+// runs at full link speed.  They are recycled: gd_free() returns a buffer to
+// this cache instead of unpinning it (pinning is expensive).
+struct PinnedCache {
+    std::mutex m;
+    std::unordered_map<void*, size_t> live;      // handed out -> capacity
+    std::vector<std::pair<void*, size_t>> idle;  // free for reuse
+    void* get(size_t n) {
+        std::lock_guard<std::mutex> g(m);
+        size_t best = (size_t)-1;
+        int bi = -1;
+        for (size_t i = 0; i < idle.size(); ++i)
+            if (idle[i].second >= n && idle[i].second < best) {
+                best = idle[i].second;
+                bi = (int)i;
+            }
+        if (bi >= 0) {
+            auto e = idle[bi];
+            idle.erase(idle.begin() + bi);
+            live[e.first] = e.second;
+            return e.first;
+        }
+        void* p = nullptr;
+        const size_t cap = n ? n : 1;
+        if (cudaHostAlloc(&p, cap, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            p = malloc(cap);  // pageable fallback for the host buffer only
+            return p;
+        }
+        live[p] = cap;
+        return p;
+    }
+    bool put(void* p) {
+        std::lock_guard<std::mutex> g(m);
+        auto it = live.find(p);
+        if (it == live.end()) return false;
+        idle.emplace_back(it->first, it->second);
+        live.erase(it);
+        // keep at most 8 idle buffers pinned
+        while (idle.size() > 8) {
+            cudaFreeHost(idle.front().first);
+            idle.erase(idle.begin());
+        }
+        return true;
+    }
+};
+PinnedCache& pinned() {
+    static PinnedCache* c = new PinnedCache();  // never destroyed: outlives CUDA teardown
+    return *c;
+}
+
+gd_status_t collect(const uint32_t* d_status, uint32_t n, cudaStream_t s) {
+    std::vector<uint32_t> st(n);
+    if (cudaMemcpyAsync(st.data(), d_status, 4ull * n, cudaMemcpyDeviceToHost, s) != cudaSuccess) return GD_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return GD_ERR_CUDA;
+    uint32_t worst = GD_OK;
+    for (uint32_t v : st)
+        if (v > worst) worst = v;
+    return (gd_status_t)worst;
+}
+
+template <typename T>
+T rd(const uint8_t* p) {
+    T v;
+    memcpy(&v, p, sizeof(T));
+    return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gd_version(void) { return "gd-b200 0.1 (sm_100a)"; }
+
+const char* gd_status_string(int s) {
+    switch (s) {
+        case GD_OK: return "ok";
+        case GD_ERR_INVALID_ARG: return "invalid argument";
+        case GD_ERR_CORRUPT: return "corrupt stream";
+        case GD_ERR_OVERRUN: return "output overrun";
+        case GD_ERR_TIMEOUT: return "device wait timed out";
+        case GD_ERR_UNSUPPORTED: return "unsupported";
+        case GD_ERR_CUDA: return "cuda error";
+        case GD_ERR_NOMEM: return "out of memory";
+        default: return "unknown";
+    }
+}
+
+void gd_free(void* p) {
+    if (p && !pinned().put(p)) free(p);
+}
+
+// ---------------------------------------------------------------------------
+gd_status_t gd_brle_decompress(const uint8_t* in, uint64_t in_n_bytes, uint8_t** out, uint64_t* out_n_bytes) {
+    if (!in || !out || !out_n_bytes || in_n_bytes < 4) return GD_ERR_INVALID_ARG;
+    const uint32_t n_ptr = rd<uint32_t>(in);
+    if (n_ptr < 1) return GD_ERR_INVALID_ARG;
+    const uint64_t hdr = 4ull + 8ull * n_ptr;
+    if (in_n_bytes < hdr + 8) return GD_ERR_INVALID_ARG;
+    const uint32_t n_chunks = n_ptr - 1;
+    const uint64_t total = rd<uint64_t>(in + hdr);
+    const uint8_t* data = in + hdr + 8;
+    const uint64_t data_n = in_n_bytes - hdr - 8;
+    const uint64_t chunk = 256 * 1024;  // CHUNK_SIZE, include/brle/brle.h:8
+    std::vector<uint64_t> ptr(n_ptr);
+    memcpy(ptr.data(), in + 4, 8ull * n_ptr);
+    if (ptr[n_chunks] > data_n) return GD_ERR_CORRUPT;
+    *out = nullptr;
+    *out_n_bytes = 0;
+    if (n_chunks == 0 || total == 0) {
+        *out = (uint8_t*)malloc(1);
+        return total == 0 ? GD_OK : GD_ERR_CORRUPT;
+    }
+    cudaStream_t s = 0;
+    uint8_t* d_data = (uint8_t*)g_pool.get(0, data_n);
+    uint64_t* d_ptr = (uint64_t*)g_pool.get(1, 8ull * n_ptr);
+    uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
+    uint32_t* d_st = (uint32_t*)g_pool.get(3, 4ull * n_chunks);
+    if (!d_data || !d_ptr || !d_out || !d_st) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(d_data, data, data_n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_ptr, ptr.data(), 8ull * n_ptr, cudaMemcpyHostToDevice, s);
+    gd_status_t r = gd_brle_decode(d_data, d_ptr, n_chunks, chunk, d_out, total, d_st, s);
+    if (r != GD_OK) return r;
+    uint8_t* h = (uint8_t*)pinned().get(total);
+    if (!h) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
+    r = collect(d_st, n_chunks, s);
+    if (r != GD_OK) {
+        gd_free(h);
+        return r;
+    }
+    *out = h;
+    *out_n_bytes = total;
+    return GD_OK;
+}
+
+// ---------------------------------------------------------------------------
+gd_status_t gd_rlev1_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* col_len,
+                                uint64_t col_n_bytes, const uint64_t* blk_off, uint64_t blk_n_bytes,
+                                uint32_t comp_col_len, uint32_t elem_bytes, uint64_t chunk_size, uint8_t** out,
+                                uint64_t* out_n_bytes) {
+    if (!in || !col_len || !blk_off || !out || !out_n_bytes || in_n_bytes < 8 || blk_n_bytes < 16)
+        return GD_ERR_INVALID_ARG;
+    const uint64_t n = blk_n_bytes / 8 - 1;
+    if (col_n_bytes < 8 * 32 * n) return GD_ERR_INVALID_ARG;
+    const uint64_t total = rd<uint64_t>(in);
+    const uint8_t* data = in + 8;
+    const uint64_t data_n = in_n_bytes - 8;
+    if (blk_off[n] > data_n || total > n * chunk_size) return GD_ERR_CORRUPT;
+    *out = nullptr;
+    *out_n_bytes = 0;
+    cudaStream_t s = 0;
+    uint8_t* d_data = (uint8_t*)g_pool.get(0, data_n);
+    uint64_t* d_cl = (uint64_t*)g_pool.get(1, 8 * 32 * n);
+    uint64_t* d_bo = (uint64_t*)g_pool.get(4, 8 * (n + 1));
+    uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
+    uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
+    if (!d_data || !d_cl || !d_bo || !d_out || !d_st) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(d_data, data, data_n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_cl, col_len, 8 * 32 * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_bo, blk_off, 8 * (n + 1), cudaMemcpyHostToDevice, s);
+    gd_status_t r = gd_rlev1_decode(d_data, d_cl, d_bo, (uint32_t)n, chunk_size, comp_col_len, elem_bytes, d_out,
+                                    total, d_st, s);
+    if (r != GD_OK) return r;
+    uint8_t* h = (uint8_t*)pinned().get(total ? total : 1);
+    if (!h) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
+    r = collect(d_st, (uint32_t)n, s);
+    if (r != GD_OK) {
+        gd_free(h);
+        return r;
+    }
+    *out = h;
+    *out_n_bytes = total;
+    return GD_OK;
+}
+
+// ---------------------------------------------------------------------------
+gd_status_t gd_rlev2_decompress(const uint8_t* in, uint64_t in_n_bytes, uint64_t n_chunks, const uint64_t* blk_off,
+                                const uint64_t* col_len, uint32_t read_unit, uint64_t chunk_size, uint8_t** out,
+                                uint64_t* out_n_bytes) {
+    if (!in || !blk_off || !col_len || !out || !out_n_bytes || n_chunks == 0) return GD_ERR_INVALID_ARG;
+    const uint64_t total = blk_off[n_chunks];  // the decompressed size (encoder_trans.h:490-492)
+    if (total > n_chunks * chunk_size || total <= (n_chunks - 1) * chunk_size) return GD_ERR_CORRUPT;
+    std::vector<uint64_t> bo(blk_off, blk_off + n_chunks + 1);
+    bo[n_chunks] = in_n_bytes;  // device API: last entry bounds the data
+    *out = nullptr;
+    *out_n_bytes = 0;
+    cudaStream_t s = 0;
+    uint8_t* d_data = (uint8_t*)g_pool.get(0, in_n_bytes);
+    uint64_t* d_cl = (uint64_t*)g_pool.get(1, 8 * 32 * n_chunks);
+    uint64_t* d_bo = (uint64_t*)g_pool.get(4, 8 * (n_chunks + 1));
+    uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
+    uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n_chunks);
+    if (!d_data || !d_cl || !d_bo || !d_out || !d_st) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(d_data, in, in_n_bytes, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_cl, col_len, 8 * 32 * n_chunks, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_bo, bo.data(), 8 * (n_chunks + 1), cudaMemcpyHostToDevice, s);
+    gd_status_t r =
+        gd_rlev2_decode(d_data, d_cl, d_bo, (uint32_t)n_chunks, chunk_size, read_unit, d_out, total, d_st, s);
+    if (r != GD_OK) return r;
+    uint8_t* h = (uint8_t*)pinned().get(total);
+    if (!h) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
+    r = collect(d_st, (uint32_t)n_chunks, s);
+    if (r != GD_OK) {
+        gd_free(h);
+        return r;
+    }
+    *out = h;
+    *out_n_bytes = total;
+    return GD_OK;
+}
+
+// ---------------------------------------------------------------------------
+int gd_lzss_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint8_t* const* meta, const uint64_t* meta_lens,
+                       uint64_t meta_num, uint8_t** out, uint64_t* out_n_bytes) {
+    if (meta_num < 4 || !meta || !meta_lens) return -1;  // as lzss_gpu2.h:2212-2213
+    if (!in || !out || !out_n_bytes || meta_lens[0] < 8) return GD_ERR_INVALID_ARG;
+    const uint64_t chunk = rd<uint64_t>(meta[0]);
+    const uint64_t n = meta_lens[1] / 8 - 1;
+    if (n == 0 || meta_lens[2] < 8 * 32 * n || meta_lens[3] < 32 * n) return GD_ERR_INVALID_ARG;
+    std::vector<uint64_t> bo(n + 1);
+    memcpy(bo.data(), meta[1], 8 * (n + 1));
+    if (bo[n] > in_n_bytes) return GD_ERR_CORRUPT;
+    const uint64_t total = n * chunk;
+    *out = nullptr;
+    *out_n_bytes = 0;
+    cudaStream_t s = 0;
+    uint8_t* d_data = (uint8_t*)g_pool.get(0, in_n_bytes);
+    uint64_t* d_cl = (uint64_t*)g_pool.get(1, 8 * 32 * n);
+    uint64_t* d_bo = (uint64_t*)g_pool.get(4, 8 * (n + 1));
+    uint8_t* d_map = (uint8_t*)g_pool.get(5, 32 * n);
+    uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
+    uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
+    if (!d_data || !d_cl || !d_bo || !d_map || !d_out || !d_st) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(d_data, in, in_n_bytes, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_cl, meta[2], 8 * 32 * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_bo, bo.data(), 8 * (n + 1), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_map, meta[3], 32 * n, cudaMemcpyHostToDevice, s);
+    int r = gd_lzss_decode(d_data, d_bo, d_cl, d_map, (uint32_t)n, chunk, d_out, total, d_st, s);
+    if (r != GD_OK) return r;
+    uint8_t* h = (uint8_t*)pinned().get(total);
+    if (!h) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
+    r = collect(d_st, (uint32_t)n, s);
+    if (r != GD_OK) {
+        gd_free(h);
+        return r;
+    }
+    *out = h;
+    *out_n_bytes = total;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+gd_status_t gd_deflate_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* col_len,
+                                  uint64_t col_n_bytes, const uint64_t* blk_offset, uint64_t blk_n_bytes,
+                                  uint64_t chunk_size, uint8_t** out, uint64_t* out_n_bytes) {
+    if (!in || !col_len || !blk_offset || !out || !out_n_bytes || blk_n_bytes < 24 || chunk_size == 0)
+        return GD_ERR_INVALID_ARG;
+    const uint64_t n = blk_n_bytes / 8 - 2;  // zlib.h:970
+    if (col_n_bytes < 8 * n) return GD_ERR_INVALID_ARG;
+    const uint64_t total = blk_offset[0];
+    if (total > n * chunk_size || total <= (n - 1) * chunk_size) return GD_ERR_CORRUPT;
+    std::vector<uint64_t> coff(n + 1), clen(n), ooff(n + 1);
+    for (uint64_t i = 0; i <= n; ++i) coff[i] = blk_offset[1 + i];
+    for (uint64_t i = 0; i < n; ++i) {
+        clen[i] = col_len[i];
+        ooff[i] = i * chunk_size;
+        if (coff[i] + clen[i] > in_n_bytes) return GD_ERR_CORRUPT;
+    }
+    ooff[n] = total;
+    *out = nullptr;
+    *out_n_bytes = 0;
+    cudaStream_t s = 0;
+    uint8_t* d_data = (uint8_t*)g_pool.get(0, in_n_bytes);
+    uint64_t* d_meta = (uint64_t*)g_pool.get(1, 8 * (3 * n + 2));
+    uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
+    uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
+    if (!d_data || !d_meta || !d_out || !d_st) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(d_data, in, in_n_bytes, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_meta, coff.data(), 8 * (n + 1), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_meta + n + 1, clen.data(), 8 * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_meta + 2 * n + 1, ooff.data(), 8 * (n + 1), cudaMemcpyHostToDevice, s);
+    gd_status_t r = gd_inflate(d_data, d_meta, d_meta + n + 1, d_meta + 2 * n + 1, (uint32_t)n, 1, d_out, d_st, s);
+    if (r != GD_OK) return r;
+    uint8_t* h = (uint8_t*)pinned().get(total);
+    if (!h) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
+    r = collect(d_st, (uint32_t)n, s);
+    if (r != GD_OK) {
+        gd_free(h);
+        return r;
+    }
+    *out = h;
+    *out_n_bytes = total;
+    return GD_OK;
+}
+
+}  // extern "C"

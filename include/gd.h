@@ -1,0 +1,240 @@
+/*
+ * gd.h -- C ABI of the B200 decode library (libgd.so).
+ *
+ * This is the drop-in boundary for the decompress calls of
+ * ZaidQureshi/compression.  Each entry point names the reference interface
+ * it replaces (file:line within that project).  The ABI uses plain pointers
+ * and sizes only; a CUDA stream is passed as an opaque `gd_stream_t`
+ * (a cudaStream_t, NULL = legacy default stream).
+ *
+ * Two tiers:
+ *   - Device API (gd_*_decode): device pointers in and out, asynchronous on
+ *     the given stream, caller owns every buffer, per-chunk status written to
+ *     device memory.  Thread safe; never allocates.
+ *   - Host API (gd_*_decompress): the reference's synchronous host-buffer
+ *     signatures (H2D copy, decode, D2H copy, callee-allocated output that
+ *     the caller releases with gd_free).  Device staging buffers come from a
+ *     per-device pool owned by the library.
+ *
+ * Status codes are returned by every call and written per chunk by kernels.
+ * No decoder traps, asserts or waits without a bound: a malformed stream
+ * yields GD_ERR_CORRUPT / GD_ERR_OVERRUN for that chunk.
+ */
+#ifndef GD_H_
+#define GD_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gd_status {
+    GD_OK = 0,
+    GD_ERR_INVALID_ARG = 1, /* bad sizes / pointers / parameters */
+    GD_ERR_CORRUPT = 2,     /* stream grammar violated or truncated */
+    GD_ERR_OVERRUN = 3,     /* stream would write past its chunk */
+    GD_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+    GD_ERR_UNSUPPORTED = 5, /* valid but unsupported feature */
+    GD_ERR_CUDA = 6,        /* CUDA runtime error */
+    GD_ERR_NOMEM = 7        /* allocation failed (host API only) */
+} gd_status_t;
+
+typedef void* gd_stream_t;
+
+/* Library version string. */
+const char* gd_version(void);
+/* Human-readable name of a status code. */
+const char* gd_status_string(int status);
+
+/* ------------------------------------------------------------------------
+ * Device API
+ * ------------------------------------------------------------------------ */
+
+/*
+ * Byte-RLE, contiguous chunk container (brle.h format).
+ * Replaces brle::kernel_decompress / brle::decompress_gpu
+ * (include/brle/brle.h:102-109, :305-342).
+ * d_data: compressed payload; d_ptr[n_chunks+1]: byte offsets of each chunk
+ * in d_data; chunk c decodes to d_out[c*chunk_size ..], the last chunk to
+ * out_n_bytes - c*chunk_size bytes.  d_status: n_chunks uint32 (may be NULL).
+ */
+gd_status_t gd_brle_decode(const uint8_t* d_data, const uint64_t* d_ptr, uint32_t n_chunks,
+                           uint64_t chunk_size, uint8_t* d_out, uint64_t out_n_bytes,
+                           uint32_t* d_status, gd_stream_t stream);
+
+/*
+ * RLE v1, 32-lane interleaved container.
+ * Replaces rle_v1::inflate / rle_v1::decompress_gpu
+ * (include/rle_v1/decoder.h:426-470, include/rle_v1/rlev1.h:100-199).
+ * d_data: compressed blocks (the container after its 8-byte size header);
+ * d_col_len[32*n_chunks]: per-lane stream bytes; d_blk_off[n_chunks+1]:
+ * block start offsets.  elem_bytes 4 or 8; comp_col_len = COMP_COL_LEN.
+ */
+gd_status_t gd_rlev1_decode(const uint8_t* d_data, const uint64_t* d_col_len, const uint64_t* d_blk_off,
+                            uint32_t n_chunks, uint64_t chunk_size, uint32_t comp_col_len,
+                            uint32_t elem_bytes, uint8_t* d_out, uint64_t out_n_bytes,
+                            uint32_t* d_status, gd_stream_t stream);
+
+/*
+ * RLE v2, 32-lane transposed container (8-byte values).
+ * Replaces rlev2::inflate / rlev2::decompress_gpu<READ_UNIT,...>
+ * (include/rlev2/decoder_new.h:618-657, include/rlev2/decoder_trans.h:615-681).
+ * read_unit = READ_UNIT (values per lane slice).
+ */
+gd_status_t gd_rlev2_decode(const uint8_t* d_data, const uint64_t* d_col_len, const uint64_t* d_blk_off,
+                            uint32_t n_chunks, uint64_t chunk_size, uint32_t read_unit,
+                            uint8_t* d_out, uint64_t out_n_bytes, uint32_t* d_status,
+                            gd_stream_t stream);
+
+/*
+ * LZSS, 32-column interleaved container.
+ * Replaces lzss::kernel_decompress(blk_off,col_len,col_map)
+ * (include/lzss/lzss_gpu2.h:1898-1907 -> decompress_func :112-325).
+ * d_col_len: stream bytes per rank (sorted descending); d_col_map: rank ->
+ * output column.  chunk_size multiple of 128 (runtime; the reference fixes
+ * it at 128 KiB, lzss_gpu2.h:25).
+ */
+gd_status_t gd_lzss_decode(const uint8_t* d_data, const uint64_t* d_blk_off, const uint64_t* d_col_len,
+                           const uint8_t* d_col_map, uint32_t n_chunks, uint64_t chunk_size,
+                           uint8_t* d_out, uint64_t out_n_bytes, uint32_t* d_status,
+                           gd_stream_t stream);
+
+/*
+ * Deflate / zlib inflate of independent chunks of any size.
+ * Replaces deflate::inflate / inflate_shared / deflate::decompress_gpu
+ * (include/zlib/zlib.h:832-962, :966-1082).  Chunk c: compressed bytes at
+ * d_data + d_comp_off[c] (d_comp_len[c] bytes, trailing zero padding
+ * allowed), output d_out[d_out_off[c] .. d_out_off[c+1]).  zlib_header: 1 =
+ * zlib streams (2-byte header skipped and checked, as zlib.h:580), 0 = raw
+ * deflate, 2 = gzip member (header parsed, trailer ignored).  Stored, fixed
+ * and dynamic blocks are all decoded (the zlib/gzip checksums are not
+ * verified).  d_data must be 16-byte aligned (compressed words are fetched
+ * as aligned 16-byte loads; nothing outside a chunk's 16-byte-aligned span
+ * is read).
+ */
+gd_status_t gd_inflate(const uint8_t* d_data, const uint64_t* d_comp_off, const uint64_t* d_comp_len,
+                       const uint64_t* d_out_off, uint32_t n_chunks, int zlib_header, uint8_t* d_out,
+                       uint32_t* d_status, gd_stream_t stream);
+
+/* gd_inflate visiting chunks in the order d_order[0..n_chunks) (a
+ * permutation), e.g. longest first.  No reference counterpart: the
+ * reference maps chunk i to thread block i (zlib.h:1044-1057). */
+gd_status_t gd_inflate_ordered(const uint8_t* d_data, const uint64_t* d_comp_off, const uint64_t* d_comp_len,
+                               const uint64_t* d_out_off, uint32_t n_chunks, int zlib_header, uint8_t* d_out,
+                               uint32_t* d_status, const uint32_t* d_order, gd_stream_t stream);
+
+/*
+ * cuDF-compatible inflate interface (layouts of gpu_inflate_input_s and
+ * gpu_inflate_status_s, include/cudf_deflate.cuh:236-250).
+ * Replaces cudf::io::gpuinflate (include/cudf_deflate.cuh:1399-1407).
+ * parse_hdr = 1: inputs are gzip members (as cuDF); 0: raw deflate.
+ * status: 0 ok, 1 corrupt / overrun (cuDF's convention).
+ */
+typedef struct gd_inflate_input {
+    const void* srcDevice;
+    uint64_t srcSize;
+    void* dstDevice;
+    uint64_t dstSize;
+} gd_inflate_input;
+
+typedef struct gd_inflate_status {
+    uint64_t bytes_written;
+    uint32_t status;
+    uint32_t reserved;
+} gd_inflate_status;
+
+gd_status_t gd_gpuinflate(const gd_inflate_input* d_inputs, gd_inflate_status* d_outputs, int count,
+                          int parse_hdr, gd_stream_t stream);
+
+/* Replaces cudf::io::gpu_copy_uncompressed_blocks (cudf_deflate.cuh:1409-1415). */
+gd_status_t gd_copy_uncompressed_blocks(const gd_inflate_input* d_inputs, int count, gd_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Host API (reference signatures; synchronous; output from malloc)
+ * ------------------------------------------------------------------------ */
+
+/* Release a buffer returned by a gd_*_decompress call. */
+void gd_free(void* p);
+
+/* brle::decompress_gpu (include/brle/brle.h:305-342).
+ * in: [u32 n_ptr][u64 ptr[n_ptr]][u64 total][data], chunk size 256 KiB. */
+gd_status_t gd_brle_decompress(const uint8_t* in, uint64_t in_n_bytes, uint8_t** out,
+                               uint64_t* out_n_bytes);
+
+/* rle_v1::decompress_gpu (include/rle_v1/rlev1.h:100-199) with the side files
+ * (col_len, blk_offset) passed in memory.  in: [u64 in_n_bytes][blocks]. */
+gd_status_t gd_rlev1_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* col_len,
+                                uint64_t col_n_bytes, const uint64_t* blk_off, uint64_t blk_n_bytes,
+                                uint32_t comp_col_len, uint32_t elem_bytes, uint64_t chunk_size,
+                                uint8_t** out, uint64_t* out_n_bytes);
+
+/* rlev2::decompress_gpu (include/rlev2/decoder_trans.h:615-681).
+ * blk_off[n_chunks] holds the decompressed size (encoder_trans.h:490-492). */
+gd_status_t gd_rlev2_decompress(const uint8_t* in, uint64_t in_n_bytes, uint64_t n_chunks,
+                                const uint64_t* blk_off, const uint64_t* col_len, uint32_t read_unit,
+                                uint64_t chunk_size, uint8_t** out, uint64_t* out_n_bytes);
+
+/* lzss::decompress_gpu (include/lzss/lzss_gpu2.h:2129-2314).  meta:
+ * [0] u64 chunk_size, [1] u64 blk_off[n+1], [2] u64 col_len[32n],
+ * [3] u8 col_map[32n].  Returns 0 on success, -1 on bad metadata (as the
+ * reference), or a positive gd_status_t. */
+int gd_lzss_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint8_t* const* meta,
+                       const uint64_t* meta_lens, uint64_t meta_num, uint8_t** out,
+                       uint64_t* out_n_bytes);
+
+/* deflate::decompress_gpu (include/zlib/zlib.h:966-1082): in = concatenated
+ * zlib streams padded to 8 bytes; col_len = padded stream lengths;
+ * blk_offset = [u64 total][u64 0][u64 cumulative offsets]; chunk_size =
+ * uniform uncompressed chunk size. */
+gd_status_t gd_deflate_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* col_len,
+                                  uint64_t col_n_bytes, const uint64_t* blk_offset, uint64_t blk_n_bytes,
+                                  uint64_t chunk_size, uint8_t** out, uint64_t* out_n_bytes);
+
+/* ------------------------------------------------------------------------
+ * Encoders and generators (host; produce the containers above)
+ * ------------------------------------------------------------------------ */
+
+uint64_t gd_brle_max_encoded_bytes(uint64_t n, uint64_t chunk_size);
+/* brle::compress_gpu (include/brle/brle.h:251-303). */
+uint64_t gd_brle_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* out);
+
+uint64_t gd_rlev1_max_encoded_bytes(uint64_t n, uint64_t chunk_size);
+/* rle_v1::compress_gpu (include/rle_v1/rlev1.h:25-97). */
+uint64_t gd_rlev1_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint32_t comp_col_len,
+                         uint32_t elem_bytes, uint8_t* data, uint64_t* blk_off, uint64_t* col_len);
+uint64_t gd_rlev1_encode_stream(const void* vals, uint64_t n, uint32_t elem_bytes, uint8_t* out,
+                                uint64_t cap);
+
+uint64_t gd_rlev2_max_encoded_bytes(uint64_t n, uint64_t chunk_size);
+/* rlev2::compress_gpu_transpose (include/rlev2/encoder_trans.h:428-537). */
+uint64_t gd_rlev2_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint32_t read_unit,
+                         uint8_t* data, uint64_t* blk_off, uint64_t* col_len);
+/* rlev2::block_encode on one stream (include/rlev2/encoder.h:795-969). */
+uint64_t gd_rlev2_encode_stream(const int64_t* vals, uint64_t n, uint8_t* out, uint64_t cap);
+
+uint64_t gd_lzss_max_encoded_bytes(uint64_t n, uint64_t chunk_size);
+/* lzss::compress_gpu (include/lzss/lzss_gpu2.h:1915-2127). */
+uint64_t gd_lzss_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* data,
+                        uint64_t* blk_off, uint64_t* col_len, uint8_t* col_map);
+/* lzss::compress_func on one stream (include/lzss/lzss_cpu.h:540-655). */
+uint64_t gd_lzss_encode_stream(const uint8_t* in, uint32_t n, uint8_t* out, uint64_t cap);
+
+uint64_t gd_deflate_max_encoded_bytes(const uint64_t* out_off, uint32_t n);
+/* zlib_chunk_compress (orig_compressor.py:44-126) with per-chunk sizes. */
+uint64_t gd_deflate_encode(const uint8_t* in, const uint64_t* out_off, uint32_t n, int level,
+                           const uint8_t* mode, int zlib_header, uint8_t* data, uint64_t* comp_off,
+                           uint64_t* comp_len);
+
+void gd_gen_rlev1_ints(uint64_t seed, uint64_t n, int32_t* out);
+void gd_gen_brle_bytes(uint64_t seed, uint64_t n, uint8_t* out);
+void gd_gen_rlev2_ints(uint64_t seed, uint64_t n, int64_t* out);
+void gd_gen_markov_copy(uint64_t seed, uint64_t n, uint32_t max_dist, uint8_t* out);
+int gd_gen_loguniform_sizes(uint64_t seed, uint32_t n, uint64_t lo, uint64_t hi, uint64_t total,
+                            uint64_t granule, uint64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GD_H_ */

@@ -1,0 +1,69 @@
+"""CPU oracle for the decode hot path -- TEST INFRASTRUCTURE ONLY.
+
+A plain-C restatement of the reference decoders (gd_oracle.c, built into
+liboracle.so by oracle/build.py) plus system zlib for Deflate.  Only tests/,
+__graft_entry__.smoke() and the CPU-baseline leg of bench.py use it, as the
+checker; the compression_b200 package never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+_L = None
+
+vp, u32, u64, i32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
+
+
+def lib():
+    global _L
+    if _L is None:
+        if not LIB_PATH.exists():
+            from . import build as _b  # noqa: F401  (oracle/build.py)
+            _b.build_oracle()
+        L = C.CDLL(str(LIB_PATH))
+        L.gdo_brle_decode.argtypes = [vp, vp, u32, u64, vp, u64]
+        L.gdo_rlev1_decode.argtypes = [vp, u64, vp, vp, u32, u64, u32, u32, vp, u64]
+        L.gdo_rlev2_decode.argtypes = [vp, u64, vp, vp, u32, u64, u32, vp, u64]
+        L.gdo_lzss_decode.argtypes = [vp, u64, vp, vp, vp, u32, u64, vp, u64]
+        L.gdo_inflate.argtypes = [vp, vp, vp, vp, u32, i32, vp]
+        for f in ("gdo_brle_decode", "gdo_rlev1_decode", "gdo_rlev2_decode", "gdo_lzss_decode", "gdo_inflate"):
+            getattr(L, f).restype = i32
+        L.gdo_version.restype = C.c_char_p
+        _L = L
+    return _L
+
+
+def _p(a):
+    return a.ctypes.data
+
+
+def decode(enc) -> tuple[int, np.ndarray]:
+    """Decode a compression_b200.codecs.Encoded container on the CPU.
+
+    Returns (status, output bytes)."""
+    L = lib()
+    m = enc.meta
+    out = np.zeros(max(enc.n_out, 1), dtype=np.uint8)
+    d = enc.data
+    if enc.codec == "brle":
+        rc = L.gdo_brle_decode(_p(d), _p(m["ptr"]), enc.n_chunks, enc.chunk_size, _p(out), enc.n_out)
+    elif enc.codec == "rlev1":
+        rc = L.gdo_rlev1_decode(_p(d), d.size, _p(m["blk_off"]), _p(m["col_len"]), enc.n_chunks, enc.chunk_size,
+                                enc.params["comp_col_len"], enc.params["elem_bytes"], _p(out), enc.n_out)
+    elif enc.codec == "rlev2":
+        rc = L.gdo_rlev2_decode(_p(d), d.size, _p(m["blk_off"]), _p(m["col_len"]), enc.n_chunks, enc.chunk_size,
+                                enc.params["read_unit"], _p(out), enc.n_out)
+    elif enc.codec == "lzss":
+        rc = L.gdo_lzss_decode(_p(d), d.size, _p(m["blk_off"]), _p(m["col_len"]), _p(m["col_map"]),
+                               enc.n_chunks, enc.chunk_size, _p(out), enc.n_out)
+    elif enc.codec == "deflate":
+        rc = L.gdo_inflate(_p(d), _p(m["comp_off"]), _p(m["comp_len"]), _p(m["out_off"]), enc.n_chunks,
+                           enc.params["zlib_header"], _p(out))
+    else:
+        raise ValueError(enc.codec)
+    return int(rc), out[: enc.n_out]

@@ -1,0 +1,158 @@
+"""GPU parity: every sm_100a decoder, called through the C ABI, against the
+CPU oracle on the same seeded inputs -- bit-exact, status OK -- plus
+truncated/corrupted streams that must yield an error status (never a fault
+or a hang: every device read and write is bounds checked)."""
+import numpy as np
+import pytest
+
+import compression_b200.codecs as cc
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu(enc, dev):
+    import torch
+    job = cc.DeviceJob(enc, dev)
+    job.launch()
+    torch.cuda.synchronize()
+    return job.status(), job.output()
+
+
+def _parity(enc, raw_bytes, dev):
+    rc, ref = oracle.decode(enc)
+    assert rc == 0 and np.array_equal(ref, raw_bytes)
+    st, out = _gpu(enc, dev)
+    assert (st == 0).all(), np.unique(st)
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("n", [1, 130, 256 * 1024, 256 * 1024 + 7, 5 * 256 * 1024 + 999])
+def test_brle(cuda, n):
+    raw = cc.gen_brle_bytes(n, n)
+    _parity(cc.brle_encode(raw), raw, cuda)
+
+
+def test_brle_patterns(cuda):
+    rng = np.random.default_rng(0)
+    for raw in [np.zeros(300000, np.uint8), np.arange(300000, dtype=np.uint8),
+                rng.integers(0, 3, 700000).astype(np.uint8),
+                np.repeat(rng.integers(0, 256, 3000), 200).astype(np.uint8)]:
+        _parity(cc.brle_encode(raw, 65536), raw, cuda)
+
+
+@pytest.mark.parametrize("eb,ccl", [(4, 128), (4, 16), (8, 64), (4, 256)])
+def test_rlev1(cuda, eb, ccl):
+    v = cc.gen_rlev1_ints(eb + ccl, 400000)
+    raw = v.astype(np.int64) if eb == 8 else v
+    enc = cc.rlev1_encode(raw, 32 * ccl * 8, ccl, eb)
+    _parity(enc, raw.view(np.uint8), cuda)
+
+
+def test_rlev1_config_chunk(cuda):
+    v = cc.gen_rlev1_ints(11, 3 * 32768 + 100)
+    _parity(cc.rlev1_encode(v, 128 * 1024, 128, 4), v.view(np.uint8), cuda)
+
+
+@pytest.mark.parametrize("ru", [1, 4, 32, 64])
+def test_rlev2(cuda, ru):
+    v = cc.gen_rlev2_ints(ru, 200000)
+    _parity(cc.rlev2_encode(v, 256 * ru * 4, ru), v.view(np.uint8), cuda)
+
+
+def test_rlev2_negative_and_wide(cuda):
+    rng = np.random.default_rng(1)
+    v = np.concatenate([rng.integers(-2**62, 2**62, 3000), -np.arange(3000), np.full(500, -7),
+                        rng.integers(0, 2**12, 3000) + (rng.random(3000) < 0.03) * 2**50]).astype(np.int64)
+    _parity(cc.rlev2_encode(v, 256 * 8 * 2, 8), v.view(np.uint8), cuda)
+
+
+@pytest.mark.parametrize("chunk", [128, 4096, 65536])
+def test_lzss(cuda, chunk):
+    raw = cc.gen_markov_copy(chunk, 5 * chunk, 4096)
+    _parity(cc.lzss_encode(raw, chunk), raw, cuda)
+
+
+def test_lzss_degenerate(cuda):
+    for raw in [np.zeros(8192, np.uint8), np.tile(np.arange(7, dtype=np.uint8), 2000)[:8192]]:
+        _parity(cc.lzss_encode(raw, 4096), raw, cuda)
+
+
+@pytest.mark.parametrize("zh", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_inflate(cuda, zh, mode):
+    raw = cc.gen_markov_copy(9 + mode, 600000, 32768)
+    oo = np.array([0, 1, 4097, 100000, 100000, 250000, 600000], dtype=np.uint64)
+    _parity(cc.deflate_encode(raw, oo, 6, np.full(6, mode, np.uint8), zh), raw, cuda)
+
+
+def test_inflate_many_uneven(cuda):
+    raw = cc.gen_markov_copy(21, 8 << 20, 32768)
+    sizes = cc.loguniform_sizes(22, 200, 4096, 1 << 20, raw.size)
+    oo = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    mode = (np.random.default_rng(3).random(200) < 0.05).astype(np.uint8)
+    _parity(cc.deflate_encode(raw, oo, 6, mode), raw, cuda)
+
+
+def test_host_api_matches(cuda):
+    raw = cc.gen_brle_bytes(5, 700000)
+    assert np.array_equal(cc.decode_host(cc.brle_encode(raw)), raw)
+    v = cc.gen_rlev1_ints(6, 100000)
+    assert np.array_equal(cc.decode_host(cc.rlev1_encode(v)), v.view(np.uint8))
+    v2 = cc.gen_rlev2_ints(7, 100000)
+    assert np.array_equal(cc.decode_host(cc.rlev2_encode(v2)), v2.view(np.uint8))
+    raw3 = cc.gen_markov_copy(8, 4 * 65536, 4096)
+    assert np.array_equal(cc.decode_host(cc.lzss_encode(raw3)), raw3)
+    raw4 = cc.gen_markov_copy(9, 5 * 131072 + 77, 32768)
+    oo = np.array([0, 131072, 262144, 393216, 524288, raw4.size], dtype=np.uint64)
+    assert np.array_equal(cc.decode_host(cc.deflate_encode(raw4, oo)), raw4)
+
+
+# ---------------------------------------------------------------------------
+# malformed inputs: error status, no fault, no hang
+# ---------------------------------------------------------------------------
+
+def _expect_error(enc, dev):
+    st, _ = _gpu(enc, dev)
+    assert (st != 0).any()
+
+
+def test_corrupt_brle(cuda):
+    raw = cc.gen_brle_bytes(3, 600000)
+    enc = cc.brle_encode(raw)
+    enc.data[5] = 255          # literal header: extra output bytes
+    _expect_error(enc, cuda)
+    enc = cc.brle_encode(raw)
+    enc.meta["ptr"][1] -= 1    # truncated chunk
+    _expect_error(enc, cuda)
+
+
+def test_corrupt_interleaved(cuda):
+    v = cc.gen_rlev1_ints(4, 70000)
+    enc = cc.rlev1_encode(v, 32 * 128 * 4, 128, 4)
+    enc.meta["col_len"][3] = 2  # truncated lane
+    _expect_error(enc, cuda)
+    v2 = cc.gen_rlev2_ints(5, 40000)
+    e2 = cc.rlev2_encode(v2, 256 * 32, 32)
+    e2.meta["col_len"][0] += 1000000  # beyond the block
+    _expect_error(e2, cuda)
+    raw = cc.gen_markov_copy(6, 4 * 4096, 4096)
+    e3 = cc.lzss_encode(raw, 4096)
+    e3.meta["col_map"][1] = e3.meta["col_map"][0]  # not a permutation
+    _expect_error(e3, cuda)
+    e4 = cc.lzss_encode(raw, 4096)
+    e4.data[:] = 0                                   # matches with offset 0
+    _expect_error(e4, cuda)
+
+
+def test_corrupt_inflate(cuda):
+    raw = cc.gen_markov_copy(7, 300000, 32768)
+    oo = np.array([0, 150000, 300000], dtype=np.uint64)
+    enc = cc.deflate_encode(raw, oo)
+    enc.meta["comp_len"][0] = 40   # truncated stream
+    enc.data[int(enc.meta["comp_off"][1]) + 5] ^= 0xFF  # flipped bits
+    _expect_error(enc, cuda)
+    rng = np.random.default_rng(0)
+    junk = cc.deflate_encode(raw, oo)
+    junk.data[:] = rng.integers(0, 256, junk.data.size).astype(np.uint8)
+    _expect_error(junk, cuda)

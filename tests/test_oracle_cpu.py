@@ -1,0 +1,92 @@
+"""CPU-side tests: encoders + oracle round trips, edge cases, corrupt inputs.
+
+The oracle (oracle/gd_oracle.c) is the checker for the GPU tests; here it is
+checked against the original input (every container round-trips) and, in
+test_golden.py, against outputs of the reference's own code."""
+import numpy as np
+import pytest
+
+import compression_b200.codecs as cc
+import oracle
+
+
+def _roundtrip(enc, raw_bytes):
+    rc, out = oracle.decode(enc)
+    assert rc == 0
+    assert np.array_equal(out, raw_bytes)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 129, 130, 131, 256 * 1024, 256 * 1024 + 7, 3 * 256 * 1024])
+def test_brle_roundtrip_sizes(n):
+    raw = cc.gen_brle_bytes(n, n)
+    _roundtrip(cc.brle_encode(raw), raw)
+
+
+def test_brle_patterns():
+    rng = np.random.default_rng(0)
+    for raw in [np.zeros(5000, np.uint8), np.arange(5000, dtype=np.uint8),
+                rng.integers(0, 3, 70000).astype(np.uint8), np.repeat(rng.integers(0, 256, 300), 200).astype(np.uint8)]:
+        _roundtrip(cc.brle_encode(raw, 4096), raw)
+
+
+@pytest.mark.parametrize("eb,ccl", [(4, 128), (4, 16), (8, 64), (4, 256)])
+def test_rlev1_roundtrip(eb, ccl):
+    v = cc.gen_rlev1_ints(eb + ccl, 70000)
+    raw = v.astype(np.int64) if eb == 8 else v
+    enc = cc.rlev1_encode(raw, 32 * ccl * 8, ccl, eb)
+    rc, out = oracle.decode(enc)
+    assert rc == 0 and np.array_equal(out, raw.view(np.uint8))
+
+
+def test_rlev1_edge_values():
+    raw = np.array([0, 0xFFFFFFFF, 5, 5, 5, 7, 9, 11, 13, 1, 2] * 2000, dtype=np.uint32)
+    enc = cc.rlev1_encode(raw, 32 * 128, 128, 4)
+    _roundtrip(enc, raw.view(np.uint8))
+
+
+@pytest.mark.parametrize("ru", [1, 4, 32, 64])
+def test_rlev2_roundtrip(ru):
+    v = cc.gen_rlev2_ints(ru, 40000)
+    enc = cc.rlev2_encode(v, 256 * ru * 4, ru)
+    _roundtrip(enc, v.view(np.uint8))
+
+
+def test_rlev2_negative_and_wide_values():
+    rng = np.random.default_rng(1)
+    v = np.concatenate([rng.integers(-2**62, 2**62, 3000), -np.arange(3000), np.full(500, -7),
+                        rng.integers(0, 2**12, 3000) + (rng.random(3000) < 0.03) * 2**50]).astype(np.int64)
+    enc = cc.rlev2_encode(v, 256 * 8 * 2, 8)
+    _roundtrip(enc, v.view(np.uint8))
+
+
+@pytest.mark.parametrize("chunk", [128, 4096, 65536])
+def test_lzss_roundtrip(chunk):
+    raw = cc.gen_markov_copy(chunk, 3 * chunk, 4096)
+    _roundtrip(cc.lzss_encode(raw, chunk), raw)
+
+
+def test_lzss_degenerate():
+    for raw in [np.zeros(8192, np.uint8), np.tile(np.arange(7, dtype=np.uint8), 2000)[:8192]]:
+        _roundtrip(cc.lzss_encode(raw, 4096), raw)
+
+
+def test_deflate_modes():
+    raw = cc.gen_markov_copy(9, 300000, 32768)
+    oo = np.array([0, 1, 4097, 100000, 100000, 300000], dtype=np.uint64)  # includes an empty chunk
+    for zh in (0, 1):
+        for m in (0, 1, 2):
+            enc = cc.deflate_encode(raw, oo, 6, np.full(5, m, np.uint8), zh)
+            _roundtrip(enc, raw)
+
+
+def test_oracle_rejects_corruption():
+    raw = cc.gen_brle_bytes(3, 300000)
+    enc = cc.brle_encode(raw)
+    enc.data[5] = 200  # a literal header claiming bytes that turn into extra output
+    rc, _ = oracle.decode(enc)
+    assert rc in (2, 3)
+    v = cc.gen_rlev2_ints(3, 20000)
+    e2 = cc.rlev2_encode(v, 256 * 32, 32)
+    e2.meta["col_len"][0] += 4
+    rc, _ = oracle.decode(e2)
+    assert rc != 0
