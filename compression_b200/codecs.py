@@ -264,12 +264,14 @@ class DeviceJob:
         return self.d_out[: self.enc.n_out].cpu().numpy()
 
 
+_PINNED_KEEP: list = []  # pinned tensors backing the numpy views below
+
+
 def _pinned_copy(a: np.ndarray) -> np.ndarray:
     import torch
     t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-    arr = t.numpy()
-    arr._keep = t  # noqa: keep the pinned tensor alive with the view  # type: ignore[attr-defined]
-    return arr
+    _PINNED_KEEP.append(t)
+    return t.numpy()
 
 
 def decode_host_pinned(enc: Encoded) -> np.ndarray:

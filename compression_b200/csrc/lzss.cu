@@ -48,8 +48,7 @@ __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restr
     if (len64 > 0x3fffffffull) err = ST_CORRUPT;
     const uint32_t q = col_map[32ull * chunk + lane];
     if (q >= 32) err = ST_CORRUPT;
-    // col_map must be a permutation
-    if (__ballot_sync(GD_FULL_MASK, true) != 0u) {
+    {  // col_map must be a permutation of the 32 columns
         uint32_t bits = 0;
 #pragma unroll
         for (int o = 0; o < 32; ++o) bits |= 1u << (__shfl_sync(GD_FULL_MASK, q, o) & 31u);
@@ -59,6 +58,7 @@ __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restr
     uint32_t tot = warp_incl_scan(nw);
     tot = __shfl_sync(GD_FULL_MASK, tot, 31);
     if (b1 < b0 || (uint64_t)tot * 4 > b1 - b0) err = ST_CORRUPT;
+    if ((reinterpret_cast<uintptr_t>(data + b0) & 3u) != 0) err = ST_CORRUPT;  // words are 4-byte loads
     if (__any_sync(GD_FULL_MASK, err != ST_OK)) {
         if (lane == 0) put_status(status, chunk, ST_CORRUPT);
         return;

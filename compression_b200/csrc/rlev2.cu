@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restr
     uint32_t tot = warp_incl_scan(nw);
     tot = __shfl_sync(GD_FULL_MASK, tot, 31);
     if (b1 < b0 || (uint64_t)tot * 4 > b1 - b0) err = ST_CORRUPT;
+    if ((reinterpret_cast<uintptr_t>(data + b0) & 3u) != 0) err = ST_CORRUPT;  // words are 4-byte loads
     if (__any_sync(GD_FULL_MASK, err != ST_OK)) {
         if (lane == 0) put_status(status, chunk, ST_CORRUPT);
         return;

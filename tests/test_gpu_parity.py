@@ -104,7 +104,7 @@ def test_host_api_matches(cuda):
     raw3 = cc.gen_markov_copy(8, 4 * 65536, 4096)
     assert np.array_equal(cc.decode_host(cc.lzss_encode(raw3)), raw3)
     raw4 = cc.gen_markov_copy(9, 5 * 131072 + 77, 32768)
-    oo = np.array([0, 131072, 262144, 393216, 524288, raw4.size], dtype=np.uint64)
+    oo = np.array([0, 131072, 262144, 393216, 524288, 655360, raw4.size], dtype=np.uint64)
     assert np.array_equal(cc.decode_host(cc.deflate_encode(raw4, oo)), raw4)
 
 
