@@ -27,8 +27,8 @@ SIGNATURES = {
     "gd_version": (C.c_char_p, []),
     "gd_status_string": (C.c_char_p, [i32]),
     "gd_brle_decode": (i32, [vp, vp, u32, u64, vp, u64, vp, vp]),
-    "gd_rlev1_decode": (i32, [vp, vp, vp, u32, u64, u32, u32, vp, u64, vp, vp]),
-    "gd_rlev2_decode": (i32, [vp, vp, vp, u32, u64, u32, vp, u64, vp, vp]),
+    "gd_rlev1_decode": (i32, [vp, vp, vp, u32, u64, u32, u32, vp, u64, u32, vp, vp]),
+    "gd_rlev2_decode": (i32, [vp, vp, vp, u32, u64, u32, vp, u64, u32, vp, vp]),
     "gd_lzss_decode": (i32, [vp, vp, vp, vp, u32, u64, vp, u64, vp, vp]),
     "gd_inflate": (i32, [vp, vp, vp, vp, u32, i32, vp, vp, vp]),
     "gd_inflate_ordered": (i32, [vp, vp, vp, vp, u32, i32, vp, vp, vp, vp]),

@@ -219,9 +219,8 @@ class DeviceJob:
         d = np.concatenate([enc.data, np.zeros(pad, dtype=np.uint8)])
         self.d_data = torch.from_numpy(d).to(self.dev)
         self.d_meta = {k: torch.from_numpy(np.ascontiguousarray(v)).to(self.dev) for k, v in enc.meta.items()}
-        if enc.codec in ("rlev1", "rlev2", "lzss"):
-            # the device API bounds the last block by blk_off[n]
-            pass
+        # bound on the longest lane stream (sizes the decoders' shared memory)
+        self.max_lane = int(enc.meta["col_len"].max()) if "col_len" in enc.meta and enc.n_chunks else 0
         out_n = enc.n_out
         if enc.codec == "lzss":
             out_n = enc.n_chunks * enc.chunk_size
@@ -242,11 +241,11 @@ class DeviceJob:
         elif e.codec == "rlev1":
             rc = L.gd_rlev1_decode(ptr(self.d_data), ptr(m["col_len"]), ptr(m["blk_off"]), e.n_chunks,
                                    e.chunk_size, e.params["comp_col_len"], e.params["elem_bytes"],
-                                   ptr(self.d_out), e.n_out, ptr(self.d_status), s)
+                                   ptr(self.d_out), e.n_out, self.max_lane, ptr(self.d_status), s)
         elif e.codec == "rlev2":
             rc = L.gd_rlev2_decode(ptr(self.d_data), ptr(m["col_len"]), ptr(m["blk_off"]), e.n_chunks,
                                    e.chunk_size, e.params["read_unit"], ptr(self.d_out), e.n_out,
-                                   ptr(self.d_status), s)
+                                   self.max_lane, ptr(self.d_status), s)
         elif e.codec == "lzss":
             rc = L.gd_lzss_decode(ptr(self.d_data), ptr(m["blk_off"]), ptr(m["col_len"]), ptr(m["col_map"]),
                                   e.n_chunks, e.chunk_size, ptr(self.d_out), self.out_n, ptr(self.d_status), s)

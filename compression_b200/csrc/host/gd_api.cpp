@@ -215,8 +215,10 @@ gd_status_t gd_rlev1_decompress(const uint8_t* in, uint64_t in_n_bytes, const ui
     cudaMemcpyAsync(d_data, data, data_n, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_cl, col_len, 8 * 32 * n, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_bo, blk_off, 8 * (n + 1), cudaMemcpyHostToDevice, s);
+    uint64_t mx = 0;
+    for (uint64_t i = 0; i < 32 * n; ++i) mx = col_len[i] > mx ? col_len[i] : mx;
     gd_status_t r = gd_rlev1_decode(d_data, d_cl, d_bo, (uint32_t)n, chunk_size, comp_col_len, elem_bytes, d_out,
-                                    total, d_st, s);
+                                    total, (uint32_t)(mx < 0xffffffffull ? mx : 0), d_st, s);
     if (r != GD_OK) return r;
     uint8_t* h = (uint8_t*)pinned().get(total ? total : 1);
     if (!h) return GD_ERR_NOMEM;
@@ -252,8 +254,10 @@ gd_status_t gd_rlev2_decompress(const uint8_t* in, uint64_t in_n_bytes, uint64_t
     cudaMemcpyAsync(d_data, in, in_n_bytes, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_cl, col_len, 8 * 32 * n_chunks, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_bo, bo.data(), 8 * (n_chunks + 1), cudaMemcpyHostToDevice, s);
-    gd_status_t r =
-        gd_rlev2_decode(d_data, d_cl, d_bo, (uint32_t)n_chunks, chunk_size, read_unit, d_out, total, d_st, s);
+    uint64_t mx = 0;
+    for (uint64_t i = 0; i < 32 * n_chunks; ++i) mx = col_len[i] > mx ? col_len[i] : mx;
+    gd_status_t r = gd_rlev2_decode(d_data, d_cl, d_bo, (uint32_t)n_chunks, chunk_size, read_unit, d_out, total,
+                                    (uint32_t)(mx < 0xffffffffull ? mx : 0), d_st, s);
     if (r != GD_OK) return r;
     uint8_t* h = (uint8_t*)pinned().get(total);
     if (!h) return GD_ERR_NOMEM;

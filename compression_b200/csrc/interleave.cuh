@@ -133,4 +133,44 @@ __device__ __forceinline__ void ring_refill(LaneRing& r, LaneWords& w, const Seg
     }
 }
 
+// Block-cooperative copy of `nlanes` adjacent lane streams (slots L0..) of
+// an interleaved block into shared memory: stream i goes to dst + i*cap.
+// For each row, the group's words are contiguous, so threads (row, slot)
+// read whole 32-byte sectors.  Also zeroes 16 bytes after every stream.
+// Must be called by every thread of the block; ends with __syncthreads().
+template <int NLANES>
+__device__ __forceinline__ void load_lane_streams(const SegTable& T, const uint32_t* s_len, const uint8_t* block,
+                                                  uint8_t* dst, uint32_t cap, uint32_t L0) {
+    const uint32_t tid = threadIdx.x;
+    uint32_t maxw = 0;
+#pragma unroll
+    for (int i = 0; i < NLANES; ++i) maxw = max(maxw, (s_len[L0 + i] + 3) >> 2);
+    const uint32_t sub = tid % NLANES;
+    const uint32_t l = L0 + sub;
+    const uint32_t nwl = (s_len[l] + 3) >> 2;
+    const uint32_t ltmask = (1u << l) - 1u;
+    uint32_t* d = reinterpret_cast<uint32_t*>(dst + sub * cap);
+    for (uint32_t k = tid / NLANES; k < maxw; k += blockDim.x / NLANES) {
+        if (k < nwl) {
+            uint32_t j = 0;
+#pragma unroll
+            for (uint32_t step = 16; step; step >>= 1)
+                if (j + step <= 31 && T.hi[j + step - 1] <= k) j += step;
+            const uint32_t lo = j ? T.hi[j - 1] : 0u;
+            const uint32_t off = T.base[j] + (k - lo) * 4u * (32u - j) + 4u * __popc(T.mask[j] & ltmask);
+            // asynchronous 4-byte global->shared copy: all of a thread's
+            // loads are in flight at once instead of one round trip each
+            const uint32_t sa = (uint32_t)__cvta_generic_to_shared(d + k);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(block + off) : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    if (tid < NLANES * 4) {
+        const uint32_t s2 = tid / 4;
+        const uint32_t w = ((s_len[L0 + s2] + 3) >> 2) + (tid & 3u);
+        reinterpret_cast<uint32_t*>(dst + s2 * cap)[w] = 0;
+    }
+    __syncthreads();
+}
+
 }  // namespace gd

@@ -2,7 +2,7 @@
 // decoder for sm_100a.  8-byte values.
 //
 // Grammar (restated from rlev2::decode_{short_repeat,direct,patched_base,
-// delta}, include/rlev2/decoder.h:28-188; the GPU decoder_warp,
+// delta}, include/rlev2/decoder.h:28-188; the reference GPU decoder_warp,
 // decoder_new.h:360-611, decodes the same bytes): the top two header bits
 // select SHORT_REPEAT, DIRECT, PATCHED_BASE or DELTA.  Lane t of a chunk owns
 // the values t*RU + k*32*RU + j, j < RU.  Corrections to the reference (the
@@ -10,24 +10,27 @@
 // the delta accumulation runs len-2 times (decoder.h:117-123 runs len), and
 // a PATCHED_BASE base with its top bit set is negative.
 //
-// Organisation as rlev1.cu: one warp per chunk, lane = lane stream, per-lane
-// shared-memory input rings fed through the segment table, one output row
-// (32 lanes x RU values) per round written with coalesced stores.  Each
-// iteration a lane emits one value, so the four sub-encodings stay in step
-// across the warp.  PATCHED_BASE patches are applied as the values stream
-// out: the patch list (which follows the values in the stream) is read
-// entry by entry straight from the block, so nothing is written back.
+// The reference decodes a chunk with one decoder warp whose lane t walks lane
+// stream t value by value, bit-serially, fed by a reader warp through spin
+// queues.  Here every lane stream gets a whole warp:
+//   * a block of 8 warps owns 8 adjacent lanes of one chunk; the block copies
+//     those 8 streams from the interleaved block into shared memory (row k of
+//     the 8 lanes is one contiguous 32-byte sector, located in O(1) through
+//     the chunk's segment table);
+//   * in each warp, lane 0 parses a run header and broadcasts it, then the 32
+//     lanes produce the run's values together: DIRECT / PATCHED_BASE values
+//     are unpacked independently (a 96-bit big-endian window per value),
+//     PATCHED_BASE patch entries are decoded one per lane and located with a
+//     warp prefix sum of their gaps, fixed-delta runs are closed form and
+//     variable-delta runs are a 64-bit warp prefix sum;
+//   * 32 consecutive values of a lane stream fall in at most two READ_UNIT
+//     slices, so each store instruction writes at most two contiguous spans.
 #include "interleave.cuh"
 
 namespace gd {
 namespace rlev2 {
 
-constexpr int WPB = 4;
-
-__host__ __device__ constexpr uint32_t stage_stride(uint32_t slice_bytes) { return ((slice_bytes + 15u) & ~15u) + 8u; }
-__host__ __device__ constexpr uint32_t warp_smem(uint32_t slice_bytes) {
-    return (uint32_t)sizeof(SegTable) + 32u * RING_STRIDE + 32u * stage_stride(slice_bytes);
-}
+constexpr int LANES_PER_BLOCK = 8;  // warps per block = lane streams per block
 
 __device__ __constant__ uint8_t W_DECODE[32] = {1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11, 12, 13, 14, 15, 16,
                                                 17, 18, 19, 20, 21, 22, 23, 24, 26, 28, 30, 32, 40, 48, 56, 64};
@@ -45,73 +48,79 @@ __device__ __forceinline__ uint32_t closest_fixed(uint32_t b) {
     return 64;
 }
 
-enum : uint32_t { M_HDR = 0, M_SR = 1, M_DIRECT = 2, M_PATCH = 3, M_DELTA = 4 };
+// Shared-memory bytes for one lane stream of `nv` values: the largest valid
+// stream (64-bit DIRECT runs of 1 value + headers) plus a 16-byte tail that
+// unaligned 96-bit reads may touch.
+__host__ __device__ constexpr uint32_t stream_cap(uint32_t nv) { return ((nv * 11u + 64u + 15u) & ~15u); }
 
-__global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restrict__ data,
-                                                         const uint64_t* __restrict__ col_len,
-                                                         const uint64_t* __restrict__ blk_off, uint32_t n_chunks,
-                                                         uint64_t chunk_size, uint32_t ru,
-                                                         uint8_t* __restrict__ out, uint64_t out_n,
-                                                         uint32_t* __restrict__ status) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
-    const uint32_t chunk = blockIdx.x * WPB + wid;
-    if (chunk >= n_chunks) return;
-    const uint32_t slice = ru * 8u;
-    const uint32_t sstride = stage_stride(slice);
-    uint8_t* wbase = smem + wid * warp_smem(slice);
-    SegTable* T_ = reinterpret_cast<SegTable*>(wbase);
-    uint8_t* ring = wbase + sizeof(SegTable);
-    uint8_t* stage = ring + 32 * RING_STRIDE;
+// Shared-memory bytes reserved for a lane stream of at most `n` bytes.
+__host__ __device__ constexpr uint32_t lane_cap(uint32_t n) { return ((n + 15u) & ~15u) + 16u; }
 
-    uint32_t err = ST_OK;
-    const uint64_t b0 = blk_off[chunk], b1 = blk_off[chunk + 1];
-    const uint64_t len64 = col_len[32ull * chunk + lane];
-    const uint32_t len = len64 > 0x3fffffffull ? 0u : (uint32_t)len64;
-    if (len64 > 0x3fffffffull) err = ST_CORRUPT;
-    const uint32_t nw = (len + 3) >> 2;
-    uint32_t tot = warp_incl_scan(nw);
-    tot = __shfl_sync(GD_FULL_MASK, tot, 31);
-    if (b1 < b0 || (uint64_t)tot * 4 > b1 - b0) err = ST_CORRUPT;
-    if ((reinterpret_cast<uintptr_t>(data + b0) & 3u) != 0) err = ST_CORRUPT;  // words are 4-byte loads
-    if (__any_sync(GD_FULL_MASK, err != ST_OK)) {
-        if (lane == 0) put_status(status, chunk, ST_CORRUPT);
-        return;
-    }
-    const uint8_t* block = data + b0;
-    seg_build(T_, nw);
-    LaneWords lw;
-    lw_init(lw, T_, nw);
-    LaneRing r{ring + lane * RING_STRIDE, 0, 0, len};
+// `w` bits (1..64) starting `bitpos` bits into buf, most significant first
+// (the bit order of readLongs, decoder.h:41-72).  buf is 4-byte aligned and
+// readable 12 bytes past bitpos/8 rounded down to 4.
+__device__ __forceinline__ uint64_t extract_msb(const uint8_t* buf, uint32_t bitpos, uint32_t w) {
+    const uint32_t a = bitpos >> 3;
+    const uint32_t* p = reinterpret_cast<const uint32_t*>(buf + (a & ~3u));
+    const uint32_t w0 = __byte_perm(p[0], 0, 0x0123), w1 = __byte_perm(p[1], 0, 0x0123),
+                   w2 = __byte_perm(p[2], 0, 0x0123);
+    const uint32_t s = ((a & 3u) << 3) + (bitpos & 7u);  // 0..31
+    const uint64_t hi = ((uint64_t)w0 << 32) | w1;
+    const uint64_t t = (hi << s) | (((uint64_t)w2 << s) >> 32);
+    return w >= 64 ? t : (t >> (64 - w));
+}
 
-    const uint64_t obase = (uint64_t)chunk * chunk_size;
-    const uint64_t want = out_n > obase ? min(chunk_size, out_n - obase) : 0;
-    const uint32_t rounds = (uint32_t)(chunk_size / 256u / ru);
-    const uint32_t row_bytes = 32u * slice;
-    uint64_t* my_stage = reinterpret_cast<uint64_t*>(stage + lane * sstride);
-    const bool aligned16 = ((reinterpret_cast<uintptr_t>(out + obase) & 15u) == 0) && (slice % 16 == 0);
+__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
+    const uint32_t lo = __shfl_sync(GD_FULL_MASK, (uint32_t)v, src);
+    const uint32_t hi = __shfl_sync(GD_FULL_MASK, (uint32_t)(v >> 32), src);
+    return ((uint64_t)hi << 32) | lo;
+}
 
-    // ---- lane state ----
-    uint32_t mode = M_HDR, rem = 0, idx = 0;
-    uint32_t fbw = 0, bits_left = 0, cur = 0;
-    uint64_t val = 0, base = 0, delta = 0;
-    bool dec_neg = false, dfixed = false;
-    // patched-base state
-    uint32_t pw = 0, cfb = 0, p_left = 0, p_bit = 0, p_start = 0, p_end = 0;
-    uint32_t p_next = 0xffffffffu;
-    uint64_t p_val = 0;
+// One parsed run header (filled by lane 0, then broadcast).
+struct Run {
+    uint32_t kind;   // 0 SR, 1 DIRECT, 2 PATCHED, 3 DELTA
+    uint32_t len;    // values
+    uint32_t fbw;    // packed width
+    uint32_t vbit;   // bit offset of the packed data in the stream
+    uint32_t next;   // byte offset of the next header
+    uint32_t pw, cfb, pll, pbit;  // patched base: patch width, entry width, entries, list bit offset
+    uint32_t flags;  // DELTA: bit0 fixed delta, bit1 subtract
+    uint32_t err;
+    uint64_t base, delta;
+};
 
-    auto rd_byte = [&](uint32_t& b) -> bool {
-        if (r.rd >= r.len) return false;
-        b = ring_byte(r, r.rd);
-        ++r.rd;
+__device__ __forceinline__ Run bcast(const Run& r) {
+    Run o;
+    o.kind = __shfl_sync(GD_FULL_MASK, r.kind, 0);
+    o.len = __shfl_sync(GD_FULL_MASK, r.len, 0);
+    o.fbw = __shfl_sync(GD_FULL_MASK, r.fbw, 0);
+    o.vbit = __shfl_sync(GD_FULL_MASK, r.vbit, 0);
+    o.next = __shfl_sync(GD_FULL_MASK, r.next, 0);
+    o.pw = __shfl_sync(GD_FULL_MASK, r.pw, 0);
+    o.cfb = __shfl_sync(GD_FULL_MASK, r.cfb, 0);
+    o.pll = __shfl_sync(GD_FULL_MASK, r.pll, 0);
+    o.pbit = __shfl_sync(GD_FULL_MASK, r.pbit, 0);
+    o.flags = __shfl_sync(GD_FULL_MASK, r.flags, 0);
+    o.err = __shfl_sync(GD_FULL_MASK, r.err, 0);
+    o.base = shfl64(r.base, 0);
+    o.delta = shfl64(r.delta, 0);
+    return o;
+}
+
+// Parse the run header at byte `pos` of stream s[0..len) (lane 0 only).
+__device__ Run parse_header(const uint8_t* s, uint32_t pos, uint32_t len) {
+    Run r{};
+    r.err = ST_OK;
+    auto byte = [&](uint32_t& b) -> bool {
+        if (pos >= len) return false;
+        b = s[pos++];
         return true;
     };
-    auto rd_uvarint = [&](uint64_t& v) -> bool {
+    auto uvarint = [&](uint64_t& v) -> bool {
         uint64_t acc = 0;
         uint32_t sh = 0, b;
         do {
-            if (!rd_byte(b)) return false;
+            if (!byte(b)) return false;
             if (sh < 64) acc |= (uint64_t)(b & 0x7fu) << sh;
             sh += 7;
             if (sh > 70) return false;
@@ -119,221 +128,204 @@ __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restr
         v = acc;
         return true;
     };
-    // next fb-bit MSB-first value of the current packed run (readLongs)
-    auto rd_bits = [&](uint32_t fb, uint64_t& v) -> bool {
-        uint64_t res = 0;
-        uint32_t need = fb;
-        while (need > bits_left) {
-            res = (bits_left ? (res << bits_left) : res) | (cur & ((1u << bits_left) - 1u));
-            need -= bits_left;
-            if (!rd_byte(cur)) return false;
-            bits_left = 8;
-        }
-        if (need) {
-            res = (res << need);
-            bits_left -= need;
-            res |= (cur >> bits_left) & ((1u << need) - 1u);
-        }
-        v = res;
-        return true;
-    };
-    // random-access byte q of this lane's stream, straight from the block
-    auto g_byte = [&](uint32_t q, uint32_t& b) -> bool {
-        if (q >= r.len) return false;
-        const uint32_t off = word_offset_at(T_, q >> 2) + (q & 3u);
-        b = block[off];
-        return true;
-    };
-    // decode the next patch entry (gap << pw | patch), cfb bits at p_bit
-    auto next_patch = [&]() -> bool {
-        if (p_left == 0) {
-            p_next = 0xffffffffu;
-            return true;
-        }
-        uint64_t e = 0;
-        uint32_t bit = p_bit, need = cfb;
-        while (need) {
-            uint32_t b;
-            if (!g_byte(p_start + (bit >> 3), b)) return false;
-            const uint32_t avail = 8u - (bit & 7u);
-            const uint32_t take = min(avail, need);
-            const uint32_t v = (b >> (avail - take)) & ((1u << take) - 1u);
-            e = (e << take) | v;
-            need -= take;
-            bit += take;
-        }
-        p_bit = bit;
-        --p_left;
-        const uint64_t pmask = (pw >= 64) ? ~0ull : ((1ull << pw) - 1ull);
-        const uint32_t gap = (uint32_t)(pw >= 64 ? 0ull : (e >> pw));
-        p_next = (p_next == 0xffffffffu ? 0u : p_next) + gap;
-        p_val = (e & pmask) << fbw;
-        return true;
-    };
-    // move the read position to byte `pos` (>= rd), discarding ring contents
-    auto skip_to = [&](uint32_t pos) {
-        if (pos <= r.fl) {
-            r.rd = pos;
-        } else {
-            r.rd = pos;
-            r.fl = pos & ~3u;
-            lw.k = r.fl >> 2;
-        }
-    };
-
-    for (uint32_t rnd = 0; rnd < rounds; ++rnd) {
-        uint32_t produced = 0;
-        for (;;) {
-            const bool act = (produced < ru) && (err == ST_OK);
-            const bool need = act && (r.fl - r.rd < (uint32_t)RING_LOW) && (lw.k < lw.nw);
-            if (__any_sync(GD_FULL_MASK, need)) ring_refill(r, lw, T_, block);
-            if (!__any_sync(GD_FULL_MASK, act)) break;
-            if (!act) continue;
-            if (mode == M_HDR) {
-                uint32_t first, b;
-                if (!rd_byte(first)) {
-                    err = ST_CORRUPT;
-                    continue;
-                }
-                const uint32_t enc = first >> 6;
-                if (enc == 0) {  // SHORT_REPEAT
-                    const uint32_t nb = ((first >> 3) & 7u) + 1u;
-                    uint64_t v = 0;
-                    for (uint32_t i = 0; i < nb && err == ST_OK; ++i) {
-                        if (!rd_byte(b)) err = ST_CORRUPT;
-                        v = (v << 8) | b;
-                    }
-                    val = v;
-                    rem = (first & 7u) + 3u;
-                    mode = M_SR;
-                } else {
-                    fbw = W_DECODE[(first >> 1) & 31u];
-                    if (!rd_byte(b)) {
-                        err = ST_CORRUPT;
-                        continue;
-                    }
-                    const uint32_t rl = (((first & 1u) << 8) | b) + 1u;
-                    rem = rl;
-                    idx = 0;
-                    bits_left = 0;
-                    if (enc == 1) {
-                        mode = M_DIRECT;
-                    } else if (enc == 2) {  // PATCHED_BASE
-                        uint32_t b3, b4;
-                        if (!rd_byte(b3) || !rd_byte(b4)) {
-                            err = ST_CORRUPT;
-                            continue;
-                        }
-                        const uint32_t bw = ((b3 >> 5) & 7u) + 1u;
-                        pw = W_DECODE[b3 & 31u];
-                        const uint32_t pgw = ((b4 >> 5) & 7u) + 1u;
-                        p_left = b4 & 31u;
-                        uint64_t bv = 0;
-                        for (uint32_t i = 0; i < bw && err == ST_OK; ++i) {
-                            if (!rd_byte(b)) err = ST_CORRUPT;
-                            bv = (bv << 8) | b;
-                        }
-                        const uint64_t msb = 1ull << (8 * bw - 1);
-                        base = (bv & msb) ? (uint64_t)(-(int64_t)(bv & ~msb)) : bv;
-                        cfb = closest_fixed(pw + pgw);
-                        // the patch list starts after ceil(rl*fbw/8) value bytes
-                        p_start = r.rd + (uint32_t)(((uint64_t)rl * fbw + 7) >> 3);
-                        p_end = p_start + (uint32_t)(((uint64_t)p_left * cfb + 7) >> 3);
-                        if (p_end > r.len) err = ST_CORRUPT;
-                        p_bit = 0;
-                        p_next = 0xffffffffu;
-                        if (err == ST_OK && !next_patch()) err = ST_CORRUPT;
-                        mode = M_PATCH;
-                    } else {  // DELTA
-                        uint64_t ub, zz;
-                        if (!rd_uvarint(ub) || !rd_uvarint(zz) || rl < 2) {
-                            err = ST_CORRUPT;
-                            continue;
-                        }
-                        base = ub;
-                        delta = (zz >> 1) ^ (0ull - (zz & 1ull));
-                        dec_neg = !((int64_t)delta > 0);
-                        dfixed = ((first >> 1) & 31u) == 0;
-                        mode = M_DELTA;
-                    }
-                }
-                if (err != ST_OK) continue;
-            }
-            // ---- emit one value ----
-            uint64_t v = 0;
-            if (mode == M_SR) {
-                v = val;
-            } else if (mode == M_DIRECT) {
-                if (!rd_bits(fbw, v)) err = ST_CORRUPT;
-            } else if (mode == M_PATCH) {
-                if (!rd_bits(fbw, v)) err = ST_CORRUPT;
-                // every patch entry whose accumulated gap lands here (entries
-                // that only carry a 255 gap have a zero patch)
-                while (idx == p_next && err == ST_OK) {
-                    v |= p_val;
-                    if (!next_patch()) err = ST_CORRUPT;
-                }
-                v += base;
-            } else {  // M_DELTA (decoder.h:106-131)
-                if (idx == 0) {
-                    v = base;
-                } else if (idx == 1) {
-                    v = base + delta;
-                } else if (dfixed) {
-                    v = val + delta;
-                } else {
-                    uint64_t d = 0;
-                    if (!rd_bits(fbw, d)) err = ST_CORRUPT;
-                    v = dec_neg ? val - d : val + d;
-                }
-                val = v;
-            }
-            if (err != ST_OK) continue;
-            my_stage[produced++] = v;
-            ++idx;
-            if (--rem == 0) {
-                if (mode == M_PATCH) {
-                    if (p_next != 0xffffffffu) err = ST_CORRUPT;  // patch beyond the run
-                    skip_to(p_end);
-                }
-                mode = M_HDR;
-            }
-        }
-        __syncwarp();
-        const uint64_t roff = (uint64_t)rnd * row_bytes;
-        if (roff < want) {
-            const uint32_t n = (uint32_t)min((uint64_t)row_bytes, want - roff);
-            uint8_t* dst = out + obase + roff;
-            if (aligned16) {
-                const uint32_t nq = n >> 4;
-                for (uint32_t i = lane; i < nq; i += 32) {
-                    const uint32_t byte = 16 * i, sl = byte / slice, o = byte - sl * slice;
-                    const uint64_t* s8 = reinterpret_cast<const uint64_t*>(stage + sl * sstride + o);
-                    uint4 q;
-                    q.x = (uint32_t)s8[0];
-                    q.y = (uint32_t)(s8[0] >> 32);
-                    q.z = (uint32_t)s8[1];
-                    q.w = (uint32_t)(s8[1] >> 32);
-                    reinterpret_cast<uint4*>(dst)[i] = q;
-                }
-                for (uint32_t i = (nq << 4) + lane; i < n; i += 32) {
-                    const uint32_t sl = i / slice;
-                    dst[i] = stage[sl * sstride + (i - sl * slice)];
-                }
-            } else {
-                for (uint32_t i = lane; i < n; i += 32) {
-                    const uint32_t sl = i / slice;
-                    dst[i] = stage[sl * sstride + (i - sl * slice)];
-                }
-            }
-        }
-        __syncwarp();
-        if (__any_sync(GD_FULL_MASK, err != ST_OK)) break;
+    uint32_t first, b;
+    if (!byte(first)) {
+        r.err = ST_CORRUPT;
+        return r;
     }
-    // a lane must end exactly at the end of its stream
-    if (err == ST_OK && (mode != M_HDR || r.rd != r.len)) err = ST_CORRUPT;
-    err = __reduce_max_sync(GD_FULL_MASK, err);
-    if (lane == 0) put_status(status, chunk, err);
+    r.kind = first >> 6;
+    if (r.kind == 0) {  // SHORT_REPEAT, decoder.h:28-39
+        const uint32_t nb = ((first >> 3) & 7u) + 1u;
+        uint64_t v = 0;
+        for (uint32_t i = 0; i < nb; ++i) {
+            if (!byte(b)) {
+                r.err = ST_CORRUPT;
+                return r;
+            }
+            v = (v << 8) | b;
+        }
+        r.base = v;
+        r.len = (first & 7u) + 3u;
+        r.next = pos;
+        return r;
+    }
+    r.fbw = W_DECODE[(first >> 1) & 31u];
+    if (!byte(b)) {
+        r.err = ST_CORRUPT;
+        return r;
+    }
+    r.len = (((first & 1u) << 8) | b) + 1u;
+    if (r.kind == 1) {  // DIRECT, decoder.h:135-142
+        r.vbit = pos * 8;
+        r.next = pos + (uint32_t)(((uint64_t)r.len * r.fbw + 7) >> 3);
+    } else if (r.kind == 2) {  // PATCHED_BASE, decoder.h:144-188
+        uint32_t b3, b4;
+        if (!byte(b3) || !byte(b4)) {
+            r.err = ST_CORRUPT;
+            return r;
+        }
+        const uint32_t bw = ((b3 >> 5) & 7u) + 1u;
+        r.pw = W_DECODE[b3 & 31u];
+        const uint32_t pgw = ((b4 >> 5) & 7u) + 1u;
+        r.pll = b4 & 31u;
+        uint64_t bv = 0;
+        for (uint32_t i = 0; i < bw; ++i) {
+            if (!byte(b)) {
+                r.err = ST_CORRUPT;
+                return r;
+            }
+            bv = (bv << 8) | b;
+        }
+        const uint64_t msb = 1ull << (8 * bw - 1);
+        r.base = (bv & msb) ? (uint64_t)(-(int64_t)(bv & ~msb)) : bv;
+        r.cfb = closest_fixed(r.pw + pgw);
+        r.vbit = pos * 8;
+        const uint32_t pstart = pos + (uint32_t)(((uint64_t)r.len * r.fbw + 7) >> 3);
+        r.pbit = pstart * 8;
+        r.next = pstart + (uint32_t)(((uint64_t)r.pll * r.cfb + 7) >> 3);
+    } else {  // DELTA, decoder.h:93-133
+        uint64_t ub, zz;
+        if (!uvarint(ub) || !uvarint(zz) || r.len < 2) {
+            r.err = ST_CORRUPT;
+            return r;
+        }
+        r.base = ub;
+        r.delta = (zz >> 1) ^ (0ull - (zz & 1ull));
+        const bool fixed = ((first >> 1) & 31u) == 0;
+        r.flags = (fixed ? 1u : 0u) | (((int64_t)r.delta > 0) ? 0u : 2u);
+        r.vbit = pos * 8;
+        r.next = pos + (fixed ? 0u : (uint32_t)(((uint64_t)(r.len - 2) * r.fbw + 7) >> 3));
+    }
+    if (r.next > len) r.err = ST_CORRUPT;
+    return r;
+}
+
+__global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
+    const uint8_t* __restrict__ data, const uint64_t* __restrict__ col_len, const uint64_t* __restrict__ blk_off,
+    uint32_t n_chunks, uint64_t chunk_size, uint32_t ru, uint8_t* __restrict__ out, uint64_t out_n, uint32_t cap,
+    uint32_t* __restrict__ status) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ SegTable T_;
+    __shared__ uint32_t s_len[32];
+    __shared__ uint32_t s_bad;
+
+    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5, tid = threadIdx.x;
+    const uint32_t chunk = blockIdx.x / (32 / LANES_PER_BLOCK);
+    const uint32_t L0 = (blockIdx.x % (32 / LANES_PER_BLOCK)) * LANES_PER_BLOCK;
+    if (chunk >= n_chunks) return;  // block-uniform
+    const uint32_t nv = (uint32_t)(chunk_size / 256u);  // values per lane stream
+    uint8_t* sbuf = smem + wid * cap;
+    const uint64_t b0 = blk_off[chunk], b1 = blk_off[chunk + 1];
+    const uint8_t* block = data + b0;
+
+    // ---- segment table of the chunk (warp 0) ----
+    if (wid == 0) {
+        const uint64_t l64 = col_len[32ull * chunk + lane];
+        uint32_t bad = (l64 > cap - 16) ? 1u : 0u;
+        const uint32_t len = bad ? 0u : (uint32_t)l64;
+        const uint32_t nw = (len + 3) >> 2;
+        uint32_t tot = warp_incl_scan(nw);
+        tot = __shfl_sync(GD_FULL_MASK, tot, 31);
+        if (b1 < b0 || (uint64_t)tot * 4 > b1 - b0) bad = 1;
+        if ((reinterpret_cast<uintptr_t>(block) & 3u) != 0) bad = 1;
+        bad = __any_sync(GD_FULL_MASK, bad);
+        seg_build(&T_, nw);
+        s_len[lane] = len;
+        if (lane == 0) s_bad = bad;
+    }
+    __syncthreads();
+    if (s_bad) {
+        if (tid == 0 && status) atomicMax(status + chunk, (uint32_t)ST_CORRUPT);
+        return;
+    }
+
+    // ---- copy this block's 8 lane streams into shared memory ----
+    load_lane_streams<LANES_PER_BLOCK>(T_, s_len, block, smem, cap, L0);
+
+    // ---- decode lane stream L0 + wid with the whole warp ----
+    const uint32_t t = L0 + wid;
+    const uint32_t len = s_len[t];
+    const uint64_t obase = (uint64_t)chunk * chunk_size;
+    const uint64_t want_vals = out_n > obase ? min(chunk_size, out_n - obase) / 8 : 0;  // values of this chunk kept
+    uint64_t* outv = reinterpret_cast<uint64_t*>(out + obase);
+    uint32_t err = ST_OK, pos = 0, g = 0;
+    while (g < nv) {
+        Run r{};
+        if (lane == 0) r = parse_header(sbuf, pos, len);
+        r = bcast(r);
+        if (r.err != ST_OK) {
+            err = r.err;
+            break;
+        }
+        if (g + r.len > nv) {
+            err = ST_OVERRUN;
+            break;
+        }
+        // patch entries: lane p < pll holds entry p (cumulative index, patch bits)
+        uint32_t pidx = 0xffffffffu;
+        uint64_t pval = 0;
+        if (r.kind == 2) {
+            uint32_t gap = 0;
+            if (lane < r.pll) {
+                const uint64_t e = extract_msb(sbuf, r.pbit + lane * r.cfb, r.cfb);
+                gap = (r.pw >= 64) ? 0u : (uint32_t)(e >> r.pw);
+                const uint64_t pmask = (r.pw >= 64) ? ~0ull : ((1ull << r.pw) - 1ull);
+                pval = (e & pmask) << r.fbw;
+            }
+            const uint32_t cum = warp_incl_scan(gap);
+            if (lane < r.pll) {
+                pidx = cum;
+                if (cum >= r.len) err = ST_CORRUPT;
+            }
+            if (__any_sync(GD_FULL_MASK, err != ST_OK)) {
+                err = ST_CORRUPT;
+                break;
+            }
+        }
+        uint64_t carry = 0;  // DELTA: running sum of unpacked deltas
+        for (uint32_t i0 = 0; i0 < r.len; i0 += 32) {
+            const uint32_t i = i0 + lane;
+            const bool act = i < r.len;
+            uint64_t v = 0;
+            if (r.kind == 0) {
+                v = r.base;
+            } else if (r.kind == 1) {
+                if (act) v = extract_msb(sbuf, r.vbit + i * r.fbw, r.fbw);
+            } else if (r.kind == 2) {
+                if (act) v = extract_msb(sbuf, r.vbit + i * r.fbw, r.fbw);
+                for (uint32_t p = 0; p < r.pll; ++p) {
+                    const uint32_t pi = __shfl_sync(GD_FULL_MASK, pidx, p);
+                    const uint64_t pv = shfl64(pval, p);
+                    if (pi == i) v |= pv;
+                }
+                v += r.base;
+            } else if (r.flags & 1u) {  // fixed delta: v_i = base + i*delta
+                v = r.base + (uint64_t)i * r.delta;
+            } else {  // v_0 = base, v_1 = base+delta, v_i = v_{i-1} +- d_{i-2}
+                uint64_t d = 0;
+                if (act && i >= 2) d = extract_msb(sbuf, r.vbit + (i - 2) * r.fbw, r.fbw);
+                uint64_t sc = d;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint64_t n = shfl64(sc, (int)lane - o < 0 ? 0 : (int)lane - o);
+                    if (lane >= (uint32_t)o) sc += n;
+                }
+                const uint64_t acc = carry + sc;
+                carry += shfl64(sc, 31);
+                const uint64_t b1v = r.base + r.delta;
+                v = (i == 0) ? r.base : ((r.flags & 2u) ? b1v - acc : b1v + acc);
+            }
+            if (act) {
+                const uint32_t e = g + i;
+                const uint64_t oe = (uint64_t)t * ru + (uint64_t)(e / ru) * 32u * ru + (e % ru);
+                if (oe < want_vals) outv[oe] = v;
+            }
+        }
+        pos = r.next;
+        g += r.len;
+    }
+    if (err == ST_OK && pos != len) err = ST_CORRUPT;  // the stream must end with the last run
+    if (lane == 0 && err != ST_OK && status) atomicMax(status + chunk, err);
 }
 
 }  // namespace rlev2
@@ -341,19 +333,28 @@ __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restr
 
 extern "C" gd_status_t gd_rlev2_decode(const uint8_t* d_data, const uint64_t* d_col_len, const uint64_t* d_blk_off,
                                        uint32_t n_chunks, uint64_t chunk_size, uint32_t read_unit,
-                                       uint8_t* d_out, uint64_t out_n_bytes, uint32_t* d_status,
-                                       gd_stream_t stream) {
+                                       uint8_t* d_out, uint64_t out_n_bytes, uint32_t max_lane_bytes,
+                                       uint32_t* d_status, gd_stream_t stream) {
     if (n_chunks == 0) return GD_OK;
     if (!d_data || !d_col_len || !d_blk_off || !d_out) return GD_ERR_INVALID_ARG;
-    if (read_unit == 0 || read_unit > 64) return GD_ERR_UNSUPPORTED;
+    if (read_unit == 0) return GD_ERR_UNSUPPORTED;
     if (chunk_size == 0 || chunk_size % (256ull * read_unit) || chunk_size > (1ull << 31)) return GD_ERR_INVALID_ARG;
     if (out_n_bytes > chunk_size * (uint64_t)n_chunks || out_n_bytes <= chunk_size * (uint64_t)(n_chunks - 1))
         return GD_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(d_out) & 7u) != 0 || out_n_bytes % 8) return GD_ERR_INVALID_ARG;
     using namespace gd::rlev2;
-    const uint32_t smem = WPB * warp_smem(read_unit * 8u);
-    const uint32_t grid = (n_chunks + WPB - 1) / WPB;
+    const uint32_t nv = (uint32_t)(chunk_size / 256u);
+    // shared memory per lane stream: the caller's bound on the longest lane
+    // stream if given, else the longest a valid stream of nv values can be
+    const uint32_t cap = max_lane_bytes ? lane_cap(max_lane_bytes) : stream_cap(nv);
+    const uint32_t smem = LANES_PER_BLOCK * cap;
+    if (smem > 200 * 1024) return GD_ERR_UNSUPPORTED;  // lane streams must fit in shared memory
+    cudaStream_t s = (cudaStream_t)stream;
+    // per-chunk status is the max over the chunk's lane streams
+    if (d_status && cudaMemsetAsync(d_status, 0, 4ull * n_chunks, s) != cudaSuccess) return GD_ERR_CUDA;
     cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    decode_kernel<<<grid, WPB * 32, smem, (cudaStream_t)stream>>>(d_data, d_col_len, d_blk_off, n_chunks, chunk_size,
-                                                                   read_unit, d_out, out_n_bytes, d_status);
+    const uint32_t grid = n_chunks * (32 / LANES_PER_BLOCK);
+    decode_kernel<<<grid, LANES_PER_BLOCK * 32, smem, s>>>(d_data, d_col_len, d_blk_off, n_chunks, chunk_size,
+                                                           read_unit, d_out, out_n_bytes, cap, d_status);
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
 }

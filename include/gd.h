@@ -70,22 +70,26 @@ gd_status_t gd_brle_decode(const uint8_t* d_data, const uint64_t* d_ptr, uint32_
  * d_data: compressed blocks (the container after its 8-byte size header);
  * d_col_len[32*n_chunks]: per-lane stream bytes; d_blk_off[n_chunks+1]:
  * block start offsets.  elem_bytes 4 or 8; comp_col_len = COMP_COL_LEN.
+ * max_lane_bytes: an upper bound on col_len (sizes the shared-memory copy
+ * of each lane stream; 0 = the worst case for chunk_size).  A lane longer
+ * than the bound fails its chunk with GD_ERR_CORRUPT.
  */
 gd_status_t gd_rlev1_decode(const uint8_t* d_data, const uint64_t* d_col_len, const uint64_t* d_blk_off,
                             uint32_t n_chunks, uint64_t chunk_size, uint32_t comp_col_len,
                             uint32_t elem_bytes, uint8_t* d_out, uint64_t out_n_bytes,
-                            uint32_t* d_status, gd_stream_t stream);
+                            uint32_t max_lane_bytes, uint32_t* d_status, gd_stream_t stream);
 
 /*
  * RLE v2, 32-lane transposed container (8-byte values).
  * Replaces rlev2::inflate / rlev2::decompress_gpu<READ_UNIT,...>
  * (include/rlev2/decoder_new.h:618-657, include/rlev2/decoder_trans.h:615-681).
- * read_unit = READ_UNIT (values per lane slice).
+ * read_unit = READ_UNIT (values per lane slice); max_lane_bytes as for
+ * gd_rlev1_decode.
  */
 gd_status_t gd_rlev2_decode(const uint8_t* d_data, const uint64_t* d_col_len, const uint64_t* d_blk_off,
                             uint32_t n_chunks, uint64_t chunk_size, uint32_t read_unit,
-                            uint8_t* d_out, uint64_t out_n_bytes, uint32_t* d_status,
-                            gd_stream_t stream);
+                            uint8_t* d_out, uint64_t out_n_bytes, uint32_t max_lane_bytes,
+                            uint32_t* d_status, gd_stream_t stream);
 
 /*
  * LZSS, 32-column interleaved container.

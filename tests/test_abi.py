@@ -29,7 +29,7 @@ def test_device_api_rejects_bad_arguments_without_gpu():
     # argument validation happens before any CUDA call
     L = _lib.lib()
     assert L.gd_brle_decode(None, None, 1, 256 * 1024, None, 10, None, None) == 1
-    assert L.gd_rlev1_decode(1, 1, 1, 1, 1000, 128, 4, 1, 1000, None, None) == 1  # chunk % (32*128)
-    assert L.gd_rlev2_decode(1, 1, 1, 1, 256 * 1024, 0, 1, 10, None, None) == 5
+    assert L.gd_rlev1_decode(1, 1, 1, 1, 1000, 128, 4, 1, 1000, 0, None, None) == 1  # chunk % (32*128)
+    assert L.gd_rlev2_decode(1, 1, 1, 1, 256 * 1024, 0, 1, 10, 0, None, None) == 5
     assert L.gd_lzss_decode(1, 1, 1, 1, 2, 65536, 16, 1000, None, None) == 1  # out != n*chunk
     assert L.gd_inflate(3, 1, 1, 1, 1, 1, 1, None, None) == 1  # unaligned data
