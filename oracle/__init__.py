@@ -33,6 +33,10 @@ def lib():
         L.gdo_inflate.argtypes = [vp, vp, vp, vp, u32, i32, vp]
         for f in ("gdo_brle_decode", "gdo_rlev1_decode", "gdo_rlev2_decode", "gdo_lzss_decode", "gdo_inflate"):
             getattr(L, f).restype = i32
+        L.gdo_rlev2_decode_stream.argtypes = [vp, u64, vp, u64]
+        L.gdo_lzss_decode_stream.argtypes = [vp, u64, vp, u64]
+        L.gdo_rlev2_decode_stream.restype = i32
+        L.gdo_lzss_decode_stream.restype = i32
         L.gdo_version.restype = C.c_char_p
         _L = L
     return _L
@@ -67,3 +71,15 @@ def decode(enc) -> tuple[int, np.ndarray]:
     else:
         raise ValueError(enc.codec)
     return int(rc), out[: enc.n_out]
+
+
+def rlev2_decode_stream(stream: np.ndarray, n_vals: int) -> tuple[int, np.ndarray]:
+    s = np.ascontiguousarray(stream, dtype=np.uint8)
+    out = np.zeros(n_vals, dtype=np.int64)
+    return int(lib().gdo_rlev2_decode_stream(_p(s), s.size, _p(out), n_vals)), out
+
+
+def lzss_decode_stream(stream: np.ndarray, n_out: int) -> tuple[int, np.ndarray]:
+    s = np.ascontiguousarray(stream, dtype=np.uint8)
+    out = np.zeros(n_out, dtype=np.uint8)
+    return int(lib().gdo_lzss_decode_stream(_p(s), s.size, _p(out), n_out)), out

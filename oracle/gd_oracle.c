@@ -581,3 +581,16 @@ int gdo_inflate(const uint8_t* data, const uint64_t* comp_off, const uint64_t* c
 
 /* Version tag so tests can check they loaded this file's build. */
 const char* gdo_version(void) { return "gd-oracle-1"; }
+
+/* Single-stream entry points (the per-lane / per-column grammars above), for
+ * checking against the reference's contiguous codecs. */
+int gdo_rlev2_decode_stream(const uint8_t* s, uint64_t len, int64_t* vals, uint64_t n_vals) {
+    uint64_t got = 0;
+    int rc = rlev2_decode_lane(s, len, vals, n_vals, &got);
+    if (rc == GDO_OK && got != n_vals) rc = GDO_CORRUPT;
+    return rc;
+}
+
+int gdo_lzss_decode_stream(const uint8_t* s, uint64_t len, uint8_t* out, uint64_t n_out) {
+    return lzss_decode_column(s, len, out, n_out);
+}

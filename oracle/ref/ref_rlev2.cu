@@ -1,0 +1,52 @@
+// ref_rlev2 -- runs the reference's own contiguous RLE v2 codec
+// (include/rlev2/encoder.h block_encode, include/rlev2/decoder.h
+// block_decode; HEAD side of the unresolved merge, patch mask widened to 64
+// bits -- see oracle/ref/Makefile) on one stream of int64 values.  The
+// transposed container applies the same per-lane encoder to each lane's
+// values (encoder_trans.h:9-289).  Oracle tooling only.
+//   ref_rlev2 encode <int64 raw> <stream>           block_encode, one chunk (<= 4096 values)
+//   ref_rlev2 decode <stream> <n_values> <int64 raw> block_decode
+#include <common.h>
+#include <rlev2/encoder.h>
+#include <rlev2/decoder.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+static std::vector<uint8_t> slurp(const char* p) {
+    FILE* f = fopen(p, "rb");
+    if (!f) exit(2);
+    std::vector<uint8_t> v;
+    uint8_t buf[1 << 16];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof buf, f)) > 0) v.insert(v.end(), buf, buf + n);
+    fclose(f);
+    return v;
+}
+static void spit(const char* p, const void* d, size_t n) {
+    FILE* f = fopen(p, "wb");
+    if (!f || fwrite(d, 1, n, f) != n) exit(3);
+    fclose(f);
+}
+
+int main(int argc, char** argv) {
+    if (argc < 4) return 1;
+    std::vector<uint8_t> in = slurp(argv[2]);
+    if (!strcmp(argv[1], "encode")) {
+        if (in.size() > CHUNK_SIZE) return 4;
+        std::vector<uint8_t> out(OUTPUT_CHUNK_SIZE * 2, 0);
+        uint64_t len = 0;
+        rlev2::block_encode(0, reinterpret_cast<int64_t*>(in.data()), in.size(), out.data(), &len);
+        spit(argv[3], out.data(), len);
+    } else {
+        const uint64_t nv = strtoull(argv[3], nullptr, 10);
+        // decode_delta writes two values past a run (decoder.h:117-123): slack
+        std::vector<int64_t> out(CHUNK_SIZE / 8 + 16, 0);
+        uint64_t off[2] = {0, in.size()};
+        rlev2::block_decode(0, in.data(), off, out.data());
+        spit(argv[4], out.data(), nv * 8);
+    }
+    return 0;
+}

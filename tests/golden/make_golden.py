@@ -1,0 +1,102 @@
+"""Regenerate the golden fixtures from the reference's own codecs.
+
+    python oracle/build.py --ref          # builds oracle/_ref/ref_{brle,lzss,rlev2}
+    python tests/golden/make_golden.py    # writes tests/golden/*.npz
+
+Inputs come from the seeded generators (compression_b200.codecs) and a few
+hand-picked patterns.  For each input the reference's own encoder output and
+the reference's own decoder output are stored, so the tests can check (a) the
+library's encoders reproduce the reference bytes exactly and (b) the oracle
+and the GPU decoders recover the input from the reference's streams.
+Deflate fixtures come from Python's zlib, the producer the reference's
+container is written with (orig_compressor.py:87).
+"""
+from __future__ import annotations
+
+import subprocess
+import sys
+import tempfile
+import zlib
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+import compression_b200.codecs as cc  # noqa: E402
+
+REF = ROOT / "oracle" / "_ref"
+OUT = Path(__file__).resolve().parent
+
+
+def run(*args):
+    subprocess.run([str(a) for a in args], check=True, stdout=subprocess.DEVNULL)
+
+
+def main():
+    tmp = Path(tempfile.mkdtemp())
+    rng = np.random.default_rng(20261203)
+
+    # ---- byte-RLE containers (brle.h) ----
+    cases = [cc.gen_brle_bytes(1, 3 * 262144 + 777), cc.gen_brle_bytes(2, 100),
+             np.zeros(5000, np.uint8), np.arange(70000, dtype=np.uint8),
+             rng.integers(0, 3, 300000).astype(np.uint8),
+             np.repeat(rng.integers(0, 256, 2000), rng.integers(1, 300, 2000)).astype(np.uint8)]
+    bz = {}
+    for i, raw in enumerate(cases):
+        raw.tofile(tmp / "in")
+        run(REF / "ref_brle", "encode", tmp / "in", tmp / "enc")
+        run(REF / "ref_brle", "decode", tmp / "enc", tmp / "dec")
+        bz[f"raw{i}"] = raw
+        bz[f"enc{i}"] = np.fromfile(tmp / "enc", np.uint8)
+        bz[f"dec{i}"] = np.fromfile(tmp / "dec", np.uint8)
+    np.savez_compressed(OUT / "brle_golden.npz", **bz)
+
+    # ---- LZSS column streams (lzss_cpu.h compress_func / decompress_func) ----
+    lz = {}
+    big = cc.gen_markov_copy(3, 64 * 1024, 4096)
+    cols = []
+    for q in (0, 7, 31):  # the 2 KiB columns of a 64 KiB chunk, as the container stripes them
+        cols.append(np.concatenate([big[128 * k + 4 * q: 128 * k + 4 * q + 4] for k in range(512)]))
+    cols += [cc.gen_markov_copy(4, 4096, 4096), np.zeros(2048, np.uint8),
+             np.tile(np.arange(7, dtype=np.uint8), 300)[:2048], rng.integers(0, 256, 1024).astype(np.uint8)]
+    for i, col in enumerate(cols):
+        col.tofile(tmp / "c")
+        run(REF / "ref_lzss", "encode", tmp / "c", tmp / "cs")
+        run(REF / "ref_lzss", "decode", tmp / "cs", col.size, tmp / "cd")
+        lz[f"raw{i}"] = col
+        lz[f"enc{i}"] = np.fromfile(tmp / "cs", np.uint8)
+        lz[f"dec{i}"] = np.fromfile(tmp / "cd", np.uint8)
+    np.savez_compressed(OUT / "lzss_golden.npz", **lz)
+
+    # ---- RLE v2 lane streams (encoder.h block_encode / decoder.h block_decode) ----
+    rv = {}
+    v = cc.gen_rlev2_ints(5, 32 * 1024)
+    lanes = [v[t * 32 + np.concatenate([np.arange(k * 1024, k * 1024 + 32) for k in range(32)])] for t in (0, 5, 31)]
+    lanes += [np.arange(1024, dtype=np.int64) * 3 + 11, np.full(700, 42, np.int64),
+              rng.integers(0, 2 ** 12, 1024).astype(np.int64) + (rng.random(1024) < 0.02) * (1 << 40),
+              np.cumsum(rng.integers(1, 1000, 1024)).astype(np.int64) + 1600000000000,
+              rng.integers(0, 2 ** 17, 1024).astype(np.int64)]
+    for i, lane in enumerate(lanes):
+        lane = lane.astype(np.int64)
+        lane.tofile(tmp / "v")
+        run(REF / "ref_rlev2", "encode", tmp / "v", tmp / "vs")
+        run(REF / "ref_rlev2", "decode", tmp / "vs", lane.size, tmp / "vd")
+        rv[f"raw{i}"] = lane
+        rv[f"enc{i}"] = np.fromfile(tmp / "vs", np.uint8)
+        rv[f"dec{i}"] = np.fromfile(tmp / "vd", np.int64)
+    np.savez_compressed(OUT / "rlev2_golden.npz", **rv)
+
+    # ---- Deflate chunks (Python zlib, level 6 / 9 as orig_compressor.py) ----
+    dz = {}
+    raw = cc.gen_markov_copy(6, 300000, 32768)
+    for i, (a, b, lvl) in enumerate([(0, 4096, 6), (4096, 150000, 6), (150000, 300000, 9), (0, 1000, 0)]):
+        dz[f"raw{i}"] = raw[a:b]
+        dz[f"enc{i}"] = np.frombuffer(zlib.compress(raw[a:b].tobytes(), lvl), np.uint8)
+        dz[f"lvl{i}"] = np.array([lvl])
+    np.savez_compressed(OUT / "deflate_golden.npz", **dz)
+    print("fixtures written to", OUT)
+
+
+if __name__ == "__main__":
+    main()

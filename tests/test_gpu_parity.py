@@ -156,3 +156,45 @@ def test_corrupt_inflate(cuda):
     junk = cc.deflate_encode(raw, oo)
     junk.data[:] = rng.integers(0, 256, junk.data.size).astype(np.uint8)
     _expect_error(junk, cuda)
+
+
+# ---------------------------------------------------------------------------
+# containers built from the reference's own encoder output (tests/golden)
+# ---------------------------------------------------------------------------
+
+def test_reference_streams_on_gpu(cuda):
+    from test_golden import _cases, interleave_streams
+    # brle: the reference's container as is
+    for raw, enc, _ in _cases("brle")[0]:
+        n_ptr = int(enc[:4].view(np.uint32)[0])
+        ptr = enc[4:4 + 8 * n_ptr].copy().view(np.uint64)
+        e = cc.Encoded("brle", enc[4 + 8 * n_ptr + 8:].copy(), raw.size, n_ptr - 1, 256 * 1024, {"ptr": ptr})
+        st, out = _gpu(e, cuda)
+        assert (st == 0).all() and np.array_equal(out, raw)
+    # LZSS: a 64 KiB chunk whose 32 columns are reference column streams
+    cases = [c for c in _cases("lzss")[0] if c[0].size == 2048]
+    cols = [cases[q % len(cases)] for q in range(32)]
+    lens = np.array([c[1].size for c in cols])
+    order = sorted(range(32), key=lambda q: (-lens[q], -q))  # rank: length desc, ties column desc
+    blk, cl = interleave_streams([cols[q][1] for q in order])
+    raw = np.zeros(65536, np.uint8)
+    for q in range(32):
+        raw.reshape(512, 32, 4)[:, q, :] = cols[q][0].reshape(512, 4)
+    e = cc.Encoded("lzss", blk, raw.size, 1, 65536,
+                   {"blk_off": np.array([0, blk.size], np.uint64), "col_len": cl,
+                    "col_map": np.array(order, np.uint8)})
+    st, out = _gpu(e, cuda)
+    assert (st == 0).all() and np.array_equal(out, raw)
+    # RLE v2: a 256 KiB chunk (READ_UNIT 32) whose lanes are reference streams
+    cases = [c for c in _cases("rlev2")[0] if c[0].size == 1024]
+    lanes = [cases[t % len(cases)] for t in range(32)]
+    blk, cl = interleave_streams([l[1] for l in lanes])
+    vals = np.zeros(32768, np.int64)
+    for t in range(32):
+        v = lanes[t][0]
+        for k in range(32):
+            vals[t * 32 + k * 1024: t * 32 + k * 1024 + 32] = v[k * 32:(k + 1) * 32]
+    e = cc.Encoded("rlev2", blk, vals.nbytes, 1, 262144,
+                   {"blk_off": np.array([0, blk.size], np.uint64), "col_len": cl}, {"read_unit": 32})
+    st, out = _gpu(e, cuda)
+    assert (st == 0).all() and np.array_equal(out, vals.view(np.uint8))
