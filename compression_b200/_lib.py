@@ -34,6 +34,8 @@ SIGNATURES = {
     "gd_inflate_ordered": (i32, [vp, vp, vp, vp, u32, i32, vp, vp, vp, vp]),
     "gd_gpuinflate": (i32, [vp, vp, i32, i32, vp]),
     "gd_copy_uncompressed_blocks": (i32, [vp, i32, vp]),
+    "gd_batch_decode": (i32, [vp, u32, vp, i32, u32, u32, vp, vp, vp, vp]),
+    "gd_batch_warps": (u32, [u32, u32]),
     "gd_free": (None, [vp]),
     "gd_brle_decompress": (i32, [vp, u64, C.POINTER(vp), u64p]),
     "gd_rlev1_decompress": (i32, [vp, u64, vp, u64, vp, u64, u32, u32, u64, C.POINTER(vp), u64p]),

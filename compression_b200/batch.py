@@ -1,0 +1,296 @@
+"""Batched mixed-codec decoding: batch construction, task tables, launches.
+
+A batch is a list of items, each one column segment encoded with one codec
+(its own container).  The planner turns items into warp-sized tasks
+(gd_task, include/gd.h): one per brle chunk, per RLE v1 / RLE v2 lane stream,
+per LZSS chunk and per Deflate stream, lays every payload and every output
+into device arenas, and launches gd_batch_decode.  The task order given to
+the launch is the scheduling decision: identity (static mapping task i ->
+warp i mod W, the fallback), or longest-predicted-first through the dynamic
+work queue (LPT list scheduling) with costs from the learned model
+(compression_b200.costmodel) or from any other estimate.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import codecs as cc
+from ._lib import lib
+
+CODECS = ["brle", "rlev1", "rlev2", "lzss", "deflate"]
+CODEC_ID = {c: i for i, c in enumerate(CODECS)}
+# size granule of an item per codec: RLE v1 chunks are multiples of 32 lanes x
+# COMP_COL_LEN (128 B); RLE v2 of 256 x READ_UNIT (32); LZSS of 128 B
+GRANULE = {"brle": 16, "rlev1": 4096, "rlev2": 8192, "lzss": 128, "deflate": 16}
+DEFAULT_CHUNK = {"brle": 256 * 1024, "rlev1": 128 * 1024, "rlev2": 256 * 1024, "lzss": 64 * 1024}
+
+TASK_DTYPE = np.dtype([
+    ("codec", "<u4"), ("param", "<u4"), ("lane", "<u4"), ("reserved", "<u4"),
+    ("src", "<u8"), ("src_len", "<u8"), ("dst", "<u8"), ("dst_len", "<u8"),
+    ("chunk_size", "<u8"), ("col_len", "<u8"), ("col_map", "<u8")])
+assert TASK_DTYPE.itemsize == 72
+
+
+@dataclass
+class Item:
+    codec: str
+    raw: np.ndarray          # the decompressed bytes (uint8 view)
+    enc: cc.Encoded
+
+
+def _gen(codec: str, seed: int, nbytes: int) -> np.ndarray:
+    if codec == "brle":
+        return cc.gen_brle_bytes(seed, nbytes)
+    if codec == "rlev1":
+        return cc.gen_rlev1_ints(seed, nbytes // 4).view(np.uint8)
+    if codec == "rlev2":
+        return cc.gen_rlev2_ints(seed, nbytes // 8).view(np.uint8)
+    return cc.gen_markov_copy(seed, nbytes, 4096 if codec == "lzss" else 32768)
+
+
+def encode_item(codec: str, raw: np.ndarray, seed: int = 0) -> cc.Encoded:
+    n = raw.size
+    if codec == "brle":
+        return cc.brle_encode(raw, min(DEFAULT_CHUNK["brle"], max(16, n)))
+    if codec == "rlev1":
+        return cc.rlev1_encode(raw, min(DEFAULT_CHUNK["rlev1"], n), 128, 4)
+    if codec == "rlev2":
+        return cc.rlev2_encode(raw, min(DEFAULT_CHUNK["rlev2"], n), 32)
+    if codec == "lzss":
+        return cc.lzss_encode(raw, min(DEFAULT_CHUNK["lzss"], n))
+    # ~3% of Deflate streams use fixed or stored blocks
+    r = (seed * 2654435761 % 1000) / 1000.0
+    mode = np.array([1 if r < 0.015 else (2 if r < 0.03 else 0)], np.uint8)
+    return cc.deflate_encode(raw, np.array([0, n], np.uint64), 6, mode, 1)
+
+
+def make_mixed_batch(seed: int, n_items: int, total_bytes: int, lo: int = 4096, hi: int = 2 << 20,
+                     mix=(0.20, 0.20, 0.10, 0.25, 0.25)) -> list[Item]:
+    """Items with sizes log-uniform in [lo, hi] scaled to total_bytes, codecs
+    RLE v1 / RLE v2 / byte-RLE / LZSS / Deflate in the proportions `mix`."""
+    sizes = cc.loguniform_sizes(seed, n_items, lo, hi, total_bytes, 16)
+    rng = np.random.default_rng(seed)
+    order = ["rlev1", "rlev2", "brle", "lzss", "deflate"]
+    counts = np.floor(np.array(mix) * n_items).astype(int)
+    counts[-1] = n_items - counts[:-1].sum()
+    codecs = np.concatenate([[order[i]] * counts[i] for i in range(5)])
+    rng.shuffle(codecs)
+    items = []
+    for i, (codec, sz) in enumerate(zip(codecs, sizes)):
+        g = GRANULE[codec]
+        n = max(g, int(sz) // g * g)
+        raw = _gen(codec, seed * 100003 + i, n)
+        items.append(Item(codec, raw, encode_item(codec, raw, seed * 7 + i)))
+    return items
+
+
+@dataclass
+class Plan:
+    """Device-resident batch: arenas, task table, per-item output views."""
+    items: list
+    tasks: np.ndarray                # TASK_DTYPE records (host copy, device addresses)
+    task_item: np.ndarray            # item index of every task
+    d_tasks: object = None
+    d_in: object = None
+    d_meta: object = None
+    d_out: object = None
+    out_off: np.ndarray = None       # byte offset of each item's output in d_out
+    out_len: np.ndarray = None
+    max_lane: int = 0
+    d_status: object = None
+    d_timing: object = None
+    d_counter: object = None
+    extra: dict = field(default_factory=dict)
+
+
+def _align(x: int, a: int = 256) -> int:
+    return (x + a - 1) // a * a
+
+
+def build_plan(items: list[Item], device="cuda") -> Plan:
+    import torch
+    dev = torch.device(device)
+    # ---- input arena (payloads) and metadata arena (col_len / col_map) ----
+    in_off, pos = [], 0
+    for it in items:
+        in_off.append(pos)
+        pos = _align(pos + it.enc.data.size + 16)
+    h_in = np.zeros(max(pos, 256), np.uint8)
+    for it, o in zip(items, in_off):
+        h_in[o:o + it.enc.data.size] = it.enc.data
+    meta_off, mpos = [], 0
+    for it in items:
+        meta_off.append(mpos)
+        if "col_len" in it.enc.meta:
+            mpos = _align(mpos + it.enc.meta["col_len"].nbytes + it.enc.meta.get("col_map", np.zeros(0)).nbytes)
+    h_meta = np.zeros(max(mpos, 256), np.uint8)
+    for it, o in zip(items, meta_off):
+        if "col_len" in it.enc.meta:
+            cl = it.enc.meta["col_len"].view(np.uint8)
+            h_meta[o:o + cl.size] = cl
+            if "col_map" in it.enc.meta:
+                cm = it.enc.meta["col_map"]
+                h_meta[o + cl.size:o + cl.size + cm.size] = cm
+    # ---- output arena ----
+    out_off, out_len, opos = [], [], 0
+    for it in items:
+        e = it.enc
+        need = e.n_chunks * e.chunk_size if it.codec == "lzss" else e.n_out
+        out_off.append(opos)
+        out_len.append(e.n_out)
+        opos = _align(opos + need + 16)
+    d_in = torch.from_numpy(h_in).to(dev)
+    d_meta = torch.from_numpy(h_meta).to(dev)
+    d_out = torch.zeros(max(opos, 256), dtype=torch.uint8, device=dev)
+    bi, bm, bo = d_in.data_ptr(), d_meta.data_ptr(), d_out.data_ptr()
+    # ---- tasks ----
+    recs, titem, tchunk = [], [], []
+    max_lane = 0
+    for ii, (it, io, mo, oo) in enumerate(zip(items, in_off, meta_off, out_off)):
+        e, c = it.enc, it.codec
+        if c == "brle":
+            p = e.meta["ptr"]
+            for k in range(e.n_chunks):
+                recs.append((0, 0, 0, 0, bi + io + int(p[k]), int(p[k + 1] - p[k]), bo + oo + k * e.chunk_size,
+                             min(e.chunk_size, e.n_out - k * e.chunk_size), e.chunk_size, 0, 0))
+                titem.append(ii)
+                tchunk.append(k)
+        elif c in ("rlev1", "rlev2"):
+            bo_ = e.meta["blk_off"]
+            max_lane = max(max_lane, int(e.meta["col_len"].max()))
+            param = (4 << 16) | 32 if c == "rlev1" else e.params["read_unit"]
+            for k in range(e.n_chunks):
+                for t in range(32):
+                    recs.append((CODEC_ID[c], param, t, 0, bi + io + int(bo_[k]), int(bo_[k + 1] - bo_[k]),
+                                 bo + oo + k * e.chunk_size, min(e.chunk_size, e.n_out - k * e.chunk_size),
+                                 e.chunk_size, bm + mo + 8 * 32 * k, 0))
+                    titem.append(ii)
+                    tchunk.append(k)
+        elif c == "lzss":
+            bo_ = e.meta["blk_off"]
+            ncl = e.meta["col_len"].nbytes
+            for k in range(e.n_chunks):
+                recs.append((3, 0, 0, 0, bi + io + int(bo_[k]), int(bo_[k + 1] - bo_[k]), bo + oo + k * e.chunk_size,
+                             e.chunk_size, e.chunk_size, bm + mo + 8 * 32 * k, bm + mo + ncl + 32 * k))
+                titem.append(ii)
+                tchunk.append(k)
+        else:
+            recs.append((4, e.params["zlib_header"], 0, 0, bi + io + int(e.meta["comp_off"][0]),
+                         int(e.meta["comp_len"][0]), bo + oo, e.n_out, 0, 0, 0))
+            titem.append(ii)
+            tchunk.append(0)
+    tasks = np.array(recs, dtype=TASK_DTYPE)
+    d_tasks = torch.from_numpy(tasks.view(np.uint8).copy()).to(dev)
+    n = tasks.size
+    plan = Plan(items, tasks, np.array(titem, np.int64), d_tasks, d_in, d_meta, d_out, np.array(out_off),
+                np.array(out_len), max_lane)
+    plan.extra["task_chunk"] = np.array(tchunk, np.int64)
+    plan.d_status = torch.zeros(n, dtype=torch.int32, device=dev)
+    plan.d_timing = torch.zeros(2 * n, dtype=torch.int64, device=dev)
+    plan.d_counter = torch.zeros(4, dtype=torch.int32, device=dev)
+    return plan
+
+
+def launch(plan: Plan, order=None, dynamic: bool = True, timing: bool = True, blocks_per_sm: int = 0,
+           stream=None) -> None:
+    """Enqueue gd_batch_decode.  `order` (device int32 tensor or None) is the
+    task order: dynamic=True pops it through the work queue, False maps
+    order[i] to warp i mod W."""
+    import torch
+    s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+    rc = lib().gd_batch_decode(p(plan.d_tasks), plan.tasks.size, p(order), 1 if dynamic else 0, plan.max_lane,
+                               blocks_per_sm, p(plan.d_counter), p(plan.d_status),
+                               p(plan.d_timing) if timing else None, C.c_void_p(s))
+    cc.check(rc, "gd_batch_decode")
+
+
+def n_warps(plan: Plan, blocks_per_sm: int = 0) -> int:
+    return int(lib().gd_batch_warps(plan.max_lane, blocks_per_sm))
+
+
+def verify(plan: Plan) -> bool:
+    """Every task OK and every item's output equal to its raw column."""
+    st = plan.d_status.cpu().numpy()
+    if (st != 0).any():
+        return False
+    out = plan.d_out.cpu().numpy()
+    for it, o, n in zip(plan.items, plan.out_off, plan.out_len):
+        if not np.array_equal(out[o:o + n], it.raw):
+            return False
+    return True
+
+
+def task_durations_ns(plan: Plan) -> np.ndarray:
+    t = plan.d_timing.cpu().numpy().reshape(-1, 2)
+    return (t[:, 1] - t[:, 0]).astype(np.float64)
+
+
+def makespan_ms(plan: Plan, order=None, dynamic=True, reps: int = 3, blocks_per_sm: int = 0) -> float:
+    """Median CUDA-event time of the whole batch launch."""
+    import torch
+    times = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        launch(plan, order, dynamic, timing=False, blocks_per_sm=blocks_per_sm)
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    return float(np.median(times))
+
+
+# --------------------------------------------------------------------------
+# per-task header features (16) for the cost model
+# --------------------------------------------------------------------------
+
+N_FEATURES = 16
+
+
+def task_features(plan: Plan) -> np.ndarray:
+    """16 features per task from container metadata only (what a scheduler
+    knows before decoding):
+      0-4  codec one-hot (brle, RLE v1, RLE v2, LZSS, Deflate)
+      5    log2 compressed bytes the task reads (its lane stream for RLE)
+      6    log2 output bytes the task writes
+      7    compressed / output bytes
+      8-9  lane-stream length skew of the chunk: max/mean, std/mean (RLE, LZSS)
+      10   this lane's length / mean lane length (RLE)
+      11   log2 chunk (or stream) size
+      12   Deflate stream stored in the clear (compressed >= half its output)
+      13   log2 of compressed bytes per 64 KiB of output
+      14   log2 size of the whole item
+      15   constant 1"""
+    T = plan.tasks
+    F = np.zeros((T.size, N_FEATURES), np.float32)
+    chunk = plan.extra["task_chunk"]
+    for i, rec in enumerate(T):
+        it = plan.items[plan.task_item[i]]
+        c = int(rec["codec"])
+        F[i, c] = 1.0
+        src_len = float(rec["src_len"])
+        dst_len = float(rec["dst_len"])
+        skew_max = skew_std = share = 1.0
+        if c in (1, 2, 3):
+            ll = it.enc.meta["col_len"].reshape(-1, 32)[chunk[i]].astype(np.float64)
+            m = max(ll.mean(), 1.0)
+            skew_max, skew_std = ll.max() / m, ll.std() / m
+            if c in (1, 2):
+                src_len = float(ll[int(rec["lane"])])
+                share = src_len / m
+                dst_len = dst_len / 32.0
+        F[i, 5] = np.log2(src_len + 1.0)
+        F[i, 6] = np.log2(dst_len + 1.0)
+        F[i, 7] = src_len / max(dst_len, 1.0)
+        F[i, 8] = skew_max
+        F[i, 9] = skew_std
+        F[i, 10] = share
+        F[i, 11] = np.log2(float(rec["chunk_size"] or rec["dst_len"]) + 1.0)
+        F[i, 12] = 1.0 if (c == 4 and it.enc.comp_bytes > 0.5 * it.enc.n_out) else 0.0
+        F[i, 13] = np.log2(src_len / max(dst_len, 1.0) * 65536.0 + 1.0)
+        F[i, 14] = np.log2(float(it.enc.n_out) + 1.0)
+        F[i, 15] = 1.0
+    return F

@@ -1,0 +1,196 @@
+// batch.cu -- batched mixed-codec decoding: one persistent launch over a
+// list of warp-sized tasks of any codec, fed from a device work queue.
+//
+// No counterpart in the reference (its decoders are one launch per column
+// and codec).  A task is one brle chunk, one RLE v1 / RLE v2 lane stream,
+// one LZSS chunk or one Deflate stream; every codec has a warp-level decoder
+// (brle_warp.cuh, rlev1.cuh, rlev2.cuh, lzss.cuh, inflate.cuh), so a single
+// kernel can run them all.  Each warp repeatedly takes the next task either
+// from a global atomic counter over an order array (dynamic: with tasks
+// sorted longest-first this is LPT list scheduling) or by the static mapping
+// task i -> warp i mod W.  Per-task %globaltimer start/end stamps (optional)
+// are the measurements the learned cost model trains on.
+#include "brle_warp.cuh"
+#include "inflate.cuh"
+#include "lzss.cuh"
+#include "rlev1.cuh"
+#include "rlev2.cuh"
+
+namespace gd {
+namespace batch {
+
+constexpr int WPB = 4;  // warps per block
+
+__host__ __device__ constexpr uint32_t warp_smem_bytes(uint32_t max_lane) {
+    // union of the per-codec warp workspaces
+    uint32_t a = (uint32_t)sizeof(infl::WarpSmem);
+    uint32_t b = lzss::WARP_SMEM;
+    uint32_t c = (uint32_t)sizeof(SegTable) + ((max_lane + 15u) & ~15u) + 160u;
+    uint32_t d = brlew::WARP_SMEM;
+    uint32_t m = a > b ? a : b;
+    m = m > c ? m : c;
+    m = m > d ? m : d;
+    return (m + 15u) & ~15u;
+}
+
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Copy lane stream `slot` (nw words) of an interleaved block into dst with
+// the calling warp (asynchronous 4-byte copies), then zero 16 tail bytes.
+__device__ __forceinline__ void load_slot_warp(const SegTable* T, const uint8_t* block, uint32_t slot, uint32_t nw,
+                                               uint8_t* dst) {
+    const uint32_t lane = lane_id();
+    const uint32_t ltmask = (1u << slot) - 1u;
+    for (uint32_t k = lane; k < nw; k += 32) {
+        uint32_t j = 0;
+#pragma unroll
+        for (uint32_t step = 16; step; step >>= 1)
+            if (j + step <= 31 && T->hi[j + step - 1] <= k) j += step;
+        const uint32_t lo = j ? T->hi[j - 1] : 0u;
+        const uint32_t off = T->base[j] + (k - lo) * 4u * (32u - j) + 4u * __popc(T->mask[j] & ltmask);
+        const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + 4 * k);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(block + off) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    if (lane < 4) reinterpret_cast<uint32_t*>(dst)[nw + lane] = 0;
+    __syncwarp();
+}
+
+// One RLE v1 / v2 lane-stream task.
+__device__ uint32_t rle_task(const gd_task& t, uint32_t max_lane, uint8_t* ws) {
+    const uint32_t lane = lane_id();
+    SegTable* T = reinterpret_cast<SegTable*>(ws);
+    uint8_t* sbuf = ws + sizeof(SegTable);
+    uint32_t bad = (t.lane >= 32 || (reinterpret_cast<uintptr_t>(t.src) & 3u)) ? 1u : 0u;
+    const uint64_t l64 = t.col_len[lane];
+    if (l64 > max_lane) bad = 1;
+    const uint32_t len = bad ? 0u : (uint32_t)l64;
+    const uint32_t nw = (len + 3) >> 2;
+    uint32_t tot = warp_incl_scan(nw);
+    tot = __shfl_sync(GD_FULL_MASK, tot, 31);
+    if ((uint64_t)tot * 4 > t.src_len) bad = 1;
+    if (__any_sync(GD_FULL_MASK, bad)) return ST_CORRUPT;
+    seg_build(T, nw);
+    const uint32_t slot = t.lane;
+    const uint32_t my_len = __shfl_sync(GD_FULL_MASK, len, (int)slot);
+    load_slot_warp(T, t.src, slot, (my_len + 3) >> 2, sbuf);
+    if (t.codec == GD_CODEC_RLEV2) {
+        const uint32_t ru = t.param;
+        if (ru == 0 || t.chunk_size % (256ull * ru) || (reinterpret_cast<uintptr_t>(t.dst) & 7u)) return ST_INVALID;
+        const uint32_t nv = (uint32_t)(t.chunk_size / 256u);
+        return rlev2::lane_warp(sbuf, my_len, nv, slot, ru, reinterpret_cast<uint64_t*>(t.dst), t.dst_len / 8);
+    }
+    const uint32_t eb = t.param >> 16, wil = t.param & 0xffffu;
+    if (!(eb == 4 || eb == 8) || wil == 0 || t.chunk_size % (32ull * wil * eb) ||
+        (reinterpret_cast<uintptr_t>(t.dst) % eb))
+        return ST_INVALID;
+    const uint32_t nv = (uint32_t)(t.chunk_size / 32u / eb);
+    if (eb == 4)
+        return rlev1::lane_warp<uint32_t>(sbuf, my_len, nv, slot, wil, reinterpret_cast<uint32_t*>(t.dst),
+                                          t.dst_len / 4);
+    return rlev1::lane_warp<uint64_t>(sbuf, my_len, nv, slot, wil, reinterpret_cast<uint64_t*>(t.dst),
+                                      t.dst_len / 8);
+}
+
+__device__ uint32_t run_task(const gd_task& t, uint32_t max_lane, uint8_t* ws) {
+    switch (t.codec) {
+        case GD_CODEC_BRLE:
+            if (t.src_len > 0x7fffffffull || t.dst_len > 0x7fffffffull) return ST_INVALID;
+            return brlew::chunk_warp(t.src, (uint32_t)t.src_len, t.dst, (uint32_t)t.dst_len, ws);
+        case GD_CODEC_RLEV1:
+        case GD_CODEC_RLEV2:
+            return rle_task(t, max_lane, ws);
+        case GD_CODEC_LZSS:
+            if (t.dst_len != t.chunk_size || (reinterpret_cast<uintptr_t>(t.dst) & 3u)) return ST_INVALID;
+            return lzss::chunk_warp(t.src, t.src_len, t.col_len, t.col_map, t.chunk_size, t.dst, ws);
+        case GD_CODEC_DEFLATE: {
+            if (t.src_len > 0xffffffffull || t.dst_len > 0xffffffffull) return ST_INVALID;
+            uint32_t fin = 0;
+            const uint32_t e = infl::stream_warp(t.src, (uint32_t)t.src_len, t.dst, (uint32_t)t.dst_len,
+                                                 (int)t.param, *reinterpret_cast<infl::WarpSmem*>(ws), &fin);
+            return (e == ST_OK && fin != (uint32_t)t.dst_len) ? (uint32_t)ST_CORRUPT : e;
+        }
+        default:
+            return ST_UNSUPPORTED;
+    }
+}
+
+__global__ void __launch_bounds__(WPB * 32) batch_kernel(const gd_task* __restrict__ tasks, uint32_t n,
+                                                        const uint32_t* __restrict__ order, uint32_t* counter,
+                                                        int dynamic, uint32_t max_lane, uint32_t ws_bytes,
+                                                        uint32_t* __restrict__ status,
+                                                        uint64_t* __restrict__ timing) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+    uint8_t* ws = smem + wid * ws_bytes;
+    const uint32_t gw = blockIdx.x * WPB + wid, W = gridDim.x * WPB;
+    for (uint32_t k = 0;; ++k) {
+        uint32_t i;
+        if (dynamic) {
+            uint32_t v = 0;
+            if (lane == 0) v = atomicAdd(counter, 1u);
+            i = __shfl_sync(GD_FULL_MASK, v, 0);
+        } else {
+            i = gw + k * W;
+        }
+        if (i >= n) break;
+        const uint32_t ti = order ? order[i] : i;
+        if (ti >= n) break;  // a malformed order array ends this worker
+        const uint64_t t0 = globaltimer();
+        const gd_task t = tasks[ti];
+        const uint32_t e = run_task(t, max_lane, ws);
+        __syncwarp();
+        const uint64_t t1 = globaltimer();
+        if (lane == 0) {
+            put_status(status, ti, e);
+            if (timing) {
+                timing[2ull * ti] = t0;
+                timing[2ull * ti + 1] = t1;
+            }
+        }
+    }
+}
+
+}  // namespace batch
+}  // namespace gd
+
+extern "C" gd_status_t gd_batch_decode(const gd_task* d_tasks, uint32_t n_tasks, const uint32_t* d_order,
+                                       int dynamic, uint32_t max_lane_bytes, uint32_t blocks_per_sm,
+                                       uint32_t* d_counter, uint32_t* d_status, uint64_t* d_timing,
+                                       gd_stream_t stream) {
+    using namespace gd::batch;
+    if (n_tasks == 0) return GD_OK;
+    if (!d_tasks || (dynamic && !d_counter)) return GD_ERR_INVALID_ARG;
+    const uint32_t ws = warp_smem_bytes(max_lane_bytes);
+    const uint32_t smem = WPB * ws;
+    if (smem > 220 * 1024) return GD_ERR_UNSUPPORTED;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int dev = 0, sms = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, WPB * 32, smem);
+    if (occ < 1) occ = 1;
+    const uint32_t bps = blocks_per_sm ? (blocks_per_sm < (uint32_t)occ ? blocks_per_sm : (uint32_t)occ) : (uint32_t)occ;
+    if (dynamic && cudaMemsetAsync(d_counter, 0, sizeof(uint32_t), s) != cudaSuccess) return GD_ERR_CUDA;
+    batch_kernel<<<bps * (uint32_t)sms, WPB * 32, smem, s>>>(d_tasks, n_tasks, d_order, d_counter, dynamic,
+                                                            max_lane_bytes, ws, d_status, d_timing);
+    return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+}
+
+extern "C" uint32_t gd_batch_warps(uint32_t max_lane_bytes, uint32_t blocks_per_sm) {
+    using namespace gd::batch;
+    const uint32_t smem = WPB * warp_smem_bytes(max_lane_bytes);
+    cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int dev = 0, sms = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, WPB * 32, smem);
+    if (occ < 1) occ = 1;
+    const uint32_t bps = blocks_per_sm ? (blocks_per_sm < (uint32_t)occ ? blocks_per_sm : (uint32_t)occ) : (uint32_t)occ;
+    return bps * (uint32_t)sms * WPB;
+}

@@ -1023,7 +1023,8 @@ uint64_t gd_lzss_encode_stream(const uint8_t* in, uint32_t n, uint8_t* out, uint
 // ---------------------------------------------------------------------------
 // LZSS interleaved container (lzss::compress_gpu, lzss_gpu2.h:1915-2127).
 // chunk_size must be a multiple of 128; a short final chunk is zero padded
-// to whole 128-byte rows (the reference drops it, lzss_gpu2.h:1959).
+// to a whole chunk (the reference drops it, lzss_gpu2.h:1959), so every
+// column of every chunk holds chunk_size/32 bytes.
 // Column q of a chunk is bytes 4q+128k..+3.  Lanes are ranked by descending
 // stream length, ties by descending column (the reversed stable ascending
 // radix sort, lzss_gpu2.h:1063-1086).  Writes blk_off[n+1], col_len[32n]
@@ -1041,7 +1042,7 @@ uint64_t gd_lzss_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint
     std::vector<std::vector<uint8_t>> cols(nc * 32);
     parallel_for(nc, [&](uint64_t c) {
         uint64_t len = std::min(chunk_size, n - c * chunk_size);
-        uint64_t padded = (len + 127) / 128 * 128;
+        uint64_t padded = chunk_size;  // a short final chunk is zero padded to a whole chunk
         std::vector<uint8_t> chunk(padded, 0);
         memcpy(chunk.data(), in + c * chunk_size, len);
         uint32_t L = (uint32_t)(padded / 32);

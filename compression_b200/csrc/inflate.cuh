@@ -1,0 +1,548 @@
+// inflate.cuh -- warp-level Deflate / zlib / gzip inflate for sm_100a
+// (shared by the plain kernels in inflate.cu and the batched decoder).
+//
+// Replaces the reference's deflate::inflate / inflate_shared
+// (include/zlib/zlib.h:832-962): there one lane per chunk decodes codes
+// bit-serially from global-memory trees (zlib.h:233-266) and a writer warp
+// copies back-references; stored blocks are dropped (zlib.h:532-543).
+//
+// Here one warp owns a chunk and alternates two phases:
+//   decode  -- lane 0 reads the bit stream from a shared-memory input ring and
+//              decodes symbols with 10-bit lookup tables (longer codes fall
+//              back to a canonical count/symbol walk), appending commands
+//              (literal runs, (length, distance) copies, stored blocks) to a
+//              shared command buffer;
+//   execute -- all 32 lanes write the commands to the output: literal runs
+//              and stored data as coalesced byte stores, copies in 32-byte
+//              waves (distance >= 32: each wave reads bytes written by earlier
+//              waves; distance < 32: the period-`distance` pattern is read
+//              from before the copy).  The warp also refills the input ring.
+// Dynamic tables are rebuilt per block; table fills are spread over the warp.
+// Every read is bounded by the chunk's compressed size and every write by its
+// output size; malformed input yields GD_ERR_CORRUPT / GD_ERR_OVERRUN.
+#pragma once
+#include "gd_common.cuh"
+
+namespace gd {
+namespace infl {
+
+constexpr int WPB = 2;             // warps (chunks) per block
+constexpr uint32_t IRING = 8192;   // input ring bytes per warp
+constexpr uint32_t LBITS = 10;     // primary lookup bits
+constexpr uint32_t NCMD = 256;     // commands per batch
+constexpr uint32_t NLIT = 2048;    // literal bytes per batch
+
+// length codes 257..285 and distance codes 0..29 (RFC 1951 3.2.5)
+__device__ __constant__ uint16_t LBASE[29] = {3,  4,  5,  6,  7,  8,  9,  10, 11,  13,  15,  17,  19,  23, 27,
+                                              31, 35, 43, 51, 59, 67, 83, 99, 115, 131, 163, 195, 227, 258};
+__device__ __constant__ uint8_t LEXT[29] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2,
+                                            2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5, 0};
+__device__ __constant__ uint16_t DBASE[30] = {1,   2,   3,   4,   5,   7,    9,    13,   17,   25,
+                                              33,  49,  65,  97,  129, 193,  257,  385,  513,  769,
+                                              1025, 1537, 2049, 3073, 4097, 6145, 8193, 12289, 16385, 24577};
+__device__ __constant__ uint8_t DEXT[30] = {0, 0, 0, 0, 1, 1, 2, 2,  3,  3,  4,  4,  5,  5,  6,
+                                            6, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 12, 12, 13, 13};
+__device__ __constant__ uint8_t CLORDER[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
+
+// A canonical Huffman code: primary table + count/symbol arrays for the walk.
+struct Huff {
+    uint32_t lut[1 << LBITS];  // (sym << 8) | len, len 0 = longer than LBITS, 0xffffffff = invalid
+    uint16_t count[16];
+    uint16_t sym[320];
+};
+
+enum : uint32_t { C_LIT = 0, C_COPY = 1, C_STORED = 2 };
+
+struct WarpSmem {
+    uint8_t ring[IRING];
+    Huff lit;
+    Huff dist;
+    uint8_t lens[320];
+    uint8_t lits[NLIT];
+    uint32_t cmd_a[NCMD];  // C_LIT: literal buffer offset | C_COPY: distance | C_STORED: input offset
+    uint32_t cmd_b[NCMD];  // length
+    uint8_t cmd_t[NCMD];
+    // decoder state shared between lane 0 and the warp
+    uint32_t n_cmd, n_lit, status, done;
+};
+
+// Build `h` from code lengths lens[0..n).  Counting / offsets on lane 0, the
+// primary table fill spread over the warp.  Returns false (on every lane) for
+// an over-subscribed or otherwise unusable code.
+static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint32_t* sh_flag) {
+    const uint32_t lane = lane_id();
+    for (uint32_t i = lane; i < (1u << LBITS); i += 32) h->lut[i] = 0xffffffffu;
+    if (lane == 0) {
+        uint16_t offs[16];
+        for (int i = 0; i < 16; ++i) h->count[i] = 0;
+        for (uint32_t s = 0; s < n; ++s) h->count[lens[s]]++;
+        int left = 1;
+        bool ok = true;
+        for (int L = 1; L < 16; ++L) {
+            left <<= 1;
+            left -= h->count[L];
+            if (left < 0) ok = false;
+        }
+        offs[1] = 0;
+        for (int L = 1; L < 15; ++L) offs[L + 1] = offs[L] + h->count[L];
+        for (uint32_t s = 0; s < n; ++s)
+            if (lens[s]) h->sym[offs[lens[s]]++] = (uint16_t)s;
+        *sh_flag = ok ? 1u : 0u;
+    }
+    __syncwarp();
+    if (!*sh_flag) return false;
+    // canonical codes in symbol order: code(s) = first(len) + rank among equal lengths
+    // lane-parallel: every lane walks the sorted symbol list for a subset of lengths
+    for (uint32_t L = 1 + lane; L <= LBITS; L += 32) {
+        uint32_t first = 0, idx = 0;
+        uint32_t code = 0;
+        for (uint32_t l = 1; l < L; ++l) {
+            code = (code + h->count[l]) << 1;
+            idx += h->count[l];
+        }
+        first = code;
+        for (uint32_t k = 0; k < h->count[L]; ++k) {
+            const uint32_t c = first + k;
+            // deflate sends codes MSB first into an LSB-first stream: reverse
+            const uint32_t rev = __brev(c) >> (32 - L);
+            const uint32_t entry = ((uint32_t)h->sym[idx + k] << 8) | L;
+            for (uint32_t f = rev; f < (1u << LBITS); f += (1u << L)) h->lut[f] = entry;
+        }
+    }
+    __syncwarp();
+    // prefixes of codes longer than LBITS: mark for the canonical walk
+    for (uint32_t L = LBITS + 1 + lane; L < 16; L += 32) {
+        uint32_t code = 0, idx = 0;
+        for (uint32_t l = 1; l < L; ++l) {
+            code = (code + h->count[l]) << 1;
+            idx += h->count[l];
+        }
+        for (uint32_t k = 0; k < h->count[L]; ++k) {
+            const uint32_t c = code + k;
+            const uint32_t pre = __brev(c >> (L - LBITS)) >> (32 - LBITS);
+            atomicExch(&h->lut[pre], 0u);  // len 0: walk
+        }
+    }
+    __syncwarp();
+    return true;
+}
+
+// Inflate one stream with the calling warp.  src: clen compressed bytes
+// (the 16-byte-aligned span around them must be readable); dst: room for
+// olen bytes; hdr: 0 raw deflate, 1 zlib, 2 gzip; S: this warp's shared
+// state.  Returns a gd status (same on every lane); *written = bytes output.
+static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ src, uint32_t clen,
+                                             uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
+                                             WarpSmem& S, uint32_t* written) {
+    const uint32_t lane = lane_id();
+    uint32_t err = ST_OK;
+    // input ring: compressed byte i (chunk-relative) at ring[(i + sh) % IRING];
+    // fills are 16-byte aligned global loads.
+    const uint32_t sh = (uint32_t)(reinterpret_cast<uintptr_t>(src) & 15u);
+    const uint8_t* src_al = src - sh;
+    const uint32_t span = clen + sh;  // bytes of the aligned view we may touch
+    uint32_t fill = 0;                // aligned-view bytes loaded so far
+    auto refill = [&](uint32_t consumed_al) {
+        // load the aligned view up to consumed_al + IRING (whole 16-byte words,
+        // plus the ragged end of the chunk once it is reached)
+        uint32_t target = min(consumed_al + IRING, span);
+        if (target < span) target &= ~15u;
+        if (target > fill) {
+            const uint32_t a = fill, b = target & ~15u;
+            for (uint32_t i = a + 16 * lane; i + 16 <= b; i += 512) {
+                const uint4 v = *reinterpret_cast<const uint4*>(src_al + i);
+                *reinterpret_cast<uint4*>(S.ring + (i & (IRING - 1))) = v;
+            }
+            for (uint32_t i = max(a, b) + lane; i < target; i += 32)
+                if (i >= sh) S.ring[i & (IRING - 1)] = src_al[i];
+            fill = target;
+        }
+        __syncwarp();
+    };
+
+    // ---- lane-0 decoder state ----
+    uint64_t bitbuf = 0;
+    uint32_t bitcnt = 0;
+    uint32_t inpos = sh;     // next aligned-view byte to move into bitbuf
+    uint32_t opos = 0;       // output bytes committed by decoded commands
+    uint32_t bfinal = 0, btype = 0xff, in_block = 0;
+
+    if (lane == 0) {
+        S.status = err;
+        S.done = 0;
+    }
+    __syncwarp();
+    refill(0);
+    if (lane == 0 && err == ST_OK && zlib_hdr == 1) {
+        // zlib (RFC 1950): CMF, FLG; no preset dictionary
+        if (clen < 2) err = ST_CORRUPT;
+        else {
+            const uint32_t cmf = S.ring[(sh + 0) & (IRING - 1)], flg = S.ring[(sh + 1) & (IRING - 1)];
+            if ((cmf & 15u) != 8u || ((cmf << 8) | flg) % 31u != 0 || (flg & 32u)) err = ST_CORRUPT;
+            inpos += 2;
+        }
+        S.status = err;
+    } else if (lane == 0 && err == ST_OK && zlib_hdr == 2) {
+        // gzip (RFC 1952) member header; the 8-byte trailer is not read
+        auto at = [&](uint32_t i) -> uint32_t { return i < clen && sh + i < fill ? S.ring[(sh + i) & (IRING - 1)] : 0x100u; };
+        uint32_t p = 10;
+        if (at(0) != 0x1fu || at(1) != 0x8bu || at(2) != 8u || clen < 18) err = ST_CORRUPT;
+        const uint32_t flg = at(3);
+        if (err == ST_OK && (flg & 4u)) {  // FEXTRA
+            const uint32_t xl = at(p) | (at(p + 1) << 8);
+            p += 2 + xl;
+        }
+        if (err == ST_OK && (flg & 8u)) {  // FNAME
+            while (p < clen && at(p) != 0) { if (at(p) > 0xffu) { err = ST_CORRUPT; break; } ++p; }
+            ++p;
+        }
+        if (err == ST_OK && (flg & 16u)) {  // FCOMMENT
+            while (p < clen && at(p) != 0) { if (at(p) > 0xffu) { err = ST_CORRUPT; break; } ++p; }
+            ++p;
+        }
+        if (err == ST_OK && (flg & 2u)) p += 2;  // FHCRC
+        if (err == ST_OK && p + 8 > clen) err = ST_CORRUPT;
+        inpos += p;
+        S.status = err;
+    }
+    __syncwarp();
+    err = S.status;
+
+    // lane-0 helpers ------------------------------------------------------
+    auto need_bits = [&](uint32_t n) -> bool {
+        while (bitcnt < n) {
+            if (inpos >= fill) return false;
+            bitbuf |= (uint64_t)S.ring[inpos & (IRING - 1)] << bitcnt;
+            ++inpos;
+            bitcnt += 8;
+        }
+        return true;
+    };
+    auto fill_bits = [&]() {
+        while (bitcnt <= 56 && inpos < fill) {
+            bitbuf |= (uint64_t)S.ring[inpos & (IRING - 1)] << bitcnt;
+            ++inpos;
+            bitcnt += 8;
+        }
+    };
+    auto get_bits = [&](uint32_t n, uint32_t& v) -> bool {
+        if (!need_bits(n)) return false;
+        v = (uint32_t)(bitbuf & ((1ull << n) - 1ull));
+        bitbuf >>= n;
+        bitcnt -= n;
+        return true;
+    };
+    // decode one symbol of code h; returns false on exhausted input / bad code
+    auto decode_sym = [&](const Huff* h, uint32_t& sym) -> bool {
+        fill_bits();
+        const uint32_t e = h->lut[bitbuf & ((1u << LBITS) - 1u)];
+        if (e != 0xffffffffu && (e & 0xffu) != 0) {
+            const uint32_t L = e & 0xffu;
+            if (L > bitcnt) return false;
+            bitbuf >>= L;
+            bitcnt -= L;
+            sym = e >> 8;
+            return true;
+        }
+        if (e == 0xffffffffu) return false;
+        // canonical walk (puff-style) for codes longer than LBITS
+        int code = 0, first = 0, index = 0;
+        uint64_t bb = bitbuf;
+        for (uint32_t L = 1; L < 16; ++L) {
+            if (L > bitcnt) return false;
+            code |= (int)(bb & 1u);
+            bb >>= 1;
+            const int cnt = h->count[L];
+            if (code - cnt < first) {
+                sym = h->sym[index + (code - first)];
+                bitbuf >>= L;
+                bitcnt -= L;
+                return true;
+            }
+            index += cnt;
+            first += cnt;
+            first <<= 1;
+            code <<= 1;
+        }
+        return false;
+    };
+
+    uint32_t* sflag = &S.done;  // scratch word for build_huff's broadcast (restored below)
+    // main loop ------------------------------------------------------------
+    while (err == ST_OK) {
+        // ---- refill input for the decoder (warp) ----
+        uint32_t inpos_b = __shfl_sync(GD_FULL_MASK, inpos, 0);
+        refill(inpos_b > 64 ? inpos_b - 64 : 0);
+
+        // ---- block header (table builds need the warp) ----
+        uint32_t hdr_state = 0;  // 0 = none, 1 = fixed, 2 = dynamic lens ready, 3 = stored, 4 = end
+        if (lane == 0) {
+            S.n_cmd = 0;
+            S.n_lit = 0;
+            if (!in_block) {
+                if (bfinal) {
+                    hdr_state = 4;
+                } else {
+                    uint32_t bf, bt;
+                    if (!get_bits(1, bf) || !get_bits(2, bt)) err = ST_CORRUPT;
+                    bfinal = bf;
+                    btype = bt;
+                    if (err == ST_OK) {
+                        if (bt == 0) {
+                            hdr_state = 3;
+                        } else if (bt == 1) {
+                            for (int i = 0; i < 144; ++i) S.lens[i] = 8;
+                            for (int i = 144; i < 256; ++i) S.lens[i] = 9;
+                            for (int i = 256; i < 280; ++i) S.lens[i] = 7;
+                            for (int i = 280; i < 288; ++i) S.lens[i] = 8;
+                            for (int i = 0; i < 30; ++i) S.lens[288 + i] = 5;
+                            hdr_state = 1;
+                        } else if (bt == 2) {
+                            hdr_state = 2;
+                        } else {
+                            err = ST_CORRUPT;
+                        }
+                    }
+                }
+            }
+            S.status = err | (hdr_state << 8);
+        }
+        __syncwarp();
+        {
+            const uint32_t w = S.status;
+            err = w & 0xffu;
+            hdr_state = w >> 8;
+        }
+        if (err != ST_OK || hdr_state == 4) break;
+
+        if (hdr_state == 2) {
+            // dynamic: code-length code, then literal/length + distance lengths
+            uint32_t nlen = 0, ndist = 0;
+            if (lane == 0) {
+                uint32_t hlit, hdist, hclen;
+                if (!get_bits(5, hlit) || !get_bits(5, hdist) || !get_bits(4, hclen)) err = ST_CORRUPT;
+                nlen = hlit + 257;
+                ndist = hdist + 1;
+                if (nlen > 286 || ndist > 30) err = ST_CORRUPT;
+                for (int i = 0; i < 19; ++i) S.lens[i] = 0;
+                for (uint32_t i = 0; i < hclen + 4 && err == ST_OK; ++i) {
+                    uint32_t v;
+                    if (!get_bits(3, v)) err = ST_CORRUPT;
+                    S.lens[CLORDER[i]] = (uint8_t)v;
+                }
+                S.status = err;
+            }
+            __syncwarp();
+            err = S.status;
+            if (err != ST_OK) break;
+            if (!build_huff(&S.lit, S.lens, 19, sflag)) {
+                err = ST_CORRUPT;
+                break;
+            }
+            if (lane == 0) {
+                // read nlen + ndist code lengths (lens[0..nlen) lit, [288..288+ndist) dist)
+                uint8_t tmp[320];
+                uint32_t i = 0;
+                const uint32_t tot = nlen + ndist;
+                while (i < tot && err == ST_OK) {
+                    uint32_t sym;
+                    if (!decode_sym(&S.lit, sym)) {
+                        err = ST_CORRUPT;
+                        break;
+                    }
+                    if (sym < 16) {
+                        tmp[i++] = (uint8_t)sym;
+                    } else {
+                        uint32_t rep = 0, v = 0, x;
+                        if (sym == 16) {
+                            if (i == 0) {
+                                err = ST_CORRUPT;
+                                break;
+                            }
+                            v = tmp[i - 1];
+                            if (!get_bits(2, x)) err = ST_CORRUPT;
+                            rep = 3 + x;
+                        } else if (sym == 17) {
+                            if (!get_bits(3, x)) err = ST_CORRUPT;
+                            rep = 3 + x;
+                        } else {
+                            if (!get_bits(7, x)) err = ST_CORRUPT;
+                            rep = 11 + x;
+                        }
+                        if (i + rep > tot) err = ST_CORRUPT;
+                        for (uint32_t k = 0; k < rep && err == ST_OK; ++k) tmp[i++] = (uint8_t)v;
+                    }
+                }
+                if (err == ST_OK && tmp[256] == 0) err = ST_CORRUPT;  // no end-of-block code
+                for (uint32_t k = 0; k < 288; ++k) S.lens[k] = (k < nlen) ? tmp[k] : 0;
+                for (uint32_t k = 0; k < 30; ++k) S.lens[288 + k] = (k < ndist) ? tmp[nlen + k] : 0;
+                S.status = err;
+            }
+            __syncwarp();
+            err = S.status;
+            if (err != ST_OK) break;
+        }
+        if (hdr_state == 1 || hdr_state == 2) {
+            const bool ok1 = build_huff(&S.lit, S.lens, 288, sflag);
+            // a distance code with a single used symbol is allowed (incomplete)
+            const bool ok2 = ok1 && build_huff(&S.dist, S.lens + 288, 30, sflag);
+            if (!ok1 || !ok2) {
+                err = ST_CORRUPT;
+                break;
+            }
+            if (lane == 0) in_block = 1;
+        }
+
+        // ---- decode a batch of commands (lane 0) ----
+        if (lane == 0) {
+            uint32_t nc = 0, nl = 0;
+            if (hdr_state == 3) {
+                // stored block: align to a byte, LEN / NLEN
+                const uint32_t drop = bitcnt & 7u;
+                bitbuf >>= drop;
+                bitcnt -= drop;
+                uint32_t ln, nln;
+                if (!get_bits(16, ln) || !get_bits(16, nln) || (ln ^ 0xffffu) != nln) err = ST_CORRUPT;
+                // the bytes still in bitbuf come first
+                uint32_t avail_bytes = bitcnt >> 3;
+                if (err == ST_OK) {
+                    if (opos + ln > olen) err = ST_OVERRUN;
+                    const uint32_t from_buf = min(avail_bytes, ln);
+                    for (uint32_t k = 0; k < from_buf && err == ST_OK; ++k) {
+                        S.lits[nl++] = (uint8_t)(bitbuf & 0xffu);
+                        bitbuf >>= 8;
+                        bitcnt -= 8;
+                    }
+                    if (from_buf && err == ST_OK) {
+                        S.cmd_t[nc] = C_LIT;
+                        S.cmd_a[nc] = 0;
+                        S.cmd_b[nc] = from_buf;
+                        ++nc;
+                    }
+                    const uint32_t rest = ln - from_buf;
+                    if (err == ST_OK && rest) {
+                        // remaining bytes straight from global (aligned-view offset inpos)
+                        if (inpos + rest > span) err = ST_CORRUPT;
+                        // the stored bytes are read from global: skip them in the ring
+                        if (fill < inpos + rest) fill = max(fill, (inpos + rest) & ~15u);
+                        S.cmd_t[nc] = C_STORED;
+                        S.cmd_a[nc] = inpos - sh;
+                        S.cmd_b[nc] = rest;
+                        ++nc;
+                        inpos += rest;
+                    }
+                    opos += ln;
+                }
+            } else {
+                // Huffman-coded symbols until the batch is full or the block ends
+                uint32_t lit_start = 0;
+                while (err == ST_OK && nc < NCMD - 1 && nl < NLIT && (fill - inpos >= 32 || fill >= span)) {
+                    uint32_t sym;
+                    if (!decode_sym(&S.lit, sym)) {
+                        err = ST_CORRUPT;
+                        break;
+                    }
+                    if (sym < 256) {
+                        if (opos >= olen) {
+                            err = ST_OVERRUN;
+                            break;
+                        }
+                        if (nl == lit_start) {  // open a literal run
+                            S.cmd_t[nc] = C_LIT;
+                            S.cmd_a[nc] = nl;
+                            S.cmd_b[nc] = 0;
+                            ++nc;
+                        }
+                        S.lits[nl++] = (uint8_t)sym;
+                        S.cmd_b[nc - 1]++;
+                        ++opos;
+                        continue;
+                    }
+                    lit_start = nl;
+                    if (sym == 256) {
+                        in_block = 0;
+                        break;
+                    }
+                    if (sym > 285) {
+                        err = ST_CORRUPT;
+                        break;
+                    }
+                    uint32_t x, len, dsym, dist;
+                    if (!get_bits(LEXT[sym - 257], x)) {
+                        err = ST_CORRUPT;
+                        break;
+                    }
+                    len = LBASE[sym - 257] + x;
+                    if (!decode_sym(&S.dist, dsym) || dsym > 29 || !get_bits(DEXT[dsym], x)) {
+                        err = ST_CORRUPT;
+                        break;
+                    }
+                    dist = DBASE[dsym] + x;
+                    if (dist > opos) {
+                        err = ST_CORRUPT;
+                        break;
+                    }
+                    if (opos + len > olen) {
+                        err = ST_OVERRUN;
+                        break;
+                    }
+                    S.cmd_t[nc] = C_COPY;
+                    S.cmd_a[nc] = dist;
+                    S.cmd_b[nc] = len;
+                    ++nc;
+                    opos += len;
+                }
+            }
+            S.n_cmd = nc;
+            S.n_lit = nl;
+            S.status = err;
+        }
+        __syncwarp();
+        err = S.status;
+        fill = __shfl_sync(GD_FULL_MASK, fill, 0);
+        if (err != ST_OK) break;
+
+        // ---- execute the batch (all lanes) ----
+        const uint32_t nc = S.n_cmd;
+        uint32_t pos = __shfl_sync(GD_FULL_MASK, opos, 0);
+        // pos is the end position after the batch; walk back to its start
+        {
+            uint32_t tot = 0;
+            for (uint32_t c = lane; c < nc; c += 32) tot += S.cmd_b[c];
+            for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(GD_FULL_MASK, tot, o);
+            pos -= tot;
+        }
+        for (uint32_t c = 0; c < nc; ++c) {
+            const uint32_t t = S.cmd_t[c], a = S.cmd_a[c], n = S.cmd_b[c];
+            uint8_t* d = dst + pos;
+            if (t == C_LIT) {
+                for (uint32_t k = lane; k < n; k += 32) d[k] = S.lits[a + k];
+            } else if (t == C_STORED) {
+                const uint8_t* s = src + a;
+                for (uint32_t k = lane; k < n; k += 32) d[k] = s[k];
+            } else {
+                const uint8_t* s = d - a;
+                if (a >= 32) {
+                    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+                        const uint32_t k = k0 + lane;
+                        uint8_t v = 0;
+                        if (k < n) v = s[k];
+                        __syncwarp();
+                        if (k < n) d[k] = v;
+                        __syncwarp();
+                    }
+                } else {
+                    for (uint32_t k = lane; k < n; k += 32) d[k] = s[k % a];
+                }
+            }
+            pos += n;
+            __syncwarp();
+        }
+    }
+    const uint32_t fin = __shfl_sync(GD_FULL_MASK, opos, 0);
+    *written = fin;
+    return __shfl_sync(GD_FULL_MASK, err, 0);
+}
+
+}  // namespace infl
+}  // namespace gd

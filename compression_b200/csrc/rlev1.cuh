@@ -1,0 +1,154 @@
+// rlev1.cuh -- RLE v1 (ORC-style integer RLE v1) decoder for sm_100a.
+//
+// Grammar (restated from decoder_warp, include/rle_v1/decoder.h:278-423):
+// int8 header h; h < 0: -h literal values, each an unsigned LEB128 varint;
+// h >= 0: a run of h+3 values, int8 delta then varint base, v_i = base+i*delta.
+// Lane t of a chunk owns elements (i / wil)*32*wil + t*wil + i % wil,
+// wil = COMP_COL_LEN / sizeof(T); a lane stream ends once it has produced
+// chunk_size/32 bytes (decoder.h:283,291).
+//
+// The reference pairs a reader warp and a decoder warp per chunk (spin
+// queues, one byte fetched per funnel-shift call, one scalar store per
+// value).  Here every lane stream gets a whole warp (same block loader as
+// RLE v2: 8 adjacent lane streams per block, copied with fully used 32-byte
+// row sectors):
+//   * runs are closed form: lane i writes base + i*delta;
+//   * a literal group is decoded 32 values at a time: the lanes load a
+//     128-byte window, ballot the varint terminators (bytes < 0x80), and lane
+//     j finds the j-th terminator with a select over the 128-bit mask, so
+//     every lane knows where its varint starts and ends and decodes it alone.
+#pragma once
+#include "interleave.cuh"
+
+namespace gd {
+namespace rlev1 {
+
+
+// Largest lane stream for nv values: literal varints of up to 10 bytes plus
+// one header per 127 values; +128 tail for terminator windows.
+__host__ __device__ constexpr uint32_t stream_cap(uint32_t nv, uint32_t eb) {
+    return (((eb == 8 ? 10u : 5u) * nv + nv / 127u + 64u + 15u) & ~15u) + 144u;
+}
+
+// Shared-memory bytes reserved for a lane stream of at most `n` bytes.
+__host__ __device__ constexpr uint32_t lane_cap(uint32_t n) { return ((n + 15u) & ~15u) + 144u; }
+
+// index (0-based) of the n-th set bit of the 128-bit mask m[0..3] (n < popc)
+__device__ __forceinline__ uint32_t select128(const uint32_t m[4], uint32_t n) {
+    uint32_t base = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const uint32_t c = __popc(m[q]);
+        if (n < c) return base + __fns(m[q], 0, (int)n + 1);
+        n -= c;
+        base += 32;
+    }
+    return 0xffffffffu;
+}
+
+// Decode one lane stream (sbuf[0..len), readable 144 bytes past len) of nv
+// elements of type T with the calling warp.  Lane stream t with wil = values
+// per lane slice: element e goes to outv[(e/wil)*32*wil + t*wil + e%wil] if
+// that index is below want.  Returns a gd status (same on every lane).
+template <typename T>
+static __device__ __noinline__ uint32_t lane_warp(const uint8_t* __restrict__ sbuf, uint32_t len, uint32_t nv, uint32_t t,
+                                           uint32_t wil, T* __restrict__ outv, uint64_t want) {
+    const uint32_t lane = lane_id();
+    auto put = [&](uint32_t e, uint64_t v) {
+        const uint64_t oe = (uint64_t)(e / wil) * 32u * wil + (uint64_t)t * wil + (e % wil);
+        if (oe < want) outv[oe] = (T)v;
+    };
+    uint32_t err = ST_OK, pos = 0, g = 0;
+    while (g < nv) {
+        // ---- header (lane 0) ----
+        uint32_t kind = 0, cnt = 0, next = 0, e = ST_OK;
+        uint64_t base = 0, delta = 0;
+        if (lane == 0) {
+            uint32_t p = pos;
+            if (p >= len) {
+                e = ST_CORRUPT;
+            } else {
+                const uint32_t h = sbuf[p++];
+                if (h & 0x80u) {
+                    kind = 1;
+                    cnt = 256u - h;
+                } else if (p >= len) {
+                    e = ST_CORRUPT;
+                } else {
+                    kind = 0;
+                    cnt = h + 3u;
+                    delta = (uint64_t)(int64_t)(int8_t)sbuf[p++];
+                    uint32_t sh = 0, b;
+                    do {
+                        if (p >= len || sh > 63) {
+                            e = ST_CORRUPT;
+                            break;
+                        }
+                        b = sbuf[p++];
+                        base |= (uint64_t)(b & 0x7fu) << sh;
+                        sh += 7;
+                    } while (b & 0x80u);
+                    if (sizeof(T) == 4) base &= 0xffffffffull;
+                }
+            }
+            next = p;
+        }
+        kind = __shfl_sync(GD_FULL_MASK, kind, 0);
+        cnt = __shfl_sync(GD_FULL_MASK, cnt, 0);
+        next = __shfl_sync(GD_FULL_MASK, next, 0);
+        e = __shfl_sync(GD_FULL_MASK, e, 0);
+        if (e != ST_OK) {
+            err = e;
+            break;
+        }
+        if (g + cnt > nv) {
+            err = ST_OVERRUN;
+            break;
+        }
+        if (kind == 0) {  // run: closed form
+            base = ((uint64_t)__shfl_sync(GD_FULL_MASK, (uint32_t)(base >> 32), 0) << 32) |
+                   __shfl_sync(GD_FULL_MASK, (uint32_t)base, 0);
+            delta = ((uint64_t)__shfl_sync(GD_FULL_MASK, (uint32_t)(delta >> 32), 0) << 32) |
+                    __shfl_sync(GD_FULL_MASK, (uint32_t)delta, 0);
+            for (uint32_t i = lane; i < cnt; i += 32) put(g + i, base + (uint64_t)i * delta);
+            g += cnt;
+            pos = next;
+            continue;
+        }
+        // literal group: cnt varints starting at `next`
+        uint32_t p = next, rem = cnt;
+        while (rem) {
+            uint32_t m[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t bpos = p + 32u * q + lane;
+                const bool term = (bpos < len) && !(sbuf[bpos] & 0x80u);
+                m[q] = __ballot_sync(GD_FULL_MASK, term);
+            }
+            const uint32_t nterm = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
+            if (nterm == 0) {  // no varint ends within 128 bytes (or the stream ran out)
+                err = ST_CORRUPT;
+                break;
+            }
+            const uint32_t take = min(min(rem, nterm), 32u);
+            if (lane < take) {
+                const uint32_t end = select128(m, lane);
+                const uint32_t beg = lane ? select128(m, lane - 1) + 1 : 0;
+                uint64_t v = 0;
+                uint32_t sh = 0;
+                for (uint32_t k = beg; k <= end; ++k, sh += 7)
+                    if (sh < 64) v |= (uint64_t)(sbuf[p + k] & 0x7fu) << sh;
+                put(g + lane, v);
+            }
+            p += select128(m, take - 1) + 1;
+            g += take;
+            rem -= take;
+        }
+        if (err != ST_OK) break;
+        pos = p;
+    }
+    return err;
+}
+
+}  // namespace rlev1
+}  // namespace gd

@@ -155,6 +155,60 @@ gd_status_t gd_gpuinflate(const gd_inflate_input* d_inputs, gd_inflate_status* d
 gd_status_t gd_copy_uncompressed_blocks(const gd_inflate_input* d_inputs, int count, gd_stream_t stream);
 
 /* ------------------------------------------------------------------------
+ * Batched mixed-codec decoding (no reference counterpart: the reference
+ * launches one decoder per column and codec)
+ * ------------------------------------------------------------------------ */
+
+typedef enum gd_codec {
+    GD_CODEC_BRLE = 0,
+    GD_CODEC_RLEV1 = 1,
+    GD_CODEC_RLEV2 = 2,
+    GD_CODEC_LZSS = 3,
+    GD_CODEC_DEFLATE = 4
+} gd_codec_t;
+
+/* One warp-sized unit of work.  All pointers are device pointers.
+ *   BRLE:    src/src_len = one chunk's token stream; dst/dst_len = its output.
+ *   RLEV1/2: src/src_len = the chunk's interleaved block; col_len = its 32
+ *            lane lengths; lane = which lane stream; dst = the chunk's output
+ *            base; dst_len = bytes of the chunk kept; chunk_size = the chunk
+ *            size; param = RLE v1: (elem_bytes << 16) | values per lane slice,
+ *            RLE v2: READ_UNIT.
+ *   LZSS:    src/src_len = the chunk's block; col_len/col_map = its 32 ranks;
+ *            dst_len = chunk_size (whole chunk written).
+ *   DEFLATE: src/src_len = one stream; dst/dst_len = its exact output;
+ *            param = 0 raw, 1 zlib, 2 gzip (src's 16-byte-aligned span readable). */
+typedef struct gd_task {
+    uint32_t codec;
+    uint32_t param;
+    uint32_t lane;
+    uint32_t reserved;
+    const uint8_t* src;
+    uint64_t src_len;
+    uint8_t* dst;
+    uint64_t dst_len;
+    uint64_t chunk_size;
+    const uint64_t* col_len;
+    const uint8_t* col_map;
+} gd_task;
+
+/*
+ * Decode n_tasks tasks in one persistent launch (blocks_per_sm x SMs blocks
+ * of 4 warps; 0 = as many as fit).  dynamic = 1: warps take tasks in the
+ * order d_order[0..n) (NULL = identity) from a work queue whose counter is
+ * d_counter (one uint32 of caller scratch, zeroed by this call); dynamic = 0:
+ * task d_order[i] runs on warp i mod W.  max_lane_bytes bounds col_len of
+ * RLE tasks.  d_status[n] (task index order) and optional d_timing[2n]
+ * (%globaltimer ns at each task's start and end) are written per task.
+ */
+gd_status_t gd_batch_decode(const gd_task* d_tasks, uint32_t n_tasks, const uint32_t* d_order, int dynamic,
+                            uint32_t max_lane_bytes, uint32_t blocks_per_sm, uint32_t* d_counter,
+                            uint32_t* d_status, uint64_t* d_timing, gd_stream_t stream);
+
+/* Number of warps gd_batch_decode runs with for these parameters. */
+uint32_t gd_batch_warps(uint32_t max_lane_bytes, uint32_t blocks_per_sm);
+
+/* ------------------------------------------------------------------------
  * Host API (reference signatures; synchronous; output from malloc)
  * ------------------------------------------------------------------------ */
 

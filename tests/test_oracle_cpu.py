@@ -90,3 +90,17 @@ def test_oracle_rejects_corruption():
     e2.meta["col_len"][0] += 4
     rc, _ = oracle.decode(e2)
     assert rc != 0
+
+
+def test_lzss_partial_last_chunk():
+    raw = cc.gen_markov_copy(12, 3 * 65536 + 1000, 4096)
+    _roundtrip(cc.lzss_encode(raw, 65536), raw)
+
+
+def test_mixed_batch_items_roundtrip():
+    import compression_b200.batch as B
+    items = B.make_mixed_batch(3, 40, 8 << 20)
+    assert {it.codec for it in items} == set(B.CODECS)
+    for it in items:
+        rc, out = oracle.decode(it.enc)
+        assert rc == 0 and np.array_equal(out, it.raw), it.codec
