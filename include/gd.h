@@ -209,6 +209,23 @@ gd_status_t gd_batch_decode(const gd_task* d_tasks, uint32_t n_tasks, const uint
 uint32_t gd_batch_warps(uint32_t max_lane_bytes, uint32_t blocks_per_sm);
 
 /* ------------------------------------------------------------------------
+ * Learned task-cost model: FP32 MLP 16 -> 64 -> 64 -> 1 (ReLU), parameters
+ * W1[16][64] | b1[64] | W2[64][64] | b2[64] | W3[64] | b3 in one float array.
+ * No reference counterpart.
+ * ------------------------------------------------------------------------ */
+
+uint32_t gd_mlp_num_params(void);
+/* d_out[i] = MLP(d_x[i*16 .. i*16+16)) for i < n. */
+gd_status_t gd_mlp_predict(const float* d_params, const float* d_x, uint32_t n, float* d_out, gd_stream_t stream);
+/* One mini-batch step on rows d_idx[0..nb) (nb <= 256) of (d_x, d_y),
+ * minimising the mean squared error.  d_grad != NULL: write the gradient and
+ * leave the parameters; else an Adam step (step >= 1) updates d_params, d_m,
+ * d_v.  d_loss (optional): the mini-batch loss. */
+gd_status_t gd_mlp_train_step(float* d_params, float* d_m, float* d_v, const float* d_x, const float* d_y,
+                              const uint32_t* d_idx, uint32_t nb, float lr, float beta1, float beta2, float eps,
+                              uint32_t step, float* d_grad, float* d_loss, gd_stream_t stream);
+
+/* ------------------------------------------------------------------------
  * Host API (reference signatures; synchronous; output from malloc)
  * ------------------------------------------------------------------------ */
 
