@@ -77,7 +77,8 @@ extern "C" gd_status_t gd_rlev2_decode(const uint8_t* d_data, const uint64_t* d_
     const uint32_t nv = (uint32_t)(chunk_size / 256u);
     // shared memory per lane stream: the caller's bound on the longest lane
     // stream if given, else the longest a valid stream of nv values can be
-    const uint32_t cap = max_lane_bytes ? lane_cap(max_lane_bytes) : stream_cap(nv);
+    // (a bound above the longest valid stream is clamped: longer lanes are corrupt)
+    const uint32_t cap = max_lane_bytes ? min(lane_cap(max_lane_bytes), stream_cap(nv)) : stream_cap(nv);
     const uint32_t smem = LANES_PER_BLOCK * cap;
     if (smem > 200 * 1024) return GD_ERR_UNSUPPORTED;  // lane streams must fit in shared memory
     cudaStream_t s = (cudaStream_t)stream;
