@@ -194,3 +194,151 @@ extern "C" uint32_t gd_batch_warps(uint32_t max_lane_bytes, uint32_t blocks_per_
     const uint32_t bps = blocks_per_sm ? (blocks_per_sm < (uint32_t)occ ? blocks_per_sm : (uint32_t)occ) : (uint32_t)occ;
     return bps * (uint32_t)sms * WPB;
 }
+
+// ---------------------------------------------------------------------------
+// Batch decode with longest-first placement and no allocation at all.
+//
+// For callers that may not allocate device memory at decode time: code that
+// runs while a stream is being captured into a CUDA graph (an allocation
+// there is an error or turns into a graph node the caller did not plan for),
+// and hosts that hand the decoder a fixed memory budget up front (a query
+// engine's pre-reserved pool) and treat any further allocation as a failure.
+// gd_batch_decode needs a work-queue counter and an order array from its
+// caller; here both live in the file-scope array below, together with the
+// buckets of the sort that makes the order, so the only memory touched is the
+// caller's tasks, costs, outputs and statuses plus this fixed array.
+//
+// Limits: at most NOALLOC_MAX_TASKS tasks per call (larger batches are
+// rejected with GD_ERR_INVALID_ARG).  Nothing has to start at zero: the sort
+// kernel clears the buckets and the counter at the start of every call.
+// Calls that overlap in time on one device (two streams, or two host
+// threads) share the array and race; the caller serialises them.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace gd {
+namespace batch {
+
+constexpr uint32_t NOALLOC_MAX_TASKS = GD_BATCH_NOALLOC_MAX_TASKS;
+constexpr uint32_t NBUCKET = 1024;  // cost buckets of the order sort
+constexpr uint32_t SORT_NT = 1024;  // threads of the single sort block
+// [0, MAX): order; [MAX, MAX + NBUCKET): bucket cursors; [MAX + NBUCKET]: counter
+static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_MAX_TASKS + NBUCKET + 64];
+
+// Bucket of cost c in [mn, mx]: the highest cost goes to bucket 0, so the
+// bucket order is longest first; NaN and equal costs go last / to bucket 0.
+__device__ __forceinline__ uint32_t cost_bucket(float c, float mn, float scale) {
+    if (!(c >= mn)) return NBUCKET - 1;  // NaN or below the minimum
+    const float q = (c - mn) * scale;
+    const uint32_t b = q >= (float)(NBUCKET - 1) ? NBUCKET - 1 : (uint32_t)q;
+    return NBUCKET - 1 - b;
+}
+
+// One block: counting sort of task indices by descending cost (bucketed, so
+// tasks within a bucket are in arbitrary order) into scratch order[0..n),
+// and the work-queue counter reset to zero.
+__global__ void __launch_bounds__(SORT_NT) lpt_sort_kernel(const float* __restrict__ cost, uint32_t n,
+                                                            uint32_t* __restrict__ scratch) {
+    __shared__ uint32_t hist[NBUCKET];
+    __shared__ float red_mn[SORT_NT / 32], red_mx[SORT_NT / 32];
+    uint32_t* order = scratch;
+    uint32_t* cursor = scratch + NOALLOC_MAX_TASKS;
+    const uint32_t tid = threadIdx.x;
+    float mn = INFINITY, mx = -INFINITY;
+    for (uint32_t i = tid; i < n; i += SORT_NT) {
+        const float c = cost[i];
+        if (c == c) {
+            mn = fminf(mn, c);
+            mx = fmaxf(mx, c);
+        }
+    }
+    for (int s = 16; s; s >>= 1) {
+        mn = fminf(mn, __shfl_xor_sync(GD_FULL_MASK, mn, s));
+        mx = fmaxf(mx, __shfl_xor_sync(GD_FULL_MASK, mx, s));
+    }
+    if ((tid & 31) == 0) {
+        red_mn[tid >> 5] = mn;
+        red_mx[tid >> 5] = mx;
+    }
+    for (uint32_t b = tid; b < NBUCKET; b += SORT_NT) hist[b] = 0;
+    if (tid == 0) scratch[NOALLOC_MAX_TASKS + NBUCKET] = 0;  // work-queue counter
+    __syncthreads();
+    mn = INFINITY;
+    mx = -INFINITY;
+    for (int w = 0; w < SORT_NT / 32; ++w) {
+        mn = fminf(mn, red_mn[w]);
+        mx = fmaxf(mx, red_mx[w]);
+    }
+    const float span = mx - mn;
+    const float scale = (span > 0.f && span < INFINITY) ? (float)(NBUCKET - 1) / span : 0.f;
+    for (uint32_t i = tid; i < n; i += SORT_NT) atomicAdd(&hist[cost_bucket(cost[i], mn, scale)], 1u);
+    __syncthreads();
+    if (tid < 32) {  // exclusive scan of the buckets by warp 0, 32 buckets per lane
+        uint32_t loc[NBUCKET / 32], s = 0;
+#pragma unroll
+        for (int k = 0; k < NBUCKET / 32; ++k) {
+            loc[k] = s;
+            s += hist[tid * (NBUCKET / 32) + k];
+        }
+        uint32_t inc = warp_incl_scan(s);
+        const uint32_t base = inc - s;
+#pragma unroll
+        for (int k = 0; k < NBUCKET / 32; ++k) cursor[tid * (NBUCKET / 32) + k] = base + loc[k];
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < n; i += SORT_NT) {
+        const uint32_t p = atomicAdd(&cursor[cost_bucket(cost[i], mn, scale)], 1u);
+        order[p] = i;
+    }
+}
+
+}  // namespace batch
+}  // namespace gd
+
+extern "C" gd_status_t gd_batch_decode_lpt_noalloc(const gd_task* d_tasks, uint32_t n_tasks, const float* d_cost,
+                                                   uint32_t max_lane_bytes, uint32_t blocks_per_sm,
+                                                   uint32_t* d_status, gd_stream_t stream) {
+    using namespace gd::batch;
+    if (n_tasks == 0) return GD_OK;
+    if (!d_tasks || !d_cost || n_tasks > NOALLOC_MAX_TASKS) return GD_ERR_INVALID_ARG;
+    // Set-up, once per device with that device current: the device address
+    // of the scratch array.  The first call on a device therefore makes a
+    // runtime query and should come before any stream capture.
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return GD_ERR_CUDA;
+    static std::mutex mu;
+    static uint32_t* scratch_of[64] = {};
+    static int sms_of[64] = {};
+    uint32_t* scratch;
+    int sms;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (!scratch_of[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return GD_ERR_CUDA;
+            int m = 0;
+            if (cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || m <= 0)
+                return GD_ERR_CUDA;
+            sms_of[dev] = m;
+            scratch_of[dev] = static_cast<uint32_t*>(p);
+        }
+        scratch = scratch_of[dev];
+        sms = sms_of[dev];
+    }
+    const uint32_t ws = warp_smem_bytes(max_lane_bytes);
+    const uint32_t smem = WPB * ws;
+    if (smem > 220 * 1024) return GD_ERR_UNSUPPORTED;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return GD_ERR_CUDA;
+    int occ = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, WPB * 32, smem);
+    if (occ < 1) occ = 1;
+    const uint32_t bps = blocks_per_sm ? (blocks_per_sm < (uint32_t)occ ? blocks_per_sm : (uint32_t)occ) : (uint32_t)occ;
+    lpt_sort_kernel<<<1, SORT_NT, 0, s>>>(d_cost, n_tasks, scratch);
+    if (cudaGetLastError() != cudaSuccess) return GD_ERR_CUDA;
+    batch_kernel<<<bps * (uint32_t)sms, WPB * 32, smem, s>>>(d_tasks, n_tasks, scratch,
+                                                            scratch + NOALLOC_MAX_TASKS + NBUCKET, 1,
+                                                            max_lane_bytes, ws, d_status, nullptr);
+    return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+}

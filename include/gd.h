@@ -208,6 +208,24 @@ gd_status_t gd_batch_decode(const gd_task* d_tasks, uint32_t n_tasks, const uint
 /* Number of warps gd_batch_decode runs with for these parameters. */
 uint32_t gd_batch_warps(uint32_t max_lane_bytes, uint32_t blocks_per_sm);
 
+/*
+ * No counterpart in the reference.  gd_batch_decode with longest-first
+ * placement and no memory allocated or taken from the caller beyond the
+ * listed arguments: the tasks are ordered by descending d_cost[n] (any cost
+ * estimate, e.g. gd_mlp_predict output; bucketed, so near-equal costs run in
+ * any order) and fed through the dynamic work queue.  The order array, sort
+ * buckets and queue counter live in a fixed device array inside the library
+ * (GD_BATCH_NOALLOC_MAX_TASKS tasks at most; more is GD_ERR_INVALID_ARG).
+ * Nothing needs zeroing beforehand.  The first call on a device looks up that
+ * array's address (a runtime query, with the device current) and should come
+ * before any stream capture.  Calls overlapping in time on one device share
+ * the array and race: serialise them.  d_status[n] is written per task.
+ */
+#define GD_BATCH_NOALLOC_MAX_TASKS 65536u
+gd_status_t gd_batch_decode_lpt_noalloc(const gd_task* d_tasks, uint32_t n_tasks, const float* d_cost,
+                                        uint32_t max_lane_bytes, uint32_t blocks_per_sm, uint32_t* d_status,
+                                        gd_stream_t stream);
+
 /* ------------------------------------------------------------------------
  * Learned task-cost model: FP32 MLP 16 -> 64 -> 64 -> 1 (ReLU), parameters
  * W1[16][64] | b1[64] | W2[64][64] | b2[64] | W3[64] | b3 in one float array.
