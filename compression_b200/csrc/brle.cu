@@ -6,25 +6,32 @@
 // data[ptr[c] .. ptr[c+1]) and expand to out[c*chunk_size ..].
 //
 // The reference decodes one chunk per thread (1024 threads on the whole GPU
-// for a 256 MiB column).  Here one 256-thread block decodes a chunk, 16 KiB
-// of compressed bytes (a tile) at a time:
-//   1. The tile (8 KiB) is staged in shared memory with 16-byte loads.
+// for a 256 MiB column).  Here one 256-thread block decodes a chunk, 8 KiB of
+// compressed bytes (a tile) at a time:
+//   1. The tile (+ a 160-byte halo for tokens that run past it) is staged in
+//      shared memory with 16-byte loads.
 //   2. Token starts form a chain (each token is 2..129 bytes).  Thread t owns
 //      a 32-byte segment and computes, by one backward pass over its bytes,
-//      where the chain leaves the segment for every possible entry offset
-//      (a 32-entry exit table).  One thread then follows the chain across
-//      the 256 segments with one table lookup each; the other tables make
-//      any entry O(1), so no speculation or re-walking is needed.
-//   3. Each thread walks its segment from its true entry; a block scan of
-//      output sizes places every token, and each warp packs its tokens into a
-//      list of (output offset, tile position).
-//   4. Each warp expands its output range in rounds of 32 x 64 bytes: lane l
-//      takes the 64-byte slice l of the round (equal work per lane whatever
-//      the token lengths), finds the token covering its first byte by binary
-//      search in the list, and builds aligned 16-byte vectors in registers
-//      (a vector inside one run is a single broadcast value) which it stores
-//      straight to HBM.  Bytes of 16-byte words shared with a neighbouring
-//      warp are stored bytewise.
+//      where the chain leaves the segment for every entry offset (an exit
+//      table).
+//   3. Warp w owns a 1 KiB region (32 segments).  Lane l follows the chain
+//      through the region from entry offset l of its first segment, one table
+//      lookup per segment, recording the entry of every segment.  All 32
+//      possible region entries are thus resolved in parallel.
+//   4. One thread links the 8 regions (8 lookups; an entry that a long
+//      literal carried past a region's first segment is walked through the
+//      segment tables instead), and every segment learns its true entry.
+//   5. Each thread walks its segment's tokens: output bytes, token count and
+//      validation; a block scan places every token, and each thread writes
+//      its tokens into the tile's token list (output offset, position,
+//      control byte, run byte).
+//   6. Expansion: the tile's output is cut into 64-byte slices dealt round
+//      robin to all 256 threads.  A thread finds the token covering its slice
+//      by a fixed-step binary search of the list, then builds each aligned
+//      16-byte vector by merging the pieces of the tokens that cover it (a run
+//      piece is a broadcast byte, a literal piece an unaligned 16-byte read
+//      of the staged tile), and stores it with one 16-byte store.  The few
+//      vectors shared with the neighbouring tile are stored bytewise.
 // Every read is bounded by the chunk's compressed length and every write by
 // its output size; a malformed chunk gets GD_ERR_CORRUPT / GD_ERR_OVERRUN.
 #include "gd_common.cuh"
@@ -34,31 +41,51 @@ namespace brle {
 
 constexpr int NT = 256;
 constexpr int NWARP = NT / 32;
-constexpr int SEG = 32;         // compressed bytes per thread segment
-constexpr int TILE = NT * SEG;  // compressed bytes per tile
-constexpr int HALO = 160;       // a token starting in the tile reads <= 129 more bytes
+constexpr int SEG = 32;          // compressed bytes per thread segment
+constexpr int REG = 32 * SEG;    // bytes per warp region
+constexpr int TILE = NT * SEG;   // compressed bytes per tile
+constexpr int HALO = 160;        // a token starting in the tile reads <= 128 more bytes
 constexpr uint32_t NONE = 0xffffffffu;
-constexpr uint32_t TPW = 32 * SEG / 2;  // most tokens a warp's segments can hold
-constexpr uint32_t SMEM = TILE + HALO + 16 + NT * SEG + NWARP * TPW * 6;
+constexpr uint32_t FALLBACK = 0x100u;
+constexpr uint32_t MAXTOK = TILE / 2;  // a token is >= 2 bytes
+// dynamic shared memory: staged tile (16 B front pad, alignment shift, tail
+// pad for unaligned 16-byte reads), exit tables, token list (which also holds
+// the region chains before the list is built)
+constexpr uint32_t OFF_TILE = 0;
+constexpr uint32_t TILE_BYTES = 16 + 16 + TILE + HALO + 32;
+constexpr uint32_t OFF_TBL = (TILE_BYTES + 15u) & ~15u;
+constexpr uint32_t OFF_LIST = OFF_TBL + TILE;
+constexpr uint32_t SMEM = OFF_LIST + MAXTOK * 8;
+static_assert(NWARP * 32 * 32 * 2 <= MAXTOK * 8, "region chains must fit in the token list space");
 
 __device__ __forceinline__ uint32_t tok_in(uint32_t c) { return c > 127u ? c - 126u : 2u; }
 __device__ __forceinline__ uint32_t tok_out(uint32_t c) { return c > 127u ? c - 127u : c + 3u; }
 
-__global__ void __launch_bounds__(NT) decode_kernel(const uint8_t* __restrict__ data,
-                                                    const uint64_t* __restrict__ ptr, uint32_t n_chunks,
-                                                    uint64_t chunk_size, uint8_t* __restrict__ out,
-                                                    uint64_t out_n, uint32_t* __restrict__ status) {
+// 16 bytes at any shared-memory address p (8-byte aligned reads p&~7 .. +24).
+__device__ __forceinline__ void lds16_unaligned(const uint8_t* p, uint64_t& lo, uint64_t& hi) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint64_t* q = reinterpret_cast<const uint64_t*>(a & ~(uintptr_t)7);
+    const uint32_t sh = (uint32_t)(a & 7u) * 8u;
+    const uint64_t q0 = q[0], q1 = q[1], q2 = q[2];
+    lo = sh ? (q0 >> sh) | (q1 << (64u - sh)) : q0;
+    hi = sh ? (q1 >> sh) | (q2 << (64u - sh)) : q1;
+}
+
+__global__ void __launch_bounds__(NT, 4) decode_kernel(const uint8_t* __restrict__ data,
+                                                       const uint64_t* __restrict__ ptr, uint32_t n_chunks,
+                                                       uint64_t chunk_size, uint8_t* __restrict__ out,
+                                                       uint64_t out_n, uint32_t* __restrict__ status) {
     extern __shared__ __align__(16) uint8_t s_dyn[];
-    uint8_t* s_tile = s_dyn;                          // TILE + HALO + 16
-    uint8_t* s_tbl = s_dyn + TILE + HALO + 16;        // NT x SEG exit tables, then token lists
+    uint8_t* s_tbl = s_dyn + OFF_TBL;
+    uint2* s_list = reinterpret_cast<uint2*>(s_dyn + OFF_LIST);
+    uint16_t* s_chain = reinterpret_cast<uint16_t*>(s_dyn + OFF_LIST);  // [warp][segment][lane]
     __shared__ uint32_t s_entry[NT];
-    __shared__ uint32_t s_scan[NWARP + 1];
+    __shared__ uint16_t s_rx[NWARP][32];
+    __shared__ uint32_t s_rentry[NWARP];
+    __shared__ uint64_t s_scan[NWARP + 1];
     __shared__ uint32_t s_carry;
 
     const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
-    // token list of this warp: output offsets and tile positions
-    uint32_t* tl_out = reinterpret_cast<uint32_t*>(s_tbl + NT * SEG) + wid * TPW;
-    uint16_t* tl_pos = reinterpret_cast<uint16_t*>(s_tbl + NT * SEG + NWARP * TPW * 4) + wid * TPW;
     for (uint32_t chunk = blockIdx.x; chunk < n_chunks; chunk += gridDim.x) {
         const uint64_t beg = ptr[chunk], end = ptr[chunk + 1];
         const uint64_t obase = (uint64_t)chunk * chunk_size;
@@ -74,75 +101,117 @@ __global__ void __launch_bounds__(NT) decode_kernel(const uint8_t* __restrict__ 
         uint32_t opos = 0;   // output bytes placed so far
 
         for (uint32_t t0 = 0; t0 < clen && err == ST_OK; t0 += TILE) {
+            // positions below are tile-relative; cl = chunk end in tile coordinates
+            const uint32_t cl = clen - t0;
             // ---- 1. stage compressed bytes [t0, min(clen, t0+TILE+HALO)) ----
-            // Tile byte i lives at tb[i] = s_tile[sh + i], sh = the global
-            // address mod 16, so aligned 16-byte global words land on aligned
-            // shared words; the ragged head and tail are copied bytewise.
-            const uint32_t n_ld = min(clen - t0, (uint32_t)(TILE + HALO));
+            // Tile byte i lives at tb[i], tb = s_dyn + 16 + (global address mod
+            // 16), so aligned 16-byte global words land on aligned shared words.
+            const uint32_t n_ld = min(cl, (uint32_t)(TILE + HALO));
             const uint8_t* g = src + t0;
             const uint32_t sh = (uint32_t)(reinterpret_cast<uintptr_t>(g) & 15u);
-            const uint8_t* tb = s_tile + sh;
+            uint8_t* tb = s_dyn + OFF_TILE + 16 + sh;
             {
                 uint32_t head = (16u - sh) & 15u;
                 if (head > n_ld) head = n_ld;
-                if (tid < head) s_tile[sh + tid] = g[tid];
+                if (tid < head) tb[tid] = g[tid];
                 const uint32_t nv = (n_ld - head) >> 4;
                 const uint4* gv = reinterpret_cast<const uint4*>(g + head);
-                uint4* sv = reinterpret_cast<uint4*>(s_tile + sh + head);
+                uint4* sv = reinterpret_cast<uint4*>(tb + head);
                 for (uint32_t i = tid; i < nv; i += NT) sv[i] = __ldg(gv + i);
-                for (uint32_t i = head + 16 * nv + tid; i < n_ld; i += NT) s_tile[sh + i] = g[i];
+                for (uint32_t i = head + 16 * nv + tid; i < n_ld; i += NT) tb[i] = g[i];
             }
             __syncthreads();
 
-            // ---- 2a. exit table of this thread's segment ----
-            // tbl[k] = (chain exit - S) when the chain enters at S + k; an
-            // exit is the first chain position >= lim (<= 64 + 129 - 1).
-            const uint32_t S = t0 + SEG * tid;
-            const uint32_t lim = min(S + SEG, clen);
-            uint8_t* tbl = s_tbl + tid * SEG;
-            if (S < clen) {
+            // ---- 2. exit table of this thread's segment ----
+            // s_tbl[p] = (chain exit - S) when the chain passes p in [S, lim);
+            // an exit is the first chain position >= lim (<= 31 + 129).
+            const uint32_t S = SEG * tid;
+            const uint32_t lim = min(S + SEG, cl);
+            if (S < cl) {
                 for (int32_t p = (int32_t)lim - 1; p >= (int32_t)S; --p) {
-                    const uint32_t n = (uint32_t)p + tok_in(tb[(uint32_t)p - t0]);
-                    tbl[(uint32_t)p - S] = (n >= lim) ? (uint8_t)(n - S) : tbl[n - S];
+                    const uint32_t n = (uint32_t)p + tok_in(tb[p]);
+                    s_tbl[p] = (n >= lim) ? (uint8_t)(n - S) : s_tbl[n];
                 }
             }
             __syncthreads();
 
-            // ---- 2b. follow the chain across the segments (one lookup each) ----
+            // ---- 3. chains through this warp's region, one per entry offset ----
+            {
+                const uint32_t R = REG * wid;
+                uint32_t e = R + lane;
+                uint16_t* ch = s_chain + wid * 32 * 32;
+#pragma unroll 4
+                for (uint32_t j = 0; j < 32; ++j) {
+                    const uint32_t Sj = R + SEG * j;
+                    const uint32_t lj = min(Sj + SEG, cl);
+                    uint16_t rec = 0xffff;
+                    if (e < lj) {  // e >= Sj always holds here
+                        rec = (uint16_t)e;
+                        e = Sj + s_tbl[e];
+                    }
+                    ch[j * 32 + lane] = rec;
+                }
+                s_rx[wid][lane] = (uint16_t)min(e, 0xffffu);
+            }
+            __syncthreads();
+
+            // ---- 4. link the regions ----
             if (tid == 0) {
-                uint32_t e = carry;
-                for (uint32_t t = 0; t < (uint32_t)NT; ++t) {
-                    const uint32_t St = t0 + SEG * t;
-                    if (St >= clen || e >= min(St + SEG, clen)) {
-                        s_entry[t] = NONE;  // no token starts in segment t
+                uint32_t e = carry - t0;  // < 129: the previous tile's last token ends here
+                for (uint32_t w = 0; w < (uint32_t)NWARP; ++w) {
+                    const uint32_t R = REG * w;
+                    if (R >= cl || e >= R + REG) {
+                        s_rentry[w] = NONE;
                         continue;
                     }
-                    s_entry[t] = e;
-                    e = St + s_tbl[t * SEG + (e - St)];
-                }
-                s_carry = e;
-            }
-            __syncthreads();
-
-            // ---- 3. token starts, output size, validation; scans; token list ----
-            uint32_t mask = 0;
-            uint32_t cnt = 0;
-            bool bad = false;
-            {
-                const uint32_t e = s_entry[tid];
-                if (e != NONE) {
-                    uint32_t p = e;
-                    while (p < lim) {
-                        mask |= 1u << (p - S);
-                        const uint32_t c = tb[p - t0];
-                        if (p + tok_in(c) > clen) bad = true;
-                        cnt += tok_out(c);
-                        p += tok_in(c);
+                    const uint32_t k = e - R;
+                    if (k < 32u) {
+                        s_rentry[w] = k;
+                        e = s_rx[w][k];
+                        continue;
+                    }
+                    // a long literal carried the chain past the region's first segment
+                    s_rentry[w] = FALLBACK;
+                    for (uint32_t j = 0; j < 32; ++j) {
+                        const uint32_t Sj = R + SEG * j;
+                        const uint32_t lj = min(Sj + SEG, cl);
+                        uint32_t rec = NONE;
+                        if (e >= Sj && e < lj) {
+                            rec = e;
+                            e = Sj + s_tbl[e];
+                        }
+                        s_entry[w * 32 + j] = rec;
                     }
                 }
+                s_carry = t0 + e;
             }
-            uint32_t total;
-            const uint32_t excl = block_excl_scan<NT>(cnt, s_scan, &total);
+            __syncthreads();
+            uint32_t ent;
+            {
+                const uint32_t rk = s_rentry[wid];
+                if (rk < 32u) {
+                    const uint16_t r = s_chain[wid * 32 * 32 + lane * 32 + rk];
+                    ent = (r == 0xffff) ? NONE : (uint32_t)r;
+                } else {
+                    ent = (rk == FALLBACK) ? s_entry[tid] : NONE;
+                }
+            }
+
+            // ---- 5. walk the segment: output bytes, tokens, validation ----
+            uint32_t cnt = 0, ntok = 0;
+            bool bad = false;
+            if (ent != NONE) {
+                for (uint32_t p = ent; p < lim;) {
+                    const uint32_t c = tb[p];
+                    if (p + tok_in(c) > cl) bad = true;
+                    cnt += tok_out(c);
+                    ++ntok;
+                    p += tok_in(c);
+                }
+            }
+            uint64_t tot64;
+            const uint64_t ex = block_excl_scan64<NT>(((uint64_t)ntok << 32) | cnt, s_scan, &tot64);
+            const uint32_t total = (uint32_t)tot64, ntot = (uint32_t)(tot64 >> 32);
             carry = s_carry;
             if (__syncthreads_or(bad)) {
                 err = ST_CORRUPT;
@@ -152,97 +221,76 @@ __global__ void __launch_bounds__(NT) decode_kernel(const uint8_t* __restrict__ 
                 err = ST_OVERRUN;
                 break;
             }
-            const uint32_t ntok = __popc(mask);
-            const uint32_t tinc = warp_incl_scan(ntok);
-            const uint32_t n_w = __shfl_sync(GD_FULL_MASK, tinc, 31);  // tokens of this warp
-            {
-                uint32_t j = tinc - ntok, o = opos + excl;
-                uint32_t m = mask;
-                while (m) {
-                    const uint32_t tp = S + (__ffs(m) - 1) - t0;
-                    tl_out[j] = o;
-                    tl_pos[j] = (uint16_t)tp;
-                    o += tok_out(tb[tp]);
-                    ++j;
-                    m &= m - 1;
+            if (ntok) {
+                uint32_t j = (uint32_t)(ex >> 32), o = opos + (uint32_t)ex;
+                for (uint32_t p = ent; p < lim;) {
+                    const uint32_t c = tb[p];
+                    s_list[j++] = make_uint2(o, p | (c << 16) | ((uint32_t)tb[p + 1] << 24));
+                    o += tok_out(c);
+                    p += tok_in(c);
                 }
             }
-            __syncwarp();
+            __syncthreads();
 
-            // ---- 4. merge-path expansion: 64 output bytes per lane per round ----
-            if (n_w) {
-                const uint32_t wbeg = __shfl_sync(GD_FULL_MASK, opos + excl, 0);
-                const uint32_t wend = __shfl_sync(GD_FULL_MASK, opos + excl + cnt, 31);
-                for (uint32_t r = wbeg & ~15u; r < wend; r += 32 * 64) {
-                    const uint32_t lo = max(r + 64 * lane, wbeg);
-                    const uint32_t hi = min(r + 64 * lane + 64, wend);
-                    if (lo >= hi) continue;
-                    // last token whose output starts at or before lo
-                    uint32_t a = 0, b = n_w;  // invariant: tl_out[a] <= lo < tl_out[b]
-                    while (b - a > 1) {
-                        const uint32_t m = (a + b) >> 1;
-                        if (tl_out[m] <= lo) a = m;
-                        else b = m;
-                    }
-                    uint32_t k = a;
-                    uint32_t ks = tl_out[k], kp = tl_pos[k];
-                    uint32_t kc = tb[kp];
-                    uint32_t ke = ks + tok_out(kc);
-                    for (uint32_t v0 = lo & ~15u; v0 < hi; v0 += 16) {
-                        const uint32_t x0 = max(v0, lo), x1 = min(v0 + 16, hi);
-                        while (ke <= x0) {  // advance to the token covering x0
-                            ++k;
-                            ks = ke;
-                            kp = tl_pos[k];
-                            kc = tb[kp];
-                            ke = ks + tok_out(kc);
-                        }
-                        if (aligned16 && x0 == v0 && x1 == v0 + 16 && kc <= 127u && ke >= x1) {
-                            const uint32_t rep = 0x01010101u * tb[kp + 1];
-                            *reinterpret_cast<uint4*>(dst + v0) = make_uint4(rep, rep, rep, rep);
-                            continue;
-                        }
-                        uint32_t w[4] = {0, 0, 0, 0};
-                        uint32_t x = x0;
-                        for (;;) {
-                            const uint32_t n = min(ke, x1) - x;
-                            if (kc <= 127u) {
-                                const uint32_t rep = 0x01010101u * tb[kp + 1];
+            // ---- 6. expansion: 64-byte slices of [opos, opos+total) ----
+            const uint32_t ob = opos, oe = opos + total;
+            for (uint32_t s0 = (ob & ~63u) + 64u * tid; s0 < oe; s0 += 64u * NT) {
+                const uint32_t lo = max(s0, ob), hi = min(s0 + 64u, oe);
+                if (lo >= hi) continue;
+                // last token whose output starts at or before lo
+                uint32_t a = 0;
 #pragma unroll
-                                for (uint32_t q = 0; q < 4; ++q) {
-                                    const uint32_t ql = v0 + 4 * q;
-                                    const uint32_t a0 = max(x, ql), a1 = min(x + n, ql + 4);
-                                    if (a0 < a1) {
-                                        const uint32_t nb = a1 - a0;
-                                        const uint32_t msk = (nb == 4 ? 0xffffffffu : ((1u << (8 * nb)) - 1u)) << (8 * (a0 - ql));
-                                        w[q] = (w[q] & ~msk) | (rep & msk);
-                                    }
-                                }
-                            } else {
-                                const uint8_t* lit = tb + kp + 1 + (x - ks);
-                                for (uint32_t i = 0; i < n; ++i) {
-                                    const uint32_t bo = x - v0 + i;
-                                    w[bo >> 2] |= (uint32_t)lit[i] << (8 * (bo & 3u));
-                                }
-                            }
-                            x += n;
-                            if (x >= x1) break;
-                            ++k;
+                for (uint32_t step = MAXTOK / 2; step; step >>= 1) {
+                    const uint32_t cand = a + step;
+                    if (cand < ntot && s_list[cand].x <= lo) a = cand;
+                }
+                uint32_t ks = s_list[a].x, info = s_list[a].y;
+                uint32_t ke = ks + tok_out((info >> 16) & 0xffu);
+                for (uint32_t v0 = lo & ~15u; v0 < hi; v0 += 16) {
+                    const uint32_t x0 = max(v0, lo), x1 = min(v0 + 16, hi);
+                    uint64_t acc0 = 0, acc1 = 0;
+                    uint32_t x = x0;
+                    for (;;) {
+                        if (ke <= x) {  // the previous piece ended exactly at this vector's start
+                            ++a;
                             ks = ke;
-                            kp = tl_pos[k];
-                            kc = tb[kp];
-                            ke = ks + tok_out(kc);
+                            info = s_list[a].y;
+                            ke = ks + tok_out((info >> 16) & 0xffu);
                         }
-                        if (aligned16 && x0 == v0 && x1 == v0 + 16) {
-                            *reinterpret_cast<uint4*>(dst + v0) = make_uint4(w[0], w[1], w[2], w[3]);
-                        } else {  // partial word (shared with a neighbouring warp) or unaligned output
-                            for (uint32_t y = x0; y < x1; ++y) dst[y] = (uint8_t)(w[(y - v0) >> 2] >> (8 * ((y - v0) & 3u)));
+                        const uint32_t c = (info >> 16) & 0xffu;
+                        uint64_t w0, w1;
+                        if (c <= 127u) {
+                            w0 = w1 = 0x0101010101010101ull * (info >> 24);
+                        } else {
+                            // literal byte at output position y sits at tb[pos + 1 + y - ks]
+                            lds16_unaligned(tb + (int32_t)((info & 0xffffu) + 1u + v0 - ks), w0, w1);
+                        }
+                        // keep bytes below x, take bytes from x on
+                        const uint32_t b8 = (x - v0) * 8u;
+                        const uint64_t m0 = b8 >= 64u ? ~0ull : ((1ull << b8) - 1ull);
+                        const uint64_t m1 = b8 <= 64u ? 0ull : ((1ull << (b8 - 64u)) - 1ull);
+                        acc0 = (acc0 & m0) | (w0 & ~m0);
+                        acc1 = (acc1 & m1) | (w1 & ~m1);
+                        x = min(ke, x1);
+                        if (x >= x1) break;
+                        ++a;
+                        ks = ke;
+                        info = s_list[a].y;
+                        ke = ks + tok_out((info >> 16) & 0xffu);
+                    }
+                    if (aligned16 && x0 == v0 && x1 == v0 + 16) {
+                        *reinterpret_cast<uint4*>(dst + v0) =
+                            make_uint4((uint32_t)acc0, (uint32_t)(acc0 >> 32), (uint32_t)acc1, (uint32_t)(acc1 >> 32));
+                    } else {  // a vector shared with the neighbouring tile, or unaligned output
+                        for (uint32_t y = x0; y < x1; ++y) {
+                            const uint32_t b = y - v0;
+                            dst[y] = (uint8_t)((b < 8 ? acc0 >> (8 * b) : acc1 >> (8 * (b - 8))) & 0xffu);
                         }
                     }
                 }
             }
             opos += total;
-            __syncthreads();  // tile, tables and lists are reused by the next tile
+            __syncthreads();  // tile, tables and list are reused by the next tile
         }
 
         if (err == ST_OK && (opos != want || carry != clen)) err = ST_CORRUPT;

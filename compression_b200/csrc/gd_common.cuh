@@ -67,4 +67,24 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* tmp, u
     return r;
 }
 
+// Block-wide exclusive scan of one uint64 per thread; as block_excl_scan.
+// `tmp` must hold NT/32 + 1 words.  Contains __syncthreads.
+template <int NT>
+__device__ __forceinline__ uint64_t block_excl_scan64(uint64_t v, uint64_t* tmp, uint64_t* total) {
+    const uint32_t l = lane_id(), w = threadIdx.x >> 5;
+    uint64_t inc = warp_incl_scan64(v);
+    if (l == 31) tmp[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        uint64_t x = (l < NT / 32) ? tmp[l] : 0;
+        uint64_t xi = warp_incl_scan64(x);
+        if (l < NT / 32) tmp[l] = xi - x;
+        if (l == NT / 32 - 1) tmp[NT / 32] = xi;
+    }
+    __syncthreads();
+    uint64_t r = tmp[w] + inc - v;
+    *total = tmp[NT / 32];
+    return r;
+}
+
 }  // namespace gd
