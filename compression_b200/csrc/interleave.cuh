@@ -150,12 +150,11 @@ __device__ __forceinline__ void load_lane_streams(const SegTable& T, const uint3
     const uint32_t nwl = (s_len[l] + 3) >> 2;
     const uint32_t ltmask = (1u << l) - 1u;
     uint32_t* d = reinterpret_cast<uint32_t*>(dst + sub * cap);
+    // a thread's rows only grow, so its segment index is tracked, not searched
+    uint32_t j = 0;
     for (uint32_t k = tid / NLANES; k < maxw; k += blockDim.x / NLANES) {
         if (k < nwl) {
-            uint32_t j = 0;
-#pragma unroll
-            for (uint32_t step = 16; step; step >>= 1)
-                if (j + step <= 31 && T.hi[j + step - 1] <= k) j += step;
+            while (j < 31 && T.hi[j] <= k) ++j;
             const uint32_t lo = j ? T.hi[j - 1] : 0u;
             const uint32_t off = T.base[j] + (k - lo) * 4u * (32u - j) + 4u * __popc(T.mask[j] & ltmask);
             // asynchronous 4-byte global->shared copy: all of a thread's
