@@ -175,6 +175,41 @@ def lzss_encode(raw, chunk_size: int = 64 * 1024) -> Encoded:
                    {"blk_off": blk, "col_len": col, "col_map": cmap}, {})
 
 
+def lzss_contig_encode(raw, chunk_size: int = 128 * 1024) -> Encoded:
+    """lzss::compress_gpu, contiguous container (include/lzss/lzss.h:1060-1124):
+    one token stream per chunk.  params["container"] is the whole file."""
+    b = _as_u8(raw)
+    L = lib()
+    cap = L.gd_lzss_contig_max_encoded_bytes(b.size, chunk_size)
+    cont = np.empty(cap, dtype=np.uint8)
+    n = L.gd_lzss_contig_encode(_p(b), b.size, chunk_size, _p(cont))
+    if n == 0:
+        raise ValueError("lzss contiguous encode failed")
+    cont = cont[:n].copy()
+    nc = (b.size + chunk_size - 1) // chunk_size
+    ends = cont[28:28 + 8 * nc].copy().view(np.uint64)
+    return Encoded("lzss_contig", cont[28 + 8 * nc:].copy(), b.size, nc, chunk_size, {"ends": ends},
+                   {"container": cont})
+
+
+def brle_trans_encode(raw, chunk_size: int = 4096) -> Encoded:
+    """brle_trans::compress_gpu (include/brle/brle_trans.h:563-660): flag-byte
+    byte-RLE columns in the ranked 32-column layout + side-file arrays."""
+    b = _as_u8(raw)
+    L = lib()
+    nc = (b.size + chunk_size - 1) // chunk_size
+    cap = L.gd_brle_trans_max_encoded_bytes(b.size, chunk_size)
+    data = np.empty(cap, dtype=np.uint8)
+    blk = np.empty(nc + 1, dtype=np.uint64)
+    col = np.empty(32 * nc, dtype=np.uint64)
+    cmap = np.empty(32 * nc, dtype=np.uint8)
+    n = L.gd_brle_trans_encode(_p(b), b.size, chunk_size, _p(data), _p(blk), _p(col), _p(cmap))
+    if n == 0:
+        raise ValueError("brle_trans encode failed")
+    return Encoded("brle_trans", data[:n].copy(), b.size, nc, chunk_size,
+                   {"blk_off": blk, "col_len": col, "col_map": cmap}, {})
+
+
 def deflate_encode(raw, out_off: np.ndarray, level: int = 6, mode: np.ndarray | None = None,
                    zlib_header: int = 1) -> Encoded:
     """Per-chunk zlib streams padded to 8 bytes (orig_compressor.py:44-126).
@@ -249,6 +284,12 @@ class DeviceJob:
         elif e.codec == "lzss":
             rc = L.gd_lzss_decode(ptr(self.d_data), ptr(m["blk_off"]), ptr(m["col_len"]), ptr(m["col_map"]),
                                   e.n_chunks, e.chunk_size, ptr(self.d_out), self.out_n, ptr(self.d_status), s)
+        elif e.codec == "lzss_contig":
+            rc = L.gd_lzss_contig_decode(ptr(self.d_data), ptr(m["ends"]), e.n_chunks, e.chunk_size, ptr(self.d_out),
+                                         e.n_out, ptr(self.d_status), s)
+        elif e.codec == "brle_trans":
+            rc = L.gd_brle_trans_decode(ptr(self.d_data), ptr(m["blk_off"]), ptr(m["col_len"]), ptr(m["col_map"]),
+                                        e.n_chunks, e.chunk_size, ptr(self.d_out), e.n_out, ptr(self.d_status), s)
         elif e.codec == "deflate":
             rc = L.gd_inflate(ptr(self.d_data), ptr(m["comp_off"]), ptr(m["comp_len"]), ptr(m["out_off"]),
                               e.n_chunks, e.params["zlib_header"], ptr(self.d_out), ptr(self.d_status), s)
@@ -317,6 +358,13 @@ def decode_host(enc: Encoded, keep: bool = True) -> np.ndarray:
         ptrs = (C.c_void_p * 4)(*[_p(a) for a in arrs])
         lens = np.array([a.nbytes for a in arrs], dtype=np.uint64)
         rc = L.gd_lzss_decompress(_p(enc.data), enc.data.size, ptrs, _p(lens), 4, C.byref(out), C.byref(n))
+    elif enc.codec == "lzss_contig":
+        cont = enc.params["container"]
+        rc = L.gd_lzss_contig_decompress(_p(cont), cont.size, C.byref(out), C.byref(n))
+    elif enc.codec == "brle_trans":
+        rc = L.gd_brle_trans_decompress(_p(enc.data), enc.data.size, _p(m["col_len"]), m["col_len"].nbytes,
+                                        _p(m["col_map"]), m["col_map"].nbytes, _p(m["blk_off"]), m["blk_off"].nbytes,
+                                        enc.chunk_size, C.byref(out), C.byref(n))
     elif enc.codec == "deflate":
         # reference triple: blk_offset = [total][0][cumulative], col_len = padded lengths
         blk = np.concatenate([np.array([enc.n_out], dtype=np.uint64), m["comp_off"]])

@@ -358,4 +358,93 @@ gd_status_t gd_deflate_decompress(const uint8_t* in, uint64_t in_n_bytes, const 
     return GD_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// LZSS contiguous container (replaces lzss::decompress_gpu_base,
+// include/lzss/lzss.h:1126-1188): [u64 in_n_bytes][u32 chunk_size]
+// [u32 n_chunks][u32 hist][u32 min][u32 max][u64 stream end per chunk][data].
+// ---------------------------------------------------------------------------
+gd_status_t gd_lzss_contig_decompress(const uint8_t* in, uint64_t in_n_bytes, uint8_t** out, uint64_t* out_n_bytes) {
+    if (!in || !out || !out_n_bytes || in_n_bytes < 28) return GD_ERR_INVALID_ARG;
+    uint64_t total;
+    uint32_t head[5];
+    memcpy(&total, in, 8);
+    memcpy(head, in + 8, 20);
+    const uint64_t chunk = head[0], n = head[1];
+    if (chunk == 0 || n == 0 || n != (total ? (total - 1) / chunk + 1 : 0)) return GD_ERR_CORRUPT;
+    if (head[2] != 2048 || head[3] != 3 || head[4] != 34) return GD_ERR_UNSUPPORTED;  // lzss.h:24-32
+    if (in_n_bytes < 28 + 8 * n) return GD_ERR_CORRUPT;
+    std::vector<uint64_t> ends(n);
+    memcpy(ends.data(), in + 28, 8 * n);  // not 8-byte aligned in the container
+    const uint64_t dlen = in_n_bytes - 28 - 8 * n;
+    if (ends[n - 1] > dlen) return GD_ERR_CORRUPT;
+    *out = nullptr;
+    *out_n_bytes = 0;
+    cudaStream_t s = 0;
+    uint8_t* d_data = (uint8_t*)g_pool.get(0, dlen + 16);
+    uint64_t* d_ends = (uint64_t*)g_pool.get(1, 8 * n);
+    uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
+    uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
+    if (!d_data || !d_ends || !d_out || !d_st) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(d_data, in + 28 + 8 * n, dlen, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_ends, ends.data(), 8 * n, cudaMemcpyHostToDevice, s);
+    gd_status_t r = gd_lzss_contig_decode(d_data, d_ends, (uint32_t)n, chunk, d_out, total, d_st, s);
+    if (r != GD_OK) return r;
+    uint8_t* h = (uint8_t*)pinned().get(total);
+    if (!h) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
+    r = collect(d_st, (uint32_t)n, s);
+    if (r != GD_OK) {
+        gd_free(h);
+        return r;
+    }
+    *out = h;
+    *out_n_bytes = total;
+    return GD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Byte-RLE flag-byte interleaved container (replaces
+// brle_trans::decompress_gpu, include/brle/brle_trans.h:661-791, which reads
+// col_len / col_map / blk_offset from ./input_data side files): the output is
+// n_chunks * chunk_size bytes, n_chunks = blk_n_bytes/8 - 1.
+// ---------------------------------------------------------------------------
+gd_status_t gd_brle_trans_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* col_len,
+                                     uint64_t col_n_bytes, const uint8_t* col_map, uint64_t map_n_bytes,
+                                     const uint64_t* blk_off, uint64_t blk_n_bytes, uint64_t chunk_size,
+                                     uint8_t** out, uint64_t* out_n_bytes) {
+    if (!in || !col_len || !col_map || !blk_off || !out || !out_n_bytes || blk_n_bytes < 16) return GD_ERR_INVALID_ARG;
+    const uint64_t n = blk_n_bytes / 8 - 1;
+    if (col_n_bytes < 8 * 32 * n || map_n_bytes < 32 * n) return GD_ERR_INVALID_ARG;
+    if (blk_off[n] > in_n_bytes) return GD_ERR_CORRUPT;
+    const uint64_t total = n * chunk_size;
+    *out = nullptr;
+    *out_n_bytes = 0;
+    cudaStream_t s = 0;
+    uint8_t* d_data = (uint8_t*)g_pool.get(0, in_n_bytes + 16);
+    uint64_t* d_cl = (uint64_t*)g_pool.get(1, 8 * 32 * n);
+    uint64_t* d_bo = (uint64_t*)g_pool.get(4, 8 * (n + 1));
+    uint8_t* d_map = (uint8_t*)g_pool.get(5, 32 * n);
+    uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
+    uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
+    if (!d_data || !d_cl || !d_bo || !d_map || !d_out || !d_st) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(d_data, in, in_n_bytes, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_cl, col_len, 8 * 32 * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_bo, blk_off, 8 * (n + 1), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_map, col_map, 32 * n, cudaMemcpyHostToDevice, s);
+    gd_status_t r = gd_brle_trans_decode(d_data, d_bo, d_cl, d_map, (uint32_t)n, chunk_size, d_out, total, d_st, s);
+    if (r != GD_OK) return r;
+    uint8_t* h = (uint8_t*)pinned().get(total);
+    if (!h) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
+    r = collect(d_st, (uint32_t)n, s);
+    if (r != GD_OK) {
+        gd_free(h);
+        return r;
+    }
+    *out = h;
+    *out_n_bytes = total;
+    return GD_OK;
+}
+
 }  // extern "C"

@@ -843,6 +843,97 @@ void lzss_encode_column(const uint8_t* d, uint32_t L, std::vector<uint8_t>& out)
     if (blocks != 0) out[flag_pos] = flags;
 }
 
+
+// Byte-RLE flag-byte column stream (restated from brle_trans::compress_func,
+// include/brle/brle_trans.h:437-562): maximal runs of equal bytes; a run of
+// 3 or more becomes a run item (count byte, value byte; flag bit 0), a
+// shorter run becomes that many literal items (one byte each; flag bit 1).
+// A flag byte precedes every 8 items, bits LSB first; after the 8th item of a
+// group the next flag byte is reserved even if no item follows (it stays 0).
+void brle_trans_encode_column(const uint8_t* d, uint32_t L, std::vector<uint8_t>& out) {
+    out.assign(1, 0);
+    size_t hpos = 0;
+    uint32_t items = 0;
+    uint8_t flags = 0;
+    auto item_done = [&]() {
+        out[hpos] = flags;
+        if (++items == 8) {
+            flags = 0;
+            items = 0;
+            hpos = out.size();
+            out.push_back(0);
+        }
+    };
+    uint32_t i = 0;
+    while (i < L) {
+        uint32_t j = i + 1;
+        while (j < L && d[j] == d[i]) ++j;
+        const uint32_t run = j - i;
+        if (run >= 3) {
+            out.push_back((uint8_t)run);
+            out.push_back(d[i]);
+            item_done();
+        } else {
+            for (uint32_t k = 0; k < run; ++k) {
+                flags |= (uint8_t)(1u << items);
+                out.push_back(d[i]);
+                item_done();
+            }
+        }
+        i = j;
+    }
+}
+
+// Columns of a chunk (column q = bytes 4q + 128k .. +3), encoded by `enc`,
+// ranked by descending length (ties by descending column), interleaved over
+// the active ranks in 4-byte words; blocks 128-byte aligned.  Shared by the
+// LZSS and byte-RLE flag containers.  chunk_size is a multiple of 128; a
+// short final chunk is zero padded.
+template <class Enc>
+uint64_t ranked_container(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* data, uint64_t* blk_off,
+                          uint64_t* col_len, uint8_t* col_map, Enc enc) {
+    if (n == 0 || chunk_size == 0 || chunk_size % 128) return 0;
+    uint64_t nc = (n - 1) / chunk_size + 1;
+    std::vector<std::vector<uint8_t>> cols(nc * 32);
+    parallel_for(nc, [&](uint64_t c) {
+        uint64_t len = std::min(chunk_size, n - c * chunk_size);
+        std::vector<uint8_t> chunk(chunk_size, 0);
+        memcpy(chunk.data(), in + c * chunk_size, len);
+        uint32_t L = (uint32_t)(chunk_size / 32);
+        std::vector<uint8_t> col(L);
+        for (int q = 0; q < 32; ++q) {
+            for (uint32_t k = 0; k < L / 4; ++k) memcpy(&col[4 * k], &chunk[128ull * k + 4 * q], 4);
+            enc(col.data(), L, cols[c * 32 + q]);
+        }
+    });
+    blk_off[0] = 0;
+    for (uint64_t c = 0; c < nc; ++c) {
+        int order[32];
+        for (int q = 0; q < 32; ++q) order[q] = q;
+        std::stable_sort(order, order + 32, [&](int a, int b) {
+            return cols[c * 32 + a].size() < cols[c * 32 + b].size();
+        });
+        uint64_t len[32];
+        for (int r = 0; r < 32; ++r) {
+            int q = order[31 - r];
+            col_map[c * 32 + r] = (uint8_t)q;
+            len[r] = col_len[c * 32 + r] = cols[c * 32 + q].size();
+        }
+        blk_off[c + 1] = blk_off[c] + block_bytes(len);
+    }
+    parallel_for(nc, [&](uint64_t c) {
+        uint64_t len[32];
+        const std::vector<uint8_t>* sl[32];
+        for (int r = 0; r < 32; ++r) {
+            len[r] = col_len[c * 32 + r];
+            sl[r] = &cols[c * 32 + col_map[c * 32 + r]];
+        }
+        memset(data + blk_off[c], 0, blk_off[c + 1] - blk_off[c]);
+        interleave(sl, len, data + blk_off[c]);
+    });
+    return blk_off[nc];
+}
+
 }  // namespace
 
 extern "C" {
@@ -1037,47 +1128,7 @@ uint64_t gd_lzss_max_encoded_bytes(uint64_t n, uint64_t chunk_size) {
 
 uint64_t gd_lzss_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* data, uint64_t* blk_off,
                         uint64_t* col_len, uint8_t* col_map) {
-    if (n == 0 || chunk_size == 0 || chunk_size % 128) return 0;
-    uint64_t nc = (n - 1) / chunk_size + 1;
-    std::vector<std::vector<uint8_t>> cols(nc * 32);
-    parallel_for(nc, [&](uint64_t c) {
-        uint64_t len = std::min(chunk_size, n - c * chunk_size);
-        uint64_t padded = chunk_size;  // a short final chunk is zero padded to a whole chunk
-        std::vector<uint8_t> chunk(padded, 0);
-        memcpy(chunk.data(), in + c * chunk_size, len);
-        uint32_t L = (uint32_t)(padded / 32);
-        std::vector<uint8_t> col(L);
-        for (int q = 0; q < 32; ++q) {
-            for (uint32_t k = 0; k < L / 4; ++k) memcpy(&col[4 * k], &chunk[128ull * k + 4 * q], 4);
-            lzss_encode_column(col.data(), L, cols[c * 32 + q]);
-        }
-    });
-    blk_off[0] = 0;
-    for (uint64_t c = 0; c < nc; ++c) {
-        int order[32];
-        for (int q = 0; q < 32; ++q) order[q] = q;
-        std::stable_sort(order, order + 32, [&](int a, int b) {
-            return cols[c * 32 + a].size() < cols[c * 32 + b].size();
-        });
-        uint64_t len[32];
-        for (int r = 0; r < 32; ++r) {
-            int q = order[31 - r];
-            col_map[c * 32 + r] = (uint8_t)q;
-            len[r] = col_len[c * 32 + r] = cols[c * 32 + q].size();
-        }
-        blk_off[c + 1] = blk_off[c] + block_bytes(len);
-    }
-    parallel_for(nc, [&](uint64_t c) {
-        uint64_t len[32];
-        const std::vector<uint8_t>* sl[32];
-        for (int r = 0; r < 32; ++r) {
-            len[r] = col_len[c * 32 + r];
-            sl[r] = &cols[c * 32 + col_map[c * 32 + r]];
-        }
-        memset(data + blk_off[c], 0, blk_off[c + 1] - blk_off[c]);
-        interleave(sl, len, data + blk_off[c]);
-    });
-    return blk_off[nc];
+    return ranked_container(in, n, chunk_size, data, blk_off, col_len, col_map, lzss_encode_column);
 }
 
 // ---------------------------------------------------------------------------
@@ -1130,6 +1181,59 @@ uint64_t gd_deflate_encode(const uint8_t* in, const uint64_t* out_off, uint32_t 
     }
     comp_off[n] = o;
     return o;
+}
+
+
+// ---------------------------------------------------------------------------
+// Byte-RLE flag-byte interleaved container (brle_trans::compress_gpu,
+// include/brle/brle_trans.h:563-660): the column streams of
+// brle_trans_encode_column in the ranked 32-column layout.  The reference
+// fixes the chunk at 4 KiB; any multiple of 128 is accepted here.  Writes
+// blk_off[n+1], col_len[32n] (sorted), col_map[32n] (rank -> column).
+// ---------------------------------------------------------------------------
+uint64_t gd_brle_trans_max_encoded_bytes(uint64_t n, uint64_t chunk_size) {
+    uint64_t nc = n ? (n - 1) / chunk_size + 1 : 0;
+    return nc * (chunk_size + chunk_size / 8 + 32 * 8 + 256);
+}
+
+uint64_t gd_brle_trans_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* data, uint64_t* blk_off,
+                              uint64_t* col_len, uint8_t* col_map) {
+    return ranked_container(in, n, chunk_size, data, blk_off, col_len, col_map, brle_trans_encode_column);
+}
+
+// ---------------------------------------------------------------------------
+// LZSS contiguous container (lzss::compress_gpu, include/lzss/lzss.h:1060-1124):
+//   [u64 in_n_bytes][u32 chunk_size][u32 n_chunks][u32 2048][u32 3][u32 34]
+//   [u64 end offset of every chunk's stream in the data][data]
+// chunk c = input bytes [c*chunk_size, ..) (the last may be short) tokenised
+// by the same find_match grammar as one LZSS column.
+// ---------------------------------------------------------------------------
+uint64_t gd_lzss_contig_max_encoded_bytes(uint64_t n, uint64_t chunk_size) {
+    uint64_t nc = n ? (n - 1) / chunk_size + 1 : 0;
+    return 28 + 8 * nc + nc * (chunk_size + chunk_size / 8 + 16);
+}
+
+uint64_t gd_lzss_contig_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* out) {
+    if (n == 0 || chunk_size == 0 || chunk_size > 0xffffffffull) return 0;
+    const uint64_t nc = (n - 1) / chunk_size + 1;
+    if (nc > 0xffffffffull) return 0;
+    std::vector<std::vector<uint8_t>> parts(nc);
+    parallel_for(nc, [&](uint64_t c) {
+        const uint64_t len = std::min(chunk_size, n - c * chunk_size);
+        lzss_encode_column(in + c * chunk_size, (uint32_t)len, parts[c]);
+    });
+    const uint32_t head[5] = {(uint32_t)chunk_size, (uint32_t)nc, 2048u, 3u, 34u};
+    memcpy(out, &n, 8);
+    memcpy(out + 8, head, 20);
+    uint64_t* lens = reinterpret_cast<uint64_t*>(out + 28);
+    uint8_t* data = out + 28 + 8 * nc;
+    uint64_t pos = 0;
+    for (uint64_t c = 0; c < nc; ++c) {
+        memcpy(data + pos, parts[c].data(), parts[c].size());
+        pos += parts[c].size();
+        memcpy(&lens[c], &pos, 8);  // the header is 28 bytes: lens are not 8-byte aligned
+    }
+    return 28 + 8 * nc + pos;
 }
 
 }  // extern "C"

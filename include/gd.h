@@ -129,6 +129,30 @@ gd_status_t gd_inflate_ordered(const uint8_t* d_data, const uint64_t* d_comp_off
                                uint32_t* d_status, const uint32_t* d_order, gd_stream_t stream);
 
 /*
+ * LZSS, contiguous container (one token stream per chunk, not interleaved).
+ * Replaces lzss::kernel_decompress(lens) / decompress_func
+ * (include/lzss/lzss.h:234-305, :1014-1020).  Chunk c's stream is
+ * d_data[d_ends[c-1] .. d_ends[c]) (d_ends = the container's cumulative
+ * stream ends, d_ends[-1] = 0) and decodes to d_out[c*chunk_size ..]; the
+ * last chunk to out_n_bytes - c*chunk_size bytes.
+ */
+gd_status_t gd_lzss_contig_decode(const uint8_t* d_data, const uint64_t* d_ends, uint32_t n_chunks,
+                                  uint64_t chunk_size, uint8_t* d_out, uint64_t out_n_bytes,
+                                  uint32_t* d_status, gd_stream_t stream);
+
+/*
+ * Byte-RLE flag-byte container, 32-column ranked interleave.
+ * Replaces brle_trans::decompress_func (include/brle/brle_trans.h:72-202).
+ * d_blk_off[n+1], d_col_len[32n] (stream bytes per rank, sorted
+ * descending), d_col_map[32n] (rank -> column).  chunk_size: a multiple of
+ * 128 up to 8192 (the reference fixes 4096, brle_trans.h:26).
+ */
+gd_status_t gd_brle_trans_decode(const uint8_t* d_data, const uint64_t* d_blk_off, const uint64_t* d_col_len,
+                                 const uint8_t* d_col_map, uint32_t n_chunks, uint64_t chunk_size,
+                                 uint8_t* d_out, uint64_t out_n_bytes, uint32_t* d_status,
+                                 gd_stream_t stream);
+
+/*
  * cuDF-compatible inflate interface (layouts of gpu_inflate_input_s and
  * gpu_inflate_status_s, include/cudf_deflate.cuh:236-250).
  * Replaces cudf::io::gpuinflate (include/cudf_deflate.cuh:1399-1407).
@@ -284,6 +308,19 @@ gd_status_t gd_deflate_decompress(const uint8_t* in, uint64_t in_n_bytes, const 
                                   uint64_t col_n_bytes, const uint64_t* blk_offset, uint64_t blk_n_bytes,
                                   uint64_t chunk_size, uint8_t** out, uint64_t* out_n_bytes);
 
+/* lzss::decompress_gpu_base (include/lzss/lzss.h:1126-1188): in = the whole
+ * contiguous container [u64 in_n_bytes][u32 chunk_size][u32 n_chunks]
+ * [u32 2048][u32 3][u32 34][u64 stream end per chunk][data]. */
+gd_status_t gd_lzss_contig_decompress(const uint8_t* in, uint64_t in_n_bytes, uint8_t** out, uint64_t* out_n_bytes);
+
+/* brle_trans::decompress_gpu (include/brle/brle_trans.h:661-791), with the
+ * arrays of its side files ./input_data/{col_len,col_map,blk_offset}.bin
+ * passed in; the output is (blk_n_bytes/8 - 1) * chunk_size bytes. */
+gd_status_t gd_brle_trans_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* col_len,
+                                     uint64_t col_n_bytes, const uint8_t* col_map, uint64_t map_n_bytes,
+                                     const uint64_t* blk_off, uint64_t blk_n_bytes, uint64_t chunk_size,
+                                     uint8_t** out, uint64_t* out_n_bytes);
+
 /* ------------------------------------------------------------------------
  * Encoders and generators (host; produce the containers above)
  * ------------------------------------------------------------------------ */
@@ -312,6 +349,15 @@ uint64_t gd_lzss_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint
                         uint64_t* blk_off, uint64_t* col_len, uint8_t* col_map);
 /* lzss::compress_func on one stream (include/lzss/lzss_cpu.h:540-655). */
 uint64_t gd_lzss_encode_stream(const uint8_t* in, uint32_t n, uint8_t* out, uint64_t cap);
+
+uint64_t gd_lzss_contig_max_encoded_bytes(uint64_t n, uint64_t chunk_size);
+/* lzss::compress_gpu, contiguous container (include/lzss/lzss.h:1060-1124). */
+uint64_t gd_lzss_contig_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* out);
+
+uint64_t gd_brle_trans_max_encoded_bytes(uint64_t n, uint64_t chunk_size);
+/* brle_trans::compress_gpu (include/brle/brle_trans.h:563-660). */
+uint64_t gd_brle_trans_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* data,
+                              uint64_t* blk_off, uint64_t* col_len, uint8_t* col_map);
 
 uint64_t gd_deflate_max_encoded_bytes(const uint64_t* out_off, uint32_t n);
 /* zlib_chunk_compress (orig_compressor.py:44-126) with per-chunk sizes. */

@@ -546,6 +546,143 @@ int gdo_lzss_decode(const uint8_t* data, uint64_t data_len, const uint64_t* blk_
 }
 
 /* ------------------------------------------------------------------------ */
+/* LZSS, contiguous container                                                */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * lzss::decompress_gpu_base container (include/lzss/lzss.h:1126-1188):
+ * [u64 in_n_bytes][u32 chunk_size][u32 n_chunks][u32 hist][u32 min][u32 max]
+ * [u64 end of every chunk's stream][data].  Each chunk is decoded as
+ * lzss::decompress_func (lzss.h:234-305) does: flag byte, then up to 8 tokens
+ * while compressed bytes remain (literal = 1 byte, match = 2-byte v with
+ * length (v & 31) + 3 and offset v >> 5 back in the chunk's own output).
+ * Chunk c's output is bytes [c*chunk_size, ..) (the last chunk may be short).
+ */
+int gdo_lzss_contig_decode(const uint8_t* in, uint64_t in_len, uint8_t* out, uint64_t out_cap) {
+    if (in_len < 28) return GDO_CORRUPT;
+    uint64_t n;
+    uint32_t h[5];
+    memcpy(&n, in, 8);
+    memcpy(h, in + 8, 20);
+    const uint64_t chunk = h[0], nc = h[1];
+    if (chunk == 0 || n > out_cap || nc != (n ? (n - 1) / chunk + 1 : 0)) return GDO_CORRUPT;
+    if (in_len < 28 + 8 * nc) return GDO_CORRUPT;
+    const uint8_t* data = in + 28 + 8 * nc;
+    const uint64_t dlen = in_len - 28 - 8 * nc;
+    uint64_t beg = 0;
+    for (uint64_t c = 0; c < nc; ++c) {
+        uint64_t end;
+        memcpy(&end, in + 28 + 8 * c, 8);
+        if (end < beg || end > dlen) return GDO_CORRUPT;
+        const uint8_t* s = data + beg;
+        const uint64_t sl = end - beg;
+        uint8_t* o = out + c * chunk;
+        const uint64_t want = n - c * chunk < chunk ? n - c * chunk : chunk;
+        uint64_t p = 0, q = 0;
+        while (p < sl) {
+            uint8_t flags = s[p++];
+            for (int i = 0; i < 8 && p < sl; ++i, flags >>= 1) {
+                if (flags & 1) {
+                    if (q >= want) return GDO_OVERRUN;
+                    o[q++] = s[p++];
+                } else {
+                    if (p + 2 > sl) return GDO_CORRUPT;
+                    uint32_t v = (uint32_t)s[p] | ((uint32_t)s[p + 1] << 8);
+                    p += 2;
+                    uint32_t len = (v & 31) + 3, off = v >> 5;
+                    if (off == 0 || off > q) return GDO_CORRUPT;
+                    if (q + len > want) return GDO_OVERRUN;
+                    for (uint32_t j = 0; j < len; ++j, ++q) o[q] = o[q - off];
+                }
+            }
+        }
+        if (q != want) return GDO_CORRUPT;
+        beg = end;
+    }
+    return GDO_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Byte-RLE, flag-byte interleaved container                                 */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * One column stream of brle_trans (restates brle_trans::decompress_func,
+ * include/brle/brle_trans.h:72-202): a flag byte, then 8 items, flag bits
+ * LSB first; bit 1 = one literal byte, bit 0 = a count byte then a value
+ * byte written count times.  After the 8th item the next byte is a flag
+ * byte again (a reserved trailing one carries no items).  The column must
+ * produce exactly col_bytes bytes.
+ */
+static int brle_trans_decode_column(const uint8_t* s, uint64_t s_len, uint8_t* col, uint64_t col_bytes) {
+    uint64_t p = 0, o = 0;
+    uint32_t block = 0, head = 0;
+    while (p < s_len) {
+        uint8_t v = s[p++];
+        if (block == 0) {
+            head = v;
+            block = 1;
+            continue;
+        }
+        const uint32_t lit = head & 1;
+        head >>= 1;
+        if (++block == 9) block = 0;
+        if (lit) {
+            if (o >= col_bytes) return GDO_OVERRUN;
+            col[o++] = v;
+        } else {
+            if (p >= s_len) return GDO_CORRUPT;  /* a count without its value byte */
+            const uint8_t x = s[p++];
+            if (o + v > col_bytes) return GDO_OVERRUN;
+            for (uint32_t k = 0; k < v; ++k) col[o++] = x;
+        }
+    }
+    return o == col_bytes ? GDO_OK : GDO_CORRUPT;
+}
+
+/*
+ * Whole-container decode (brle_trans::decompress_gpu, brle_trans.h:661-791):
+ * blk_off[n+1], col_len[32n] (sorted descending), col_map[32n] (rank ->
+ * column); column q of chunk c owns output bytes c*chunk_size + 4q + 128k
+ * .. +3 (brle_trans.h:107-119,146-159).
+ */
+int gdo_brle_trans_decode(const uint8_t* data, uint64_t data_len, const uint64_t* blk_off,
+                          const uint64_t* col_len, const uint8_t* col_map, uint32_t n_chunks,
+                          uint64_t chunk_size, uint8_t* out, uint64_t out_total) {
+    if (chunk_size == 0 || chunk_size % 128) return GDO_INVALID;
+    uint64_t col_bytes = chunk_size / 32;
+    uint8_t* col = (uint8_t*)malloc(col_bytes);
+    uint8_t* tmp = (uint8_t*)malloc(chunk_size);
+    uint8_t* ranks[32];
+    uint64_t cap = 0;
+    for (uint64_t i = 0; i < 32ull * n_chunks; ++i)
+        if (col_len[i] + 8 > cap) cap = col_len[i] + 8;
+    for (int t = 0; t < 32; ++t) ranks[t] = (uint8_t*)calloc(cap, 1);
+    int rc = GDO_OK;
+    for (uint32_t c = 0; c < n_chunks && rc == GDO_OK; ++c) {
+        if (blk_off[c] > data_len) { rc = GDO_CORRUPT; break; }
+        rc = deinterleave(data + blk_off[c], data_len - blk_off[c], col_len + 32ull * c, ranks);
+        for (int r = 0; r < 32 && rc == GDO_OK; ++r) {
+            uint32_t q = col_map[32ull * c + r];
+            if (q >= 32) { rc = GDO_CORRUPT; break; }
+            rc = brle_trans_decode_column(ranks[r], col_len[32ull * c + r], col, col_bytes);
+            for (uint64_t k = 0; k < col_bytes / 4 && rc == GDO_OK; ++k)
+                memcpy(tmp + 128 * k + 4 * q, col + 4 * k, 4);
+        }
+        if (rc) break;
+        uint64_t base = (uint64_t)c * chunk_size;
+        if (base < out_total) {
+            uint64_t n = out_total - base < chunk_size ? out_total - base : chunk_size;
+            memcpy(out + base, tmp, n);
+        }
+    }
+    for (int t = 0; t < 32; ++t) free(ranks[t]);
+    free(col);
+    free(tmp);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Deflate / zlib                                                           */
 /* ------------------------------------------------------------------------ */
 

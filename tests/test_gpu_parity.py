@@ -198,3 +198,62 @@ def test_reference_streams_on_gpu(cuda):
                    {"blk_off": np.array([0, blk.size], np.uint64), "col_len": cl}, {"read_unit": 32})
     st, out = _gpu(e, cuda)
     assert (st == 0).all() and np.array_equal(out, vals.view(np.uint8))
+
+
+# ---------------------------------------------------------------------------
+# LZSS contiguous container and byte-RLE flag-byte container
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("n,chunk", [(1, 1024), (5000, 4096), (3 * 65536, 65536), (1 << 20, 128 * 1024),
+                                     (700001, 128 * 1024)])
+def test_lzss_contig(cuda, n, chunk):
+    raw = cc.gen_markov_copy(n, n, 4096)
+    _parity(cc.lzss_contig_encode(raw, chunk), raw, cuda)
+
+
+def test_lzss_contig_patterns(cuda):
+    rng = np.random.default_rng(2)
+    for raw in [np.zeros(200000, np.uint8), rng.integers(0, 256, 200000).astype(np.uint8),
+                np.tile(np.arange(11, dtype=np.uint8), 20000)]:
+        _parity(cc.lzss_contig_encode(raw, 65536), raw, cuda)
+
+
+@pytest.mark.parametrize("n,chunk", [(128, 128), (4096 * 300, 4096), (4096 * 7 + 1000, 4096), (8192 * 33, 8192),
+                                     (1024 * 77, 1024)])
+def test_brle_trans(cuda, n, chunk):
+    raw = cc.gen_brle_bytes(n + chunk, n)
+    _parity(cc.brle_trans_encode(raw, chunk), raw, cuda)
+
+
+def test_brle_trans_patterns(cuda):
+    rng = np.random.default_rng(4)
+    for raw in [np.zeros(64 * 4096, np.uint8), rng.integers(0, 256, 64 * 4096).astype(np.uint8),
+                np.repeat(rng.integers(0, 4, 32768), 8).astype(np.uint8)]:
+        _parity(cc.brle_trans_encode(raw, 4096), raw, cuda)
+
+
+def test_new_containers_host_api(cuda):
+    raw = cc.gen_markov_copy(8, 5 * 65536 + 333, 4096)
+    assert np.array_equal(cc.decode_host(cc.lzss_contig_encode(raw, 65536)), raw)
+    raw2 = cc.gen_brle_bytes(9, 4096 * 40)
+    assert np.array_equal(cc.decode_host(cc.brle_trans_encode(raw2, 4096)), raw2)
+
+
+def test_new_containers_corrupt(cuda):
+    raw = cc.gen_markov_copy(5, 200000, 4096)
+    e = cc.lzss_contig_encode(raw, 8192)
+    e.data[0] ^= 1  # chunk 0's first token becomes a match with no history
+    _expect_error(e, cuda)
+    e = cc.lzss_contig_encode(raw, 8192)
+    e.meta["ends"][3] -= 1  # chunk 3 truncated, chunk 4 starts one byte early
+    _expect_error(e, cuda)
+    r2 = cc.gen_brle_bytes(6, 4096 * 8)
+    e2 = cc.brle_trans_encode(r2, 4096)
+    e2.meta["col_len"][0] -= 1  # truncated rank-0 stream
+    _expect_error(e2, cuda)
+    e3 = cc.brle_trans_encode(r2, 4096)
+    e3.meta["col_map"][1] = e3.meta["col_map"][0]  # not a permutation
+    _expect_error(e3, cuda)
+    e4 = cc.brle_trans_encode(r2, 4096)
+    e4.meta["col_len"][32] = 10_000  # longer than any valid column stream
+    _expect_error(e4, cuda)

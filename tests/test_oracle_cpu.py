@@ -104,3 +104,75 @@ def test_mixed_batch_items_roundtrip():
     for it in items:
         rc, out = oracle.decode(it.enc)
         assert rc == 0 and np.array_equal(out, it.raw), it.codec
+
+
+@pytest.mark.parametrize("n,chunk", [(1, 1024), (5000, 4096), (3 * 65536, 65536), (300000, 65536)])
+def test_lzss_contig_roundtrip(n, chunk):
+    raw = cc.gen_markov_copy(n, n, 4096)
+    e = cc.lzss_contig_encode(raw, chunk)
+    cont = e.params["container"]
+    # header: in_n_bytes, chunk_size, n_chunks, history, min and max match (lzss.h:1107-1113)
+    assert int(cont[:8].view(np.uint64)[0]) == n
+    assert list(cont[8:28].view(np.uint32)) == [chunk, e.n_chunks, 2048, 3, 34]
+    _roundtrip(e, raw)
+
+
+def test_lzss_contig_chunk_streams_are_column_streams():
+    # every chunk's stream is the reference grammar's tokenisation of that chunk
+    raw = cc.gen_markov_copy(31, 3 * 8192 + 77, 4096)
+    e = cc.lzss_contig_encode(raw, 8192)
+    L = cc.lib()
+    beg = 0
+    for c in range(e.n_chunks):
+        part = raw[c * 8192:(c + 1) * 8192].copy()
+        buf = np.zeros(part.size * 2 + 64, np.uint8)
+        n = L.gd_lzss_encode_stream(part.ctypes.data, part.size, buf.ctypes.data, buf.size)
+        end = int(e.meta["ends"][c])
+        assert np.array_equal(e.data[beg:end], buf[:n])
+        beg = end
+
+
+@pytest.mark.parametrize("n,chunk", [(128, 128), (4096 * 50, 4096), (4096 * 7 + 1000, 4096), (8192 * 3, 8192)])
+def test_brle_trans_roundtrip(n, chunk):
+    raw = cc.gen_brle_bytes(n + chunk, n)
+    _roundtrip(cc.brle_trans_encode(raw, chunk), raw)
+
+
+def test_brle_trans_patterns():
+    rng = np.random.default_rng(4)
+    for raw in [np.zeros(4 * 4096, np.uint8), rng.integers(0, 256, 4 * 4096).astype(np.uint8),
+                np.repeat(rng.integers(0, 4, 2048), 8).astype(np.uint8)]:
+        e = cc.brle_trans_encode(raw, 4096)
+        _roundtrip(e, raw)
+    # an all-zero column is one run item: flag byte, count 128, value
+    e = cc.brle_trans_encode(np.zeros(4096, np.uint8), 4096)
+    assert (e.meta["col_len"] == 3).all()
+    w = e.data[:128].reshape(32, 4)  # one word row: rank r's word 0 at bytes 4r..4r+3
+    assert (w[:, :3] == [0, 128, 0]).all()
+
+
+def test_brle_trans_column_grammar():
+    # column 0 of a chunk: runs of 5 x 7, then 2 x 9 (literals), then 3 x 1
+    col = np.array([7] * 5 + [9, 9] + [1] * 3 + [4] * 118, np.uint8)
+    raw = np.zeros(4096, np.uint8)
+    for k in range(32):
+        raw[128 * k:128 * k + 4] = col[4 * k:4 * k + 4]
+    e = cc.brle_trans_encode(raw, 4096)
+    r = int(np.nonzero(e.meta["col_map"][:32] == 0)[0][0])
+    assert int(e.meta["col_len"][r]) == 1 + 2 + 1 + 1 + 2 + 2
+    rc, out = oracle.decode(e)
+    assert rc == 0 and np.array_equal(out, raw)
+
+
+def test_new_containers_reject_corruption():
+    raw = cc.gen_markov_copy(5, 20000, 4096)
+    e = cc.lzss_contig_encode(raw, 8192)
+    cont = e.params["container"]
+    cont[28 + 8 * e.n_chunks] ^= 1  # chunk 0's first token becomes a match with no history
+    rc, _ = oracle.decode(e)
+    assert rc != 0
+    r2 = cc.gen_brle_bytes(6, 8192)
+    e2 = cc.brle_trans_encode(r2, 4096)
+    e2.meta["col_len"][0] -= 1  # truncated rank-0 stream
+    rc, _ = oracle.decode(e2)
+    assert rc != 0
