@@ -124,6 +124,48 @@ inline int decompress_gpu(const uint8_t* const in, const uint64_t in_n_bytes, co
 }
 }  // namespace lzss
 
+// include/lzss/lzss.h:1126-1188 (contiguous container)
+namespace lzss {
+inline void decompress_gpu_base(const uint8_t* const in, uint8_t** out, const uint64_t in_n_bytes,
+                                uint64_t* out_n_bytes) {
+    uint8_t* p = nullptr;
+    uint64_t n = 0;
+    const gd_status_t rc = gd_lzss_contig_decompress(in, in_n_bytes, &p, &n);
+    gd_compat_detail::report(rc, "lzss::decompress_gpu_base");
+    *out = rc == GD_OK ? gd_compat_detail::adopt(p, n) : nullptr;
+    *out_n_bytes = rc == GD_OK ? n : 0;
+}
+}  // namespace lzss
+
+// include/brle/brle_trans.h:661-791: metadata from the side files the
+// reference's compress_gpu writes (./input_data/{col_len,col_map,blk_offset}.bin),
+// 4 KiB chunks.
+namespace brle_trans {
+inline void decompress_gpu(const uint8_t* const in, uint8_t** out, const uint64_t in_n_bytes, uint64_t* out_n_bytes) {
+    std::vector<uint64_t> col, blk;
+    *out = nullptr;
+    *out_n_bytes = 0;
+    std::ifstream fm("./input_data/col_map.bin", std::ios::binary | std::ios::ate);
+    if (!gd_compat_detail::read_file("./input_data/col_len.bin", col) ||
+        !gd_compat_detail::read_file("./input_data/blk_offset.bin", blk) || !fm) {
+        std::fprintf(stderr, "Fatal Error: Col Len read error\n");
+        return;
+    }
+    std::vector<uint8_t> map((size_t)fm.tellg());
+    fm.seekg(0);
+    fm.read(reinterpret_cast<char*>(map.data()), (std::streamsize)map.size());
+    uint8_t* p = nullptr;
+    uint64_t n = 0;
+    const gd_status_t rc = gd_brle_trans_decompress(in, in_n_bytes, col.data(), col.size() * 8, map.data(),
+                                                    map.size(), blk.data(), blk.size() * 8, 4096, &p, &n);
+    gd_compat_detail::report(rc, "brle_trans::decompress_gpu");
+    if (rc == GD_OK) {
+        *out = gd_compat_detail::adopt(p, n);
+        *out_n_bytes = n;
+    }
+}
+}  // namespace brle_trans
+
 // include/zlib/zlib.h:966-1082
 namespace deflate {
 template <typename READ_COL_TYPE, size_t WRITE_COL_LEN, uint16_t queue_depth, uint8_t NUM_SUBCHUNKS,

@@ -33,3 +33,41 @@ def test_device_api_rejects_bad_arguments_without_gpu():
     assert L.gd_rlev2_decode(1, 1, 1, 1, 256 * 1024, 0, 1, 10, 0, None, None) == 5
     assert L.gd_lzss_decode(1, 1, 1, 1, 2, 65536, 16, 1000, None, None) == 1  # out != n*chunk
     assert L.gd_inflate(3, 1, 1, 1, 1, 1, 1, None, None) == 1  # unaligned data
+
+
+def test_compat_header_compiles_and_links(tmp_path):
+    # a reference-style caller: the reference's namespaced calls from
+    # include/gd_compat.hpp, linked against libgd.so (compiled, not run)
+    import shutil
+    import subprocess
+    from pathlib import Path
+    gxx = shutil.which("g++")
+    if gxx is None:
+        import pytest
+        pytest.skip("no g++")
+    root = Path(_lib.__file__).resolve().parent.parent
+    src = tmp_path / "caller.cpp"
+    src.write_text(r'''
+#include "gd_compat.hpp"
+int main(int argc, char**) {
+    uint8_t* out = nullptr; uint64_t n = 0;
+    if (argc > 5) {
+        brle::decompress_gpu(nullptr, &out, 0, &n);
+        rle_v1::decompress_gpu<uint64_t, uint8_t, uint32_t, 2>(nullptr, &out, 0, &n, 128, 128 * 1024);
+        uint64_t* o64 = nullptr; uint64_t bo[2] = {0, 0}, cl[32] = {};
+        rlev2::decompress_gpu<32, 4, uint64_t>(nullptr, 0, 1, bo, cl, o64, n, 256 * 1024);
+        lzss::decompress_gpu(nullptr, 0, nullptr, nullptr, 4, &out, &n);
+        lzss::decompress_gpu_base(nullptr, &out, 0, &n);
+        brle_trans::decompress_gpu(nullptr, &out, 0, &n);
+        deflate::decompress_gpu<uint64_t, 8, 2, 1>(nullptr, &out, 0, &n, cl, 8, bo, 16, 65536);
+        cudf::io::gpuinflate(nullptr, nullptr, 0, 1);
+    }
+    return 0;
+}
+''')
+    exe = tmp_path / "caller"
+    lib_dir = root / "compression_b200"
+    r = subprocess.run([gxx, "-std=c++17", f"-I{root / 'include'}", str(src), f"-L{lib_dir}", "-lgd",
+                        f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert subprocess.run([str(exe)]).returncode == 0
