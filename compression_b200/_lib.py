@@ -39,6 +39,8 @@ SIGNATURES = {
     "gd_batch_decode": (i32, [vp, u32, vp, i32, u32, u32, vp, vp, vp, vp]),
     "gd_batch_warps": (u32, [u32, u32]),
     "gd_batch_decode_lpt_noalloc": (i32, [vp, u32, vp, u32, u32, vp, vp]),
+    "gd_tune_set": (i32, [i32, i32]),
+    "gd_tune_get": (i32, [i32]),
     "gd_mlp_num_params": (u32, []),
     "gd_mlp_predict": (i32, [vp, vp, u32, vp, vp]),
     "gd_mlp_train_step": (i32, [vp, vp, vp, vp, vp, vp, u32, C.c_float, C.c_float, C.c_float, C.c_float, u32, vp,

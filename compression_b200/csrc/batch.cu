@@ -110,7 +110,7 @@ __device__ uint32_t run_task(const gd_task& t, uint32_t max_lane, uint8_t* ws) {
         case GD_CODEC_DEFLATE: {
             if (t.src_len > 0xffffffffull || t.dst_len > 0xffffffffull) return ST_INVALID;
             uint32_t fin = 0;
-            const uint32_t e = infl::stream_warp(t.src, (uint32_t)t.src_len, t.dst, (uint32_t)t.dst_len,
+            const uint32_t e = infl::stream_warp<0>(t.src, (uint32_t)t.src_len, t.dst, (uint32_t)t.dst_len,
                                                  (int)t.param, *reinterpret_cast<infl::WarpSmem*>(ws), &fin);
             return (e == ST_OK && fin != (uint32_t)t.dst_len) ? (uint32_t)ST_CORRUPT : e;
         }

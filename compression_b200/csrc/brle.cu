@@ -313,7 +313,8 @@ extern "C" gd_status_t gd_brle_decode(const uint8_t* d_data, const uint64_t* d_p
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     uint32_t grid = n_chunks;
-    const uint32_t cap = (uint32_t)sms * 8;
+    const int bps = gd_tune_get(GD_TUNE_BRLE_BLOCKS_PER_SM);
+    const uint32_t cap = (uint32_t)sms * (bps > 0 ? (uint32_t)bps : 8u);
     if (grid > cap) grid = cap;
     constexpr uint32_t smem = gd::brle::SMEM;
     static bool attr = false;

@@ -44,22 +44,25 @@ struct CudfChunks {
     }
 };
 
-template <class Chunks>
-__global__ void __launch_bounds__(WPB * 32) inflate_kernel(Chunks ch, uint32_t n_chunks, int zlib_hdr,
-                                                          const uint32_t* __restrict__ order) {
+// NW warps per block, one stream per warp; WIN: output window (see
+// WarpSmemT).  Blocks are handed out by the hardware in launch order, so
+// `order` (longest first, say) is also the order streams start in.
+template <class Chunks, uint32_t WIN, int NW>
+__global__ void __launch_bounds__(NW * 32) inflate_kernel(Chunks ch, uint32_t n_chunks, int zlib_hdr,
+                                                         const uint32_t* __restrict__ order) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     const uint32_t wid = threadIdx.x >> 5;
-    const uint32_t slot = blockIdx.x * WPB + wid;
+    const uint32_t slot = blockIdx.x * NW + wid;
     if (slot >= n_chunks) return;
     const uint32_t chunk = order ? order[slot] : slot;
-    WarpSmem& S = *reinterpret_cast<WarpSmem*>(smem_raw + wid * sizeof(WarpSmem));
+    WarpSmemT<WIN>& S = *reinterpret_cast<WarpSmemT<WIN>*>(smem_raw + wid * sizeof(WarpSmemT<WIN>));
     const uint8_t* src;
     uint8_t* dst;
     uint64_t clen64, olen64;
     uint32_t err = ch.get(chunk, src, clen64, dst, olen64) ? ST_OK : ST_CORRUPT;
     if (olen64 > 0xffffffffull || clen64 > 0xffffffffull) err = ST_CORRUPT;
     uint32_t fin = 0;
-    if (err == ST_OK) err = stream_warp(src, (uint32_t)clen64, dst, (uint32_t)olen64, zlib_hdr, S, &fin);
+    if (err == ST_OK) err = stream_warp<WIN>(src, (uint32_t)clen64, dst, (uint32_t)olen64, zlib_hdr, S, &fin);
     if (err == ST_OK && Chunks::exact && fin != (uint32_t)olen64) err = ST_CORRUPT;
     if (lane_id() == 0) ch.put(chunk, err, err == ST_OK ? fin : 0);
 }
@@ -77,18 +80,31 @@ __global__ void copy_uncompressed_kernel(const gd_inflate_input* in, int count) 
     for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) d[i] = s[i];
 }
 
-template <class Chunks>
-gd_status_t launch_inflate(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32_t* order, cudaStream_t s) {
+template <class Chunks, uint32_t WIN, int NW>
+gd_status_t launch_cfg(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32_t* order, cudaStream_t s) {
     using namespace gd::infl;
-    const uint32_t smem = WPB * (uint32_t)sizeof(WarpSmem);
+    const uint32_t smem = NW * (uint32_t)sizeof(WarpSmemT<WIN>);
     static bool attr_set = false;  // benign race: the attribute call is idempotent
     if (!attr_set) {
-        cudaFuncSetAttribute(inflate_kernel<Chunks>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (cudaFuncSetAttribute(inflate_kernel<Chunks, WIN, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem) != cudaSuccess)
+            return GD_ERR_CUDA;
         attr_set = true;
     }
-    const uint32_t grid = (n + WPB - 1) / WPB;
-    inflate_kernel<Chunks><<<grid, WPB * 32, smem, s>>>(ch, n, zlib_hdr, order);
+    const uint32_t grid = (n + NW - 1) / NW;
+    inflate_kernel<Chunks, WIN, NW><<<grid, NW * 32, smem, s>>>(ch, n, zlib_hdr, order);
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+}
+
+// Launch configuration (GD_TUNE_INFLATE_VARIANT): 0 = 32 KiB shared window,
+// one warp per block (default); 1 / 2 = no window, 2 / 4 warps per block.
+template <class Chunks>
+gd_status_t launch_inflate(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32_t* order, cudaStream_t s) {
+    switch (gd_tune_get(GD_TUNE_INFLATE_VARIANT)) {
+        case 1: return launch_cfg<Chunks, 0, 2>(ch, n, zlib_hdr, order, s);
+        case 2: return launch_cfg<Chunks, 0, 4>(ch, n, zlib_hdr, order, s);
+        default: return launch_cfg<Chunks, 32768, 1>(ch, n, zlib_hdr, order, s);
+    }
 }
 }  // namespace
 

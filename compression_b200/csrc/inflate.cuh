@@ -17,6 +17,8 @@
 //              waves (distance >= 32: each wave reads bytes written by earlier
 //              waves; distance < 32: the period-`distance` pattern is read
 //              from before the copy).  The warp also refills the input ring.
+//              With a window (WIN > 0) the last 32 KiB of output are kept in
+//              shared memory and copies read only there.
 // Dynamic tables are rebuilt per block; table fills are spread over the warp.
 // Every read is bounded by the chunk's compressed size and every write by its
 // output size; malformed input yields GD_ERR_CORRUPT / GD_ERR_OVERRUN.
@@ -53,7 +55,14 @@ struct Huff {
 
 enum : uint32_t { C_LIT = 0, C_COPY = 1, C_STORED = 2 };
 
-struct WarpSmem {
+// Per-warp shared state.  WIN > 0: the last WIN output bytes are kept in a
+// shared-memory window (WIN a power of two >= 32768, the Deflate window), so
+// back-references never read global memory; WIN = 0: copies read the output
+// already written to global memory (a smaller footprint, for kernels that
+// run other decoders beside this one).
+template <uint32_t WIN>
+struct WarpSmemT {
+    uint8_t win[WIN ? WIN : 16];
     uint8_t ring[IRING];
     Huff lit;
     Huff dist;
@@ -65,6 +74,7 @@ struct WarpSmem {
     // decoder state shared between lane 0 and the warp
     uint32_t n_cmd, n_lit, status, done;
 };
+using WarpSmem = WarpSmemT<0>;
 
 // Build `h` from code lengths lens[0..n).  Counting / offsets on lane 0, the
 // primary table fill spread over the warp.  Returns false (on every lane) for
@@ -131,9 +141,11 @@ static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint
 // (the 16-byte-aligned span around them must be readable); dst: room for
 // olen bytes; hdr: 0 raw deflate, 1 zlib, 2 gzip; S: this warp's shared
 // state.  Returns a gd status (same on every lane); *written = bytes output.
+template <uint32_t WIN>
 static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ src, uint32_t clen,
-                                             uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
-                                             WarpSmem& S, uint32_t* written) {
+                                                    uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
+                                                    WarpSmemT<WIN>& S, uint32_t* written) {
+    static_assert(WIN == 0 || (WIN >= 32768 && (WIN & (WIN - 1)) == 0), "window: 0 or a power of two >= 32 KiB");
     const uint32_t lane = lane_id();
     uint32_t err = ST_OK;
     // input ring: compressed byte i (chunk-relative) at ring[(i + sh) % IRING];
@@ -515,6 +527,50 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
         for (uint32_t c = 0; c < nc; ++c) {
             const uint32_t t = S.cmd_t[c], a = S.cmd_a[c], n = S.cmd_b[c];
             uint8_t* d = dst + pos;
+            if constexpr (WIN != 0) {
+                // every output byte also goes to the window; copies read it there
+                constexpr uint32_t M = WIN - 1;
+                if (t == C_LIT) {
+                    for (uint32_t k = lane; k < n; k += 32) {
+                        const uint8_t v = S.lits[a + k];
+                        d[k] = v;
+                        S.win[(pos + k) & M] = v;
+                    }
+                } else if (t == C_STORED) {
+                    const uint8_t* s = src + a;
+                    for (uint32_t k = lane; k < n; k += 32) {
+                        const uint8_t v = s[k];
+                        d[k] = v;
+                        S.win[(pos + k) & M] = v;
+                    }
+                } else if (a >= 32) {
+                    // 32-byte waves: a wave reads bytes written before it (earlier
+                    // waves or earlier commands) and writes after every lane has read
+                    const uint32_t sp = pos - a;
+                    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+                        const uint32_t k = k0 + lane;
+                        uint8_t v = 0;
+                        if (k < n) v = S.win[(sp + k) & M];
+                        __syncwarp();
+                        if (k < n) {
+                            d[k] = v;
+                            S.win[(pos + k) & M] = v;
+                        }
+                        __syncwarp();
+                    }
+                } else {
+                    // distance < 32: the copy repeats the a bytes before it
+                    const uint32_t sp = pos - a;
+                    for (uint32_t k = lane; k < n; k += 32) {
+                        const uint8_t v = S.win[(sp + k % a) & M];
+                        d[k] = v;
+                        S.win[(pos + k) & M] = v;
+                    }
+                }
+                pos += n;
+                __syncwarp();
+                continue;
+            }
             if (t == C_LIT) {
                 for (uint32_t k = lane; k < n; k += 32) d[k] = S.lits[a + k];
             } else if (t == C_STORED) {

@@ -5,8 +5,8 @@
 namespace gd {
 namespace lzss {
 
-constexpr int WPB = 4;
-
+// WPB: warps (chunks) per block, 4 by default (GD_TUNE_LZSS_WARPS_PER_BLOCK)
+template <int WPB>
 __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restrict__ data,
                                                          const uint64_t* __restrict__ blk_off,
                                                          const uint64_t* __restrict__ col_len,
@@ -43,10 +43,17 @@ extern "C" gd_status_t gd_lzss_decode(const uint8_t* d_data, const uint64_t* d_b
     if (out_n_bytes != chunk_size * (uint64_t)n_chunks) return GD_ERR_INVALID_ARG;
     if ((reinterpret_cast<uintptr_t>(d_out) & 3u) != 0) return GD_ERR_INVALID_ARG;
     using namespace gd::lzss;
-    const uint32_t smem = WPB * WARP_SMEM;
-    const uint32_t grid = (n_chunks + WPB - 1) / WPB;
-    cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    decode_kernel<<<grid, WPB * 32, smem, (cudaStream_t)stream>>>(d_data, d_blk_off, d_col_len, d_col_map, n_chunks,
-                                                                   chunk_size, d_out, d_status);
+    const int k = gd_tune_get(GD_TUNE_LZSS_WARPS_PER_BLOCK);
+    const int wpb = (k == 2 || k == 8) ? k : 4;
+    auto go = [&](auto kern) {
+        const uint32_t smem = (uint32_t)wpb * WARP_SMEM;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        kern<<<(n_chunks + wpb - 1) / wpb, wpb * 32, smem, (cudaStream_t)stream>>>(d_data, d_blk_off, d_col_len,
+                                                                                d_col_map, n_chunks, chunk_size,
+                                                                                d_out, d_status);
+    };
+    if (wpb == 2) go(decode_kernel<2>);
+    else if (wpb == 8) go(decode_kernel<8>);
+    else go(decode_kernel<4>);
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
 }

@@ -1,14 +1,15 @@
 // rlev1.cu -- RLE v1 (32-lane interleaved container) decoder for sm_100a: a
-// block of 8 warps owns 8 adjacent lane streams of one chunk, copies them into
-// shared memory, and each warp decodes one (warp-level decoder in rlev1.cuh).
+// block of 8 (or 4) warps owns as many adjacent lane streams of one chunk,
+// copies them into shared memory, and each warp decodes one (warp-level
+// decoder in rlev1.cuh).
 #include "rlev1.cuh"
 
 namespace gd {
 namespace rlev1 {
 
-constexpr int LANES_PER_BLOCK = 8;
-
-template <typename T>
+// LANES_PER_BLOCK (8 default, 4 by GD_TUNE_RLEV1_LANES_PER_BLOCK): warps per
+// block = lane streams per block
+template <typename T, int LANES_PER_BLOCK>
 __global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
     const uint8_t* __restrict__ data, const uint64_t* __restrict__ col_len, const uint64_t* __restrict__ blk_off,
     uint32_t n_chunks, uint64_t chunk_size, uint32_t wil, uint8_t* __restrict__ out, uint64_t out_n, uint32_t cap,
@@ -79,19 +80,22 @@ extern "C" gd_status_t gd_rlev1_decode(const uint8_t* d_data, const uint64_t* d_
     // (a bound above the longest valid stream is clamped: longer lanes are corrupt)
     const uint32_t cap =
         max_lane_bytes ? min(lane_cap(max_lane_bytes), stream_cap(nv, elem_bytes)) : stream_cap(nv, elem_bytes);
-    const uint32_t smem = LANES_PER_BLOCK * cap;
+    const int lpb = gd_tune_get(GD_TUNE_RLEV1_LANES_PER_BLOCK) == 4 ? 4 : 8;
+    const uint32_t smem = (uint32_t)lpb * cap;
     if (smem > 200 * 1024) return GD_ERR_UNSUPPORTED;
     cudaStream_t s = (cudaStream_t)stream;
     if (d_status && cudaMemsetAsync(d_status, 0, 4ull * n_chunks, s) != cudaSuccess) return GD_ERR_CUDA;
-    const uint32_t grid = n_chunks * (32 / LANES_PER_BLOCK);
+    auto go = [&](auto kern, int lanes) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        kern<<<n_chunks * (32 / lanes), lanes * 32, smem, s>>>(d_data, d_col_len, d_blk_off, n_chunks, chunk_size, wil,
+                                                            d_out, out_n_bytes, cap, d_status);
+    };
     if (elem_bytes == 4) {
-        cudaFuncSetAttribute(decode_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        decode_kernel<uint32_t><<<grid, LANES_PER_BLOCK * 32, smem, s>>>(d_data, d_col_len, d_blk_off, n_chunks,
-                                                                        chunk_size, wil, d_out, out_n_bytes, cap, d_status);
+        if (lpb == 4) go(decode_kernel<uint32_t, 4>, 4);
+        else go(decode_kernel<uint32_t, 8>, 8);
     } else {
-        cudaFuncSetAttribute(decode_kernel<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        decode_kernel<uint64_t><<<grid, LANES_PER_BLOCK * 32, smem, s>>>(d_data, d_col_len, d_blk_off, n_chunks,
-                                                                        chunk_size, wil, d_out, out_n_bytes, cap, d_status);
+        if (lpb == 4) go(decode_kernel<uint64_t, 4>, 4);
+        else go(decode_kernel<uint64_t, 8>, 8);
     }
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
 }

@@ -1,6 +1,6 @@
 // rlev2.cu -- RLE v2 (transposed container) decoder for sm_100a.
 //
-// A block of 4 warps owns 4 adjacent lane streams of one chunk and copies
+// A block of 4 (or 8) warps owns as many adjacent lane streams of one chunk and copies
 // them from the interleaved block into shared memory.  Then, in batches of
 // up to RCAP runs per stream:
 //   * parse: lanes 0..3 of warp 0 each walk one stream's run boundaries
@@ -27,15 +27,14 @@
 namespace gd {
 namespace rlev2 {
 
-#ifndef GD_RLEV2_LPB
-#define GD_RLEV2_LPB 4
-#endif
-constexpr int LANES_PER_BLOCK = GD_RLEV2_LPB;  // warps per block = lane streams per block
-constexpr int RCAP = 64;            // runs per stream per batch
+constexpr int RCAP = 64;  // runs per stream per batch
 
-// Run tables of one batch (structure of arrays, one row per stream).
+// Run tables of one batch (structure of arrays, one row per stream);
+// LANES_PER_BLOCK = warps per block = lane streams per block (4 default, 8
+// by GD_TUNE_RLEV2_LANES_PER_BLOCK).
 // meta = kind | fbw << 2 | flags << 9 | pll << 11 | pw << 16 | cfb << 23;
 // aux = delta (DELTA) or the bit offset of the patch list (PATCHED_BASE).
+template <int LANES_PER_BLOCK>
 struct RunTab {
     uint32_t vs[LANES_PER_BLOCK][RCAP + 1];  // first value of each run; [nr] = end of the batch
     uint32_t pos[LANES_PER_BLOCK][RCAP];     // byte offset of each run's header
@@ -186,6 +185,7 @@ static __device__ __forceinline__ Skip skip_run(const uint8_t* s, uint32_t pos, 
     return k;
 }
 
+template <int LANES_PER_BLOCK>
 __global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
     const uint8_t* __restrict__ data, const uint64_t* __restrict__ col_len, const uint64_t* __restrict__ blk_off,
     uint32_t n_chunks, uint64_t chunk_size, uint32_t ru, uint8_t* __restrict__ out, uint64_t out_n, uint32_t cap,
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
     __shared__ SegTable T_;
     __shared__ uint32_t s_len[32];
     __shared__ uint32_t s_bad;
-    __shared__ RunTab R;
+    __shared__ RunTab<LANES_PER_BLOCK> R;
 
     const uint32_t lane = lane_id(), wid = threadIdx.x >> 5, tid = threadIdx.x;
     const uint32_t chunk = blockIdx.x / (32 / LANES_PER_BLOCK);
@@ -415,14 +415,18 @@ extern "C" gd_status_t gd_rlev2_decode(const uint8_t* d_data, const uint64_t* d_
     // (a bound above the longest valid stream is clamped: longer lanes are
     // corrupt), plus 16 bytes for the header parser's 24-byte window reads
     const uint32_t cap = (max_lane_bytes ? min(lane_cap(max_lane_bytes), stream_cap(nv)) : stream_cap(nv)) + 16u;
-    const uint32_t smem = LANES_PER_BLOCK * cap;
+    const int lpb = gd_tune_get(GD_TUNE_RLEV2_LANES_PER_BLOCK) == 8 ? 8 : 4;
+    const uint32_t smem = (uint32_t)lpb * cap;
     if (smem > 200 * 1024) return GD_ERR_UNSUPPORTED;  // lane streams must fit in shared memory
     cudaStream_t s = (cudaStream_t)stream;
     // per-chunk status is the max over the chunk's lane streams
     if (d_status && cudaMemsetAsync(d_status, 0, 4ull * n_chunks, s) != cudaSuccess) return GD_ERR_CUDA;
-    cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    const uint32_t grid = n_chunks * (32 / LANES_PER_BLOCK);
-    decode_kernel<<<grid, LANES_PER_BLOCK * 32, smem, s>>>(d_data, d_col_len, d_blk_off, n_chunks, chunk_size,
-                                                           read_unit, d_out, out_n_bytes, cap, d_status);
+    auto go = [&](auto kern, int lanes) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        kern<<<n_chunks * (32 / lanes), lanes * 32, smem, s>>>(d_data, d_col_len, d_blk_off, n_chunks, chunk_size,
+                                                            read_unit, d_out, out_n_bytes, cap, d_status);
+    };
+    if (lpb == 8) go(decode_kernel<8>, 8);
+    else go(decode_kernel<4>, 4);
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
 }

@@ -251,6 +251,28 @@ gd_status_t gd_batch_decode_lpt_noalloc(const gd_task* d_tasks, uint32_t n_tasks
                                         gd_stream_t stream);
 
 /* ------------------------------------------------------------------------
+ * Launch tuning knobs (no reference counterpart: its launch shapes are
+ * compile-time constants).  Process-wide; each selects among compiled kernel
+ * variants or sets a launch shape, 0 = the built-in default.  Set by the
+ * autotuner, which times the choices on the device.
+ * ------------------------------------------------------------------------ */
+typedef enum gd_tune_key {
+    GD_TUNE_INFLATE_VARIANT = 0, /* 0: 32 KiB shared output window, 1 warp per block;
+                                    1: no window, 2 warps per block; 2: no window, 4 warps per block */
+    GD_TUNE_BRLE_BLOCKS_PER_SM = 1,   /* byte-RLE grid = value x SMs blocks (default 8) */
+    GD_TUNE_RLEV1_LANES_PER_BLOCK = 2, /* 0/8: 8 lane streams per block; 4: 4 */
+    GD_TUNE_RLEV2_LANES_PER_BLOCK = 3, /* 0/4: 4 lane streams per block; 8: 8 */
+    GD_TUNE_LZSS_WARPS_PER_BLOCK = 4,  /* 0/4: 4 chunks (warps) per block; 2: 2; 8: 8 */
+    GD_TUNE_COUNT = 5
+} gd_tune_key_t;
+
+/* Set a knob; returns its previous value, or -1 for an unknown key or a
+ * negative value.  Takes effect for launches made afterwards. */
+int gd_tune_set(int key, int value);
+/* Current value of a knob, -1 for an unknown key. */
+int gd_tune_get(int key);
+
+/* ------------------------------------------------------------------------
  * Learned task-cost model: FP32 MLP 16 -> 64 -> 64 -> 1 (ReLU), parameters
  * W1[16][64] | b1[64] | W2[64][64] | b2[64] | W3[64] | b3 in one float array.
  * No reference counterpart.

@@ -71,3 +71,14 @@ int main(int argc, char**) {
                         f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert subprocess.run([str(exe)]).returncode == 0
+
+
+def test_tuning_knobs_set_and_get():
+    L = _lib.lib()
+    for key in range(5):
+        old = L.gd_tune_get(key)
+        assert old >= 0
+        assert L.gd_tune_set(key, 4) == old
+        assert L.gd_tune_get(key) == 4
+        assert L.gd_tune_set(key, old) == 4
+    assert L.gd_tune_get(5) == -1 and L.gd_tune_set(5, 1) == -1 and L.gd_tune_set(0, -1) == -1
