@@ -10,7 +10,7 @@ A step decodes both columns from HBM to HBM.  Synthetic seeded data stands in
 for the reference's datasets, which are not available.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload brle_rlev2|rlev1|lzss|deflate]
+                    [--workload brle_rlev2|rlev1|lzss|deflate|mixed] [--scale F]
 
 Multi-GPU (torchrun, one process per GPU): every rank decodes its own copy of
 the workload (independent chunks, no exchange step), weak scaling, time = max
@@ -228,8 +228,16 @@ def run_ours(args, rank, world, local_rank):
     for (name, e, raw), j in zip(cols, jobs):
         j.launch()
         torch.cuda.synchronize()
-        if not (j.status() == 0).all() or not np.array_equal(j.output(), raw):
-            raise RuntimeError(f"{name}: GPU output differs from the input column")
+        ok = (j.status() == 0).all() and np.array_equal(j.output(), raw)
+        if not ok and (j.status() == 0).all():
+            # the reference's own encoder can write a container that does not
+            # round-trip (RLE v2 fixed-delta quirk): parity is then checked
+            # against the reference decoder (the oracle)
+            import oracle
+            rc, ref = oracle.decode(e)
+            ok = rc == 0 and np.array_equal(j.output(), ref)
+        if not ok:
+            raise RuntimeError(f"{name}: GPU output differs from the reference decoder")
 
     flush = torch.empty(256 * MiB, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
@@ -320,6 +328,189 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+# --------------------------------------------------------------------------
+# mixed-codec batch with the learned scheduler
+# --------------------------------------------------------------------------
+
+def run_mixed(args, rank, world, local_rank):
+    """Mixed-codec batch: 16384 items (log-uniform 4 KiB - 2 MiB, 4 GiB
+    decompressed in all; 20% RLE v1, 20% RLE v2, 10% byte-RLE, 25% LZSS, 25%
+    Deflate) decoded in one persistent launch.  The cost model is trained on
+    the decoder's own per-task timings (random task orders) during warm-up;
+    the timed step is the CUDA-graph replay of [MLP inference -> longest-first
+    order -> batch decode].  The static mapping (task i -> warp i mod W) and
+    the plain FIFO work queue are timed beside it on the same data."""
+    import torch
+    import compression_b200.batch as B
+    import compression_b200.costmodel as CM
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    n_items = max(64, int(16384 * args.scale))
+    total = int(4 * GiB * args.scale)
+    t0 = time.perf_counter()
+    items = B.make_mixed_batch(0xE0 + rank, n_items, total, 4096, 2 * MiB)
+    plan = B.build_plan(items, dev)
+    t_build = time.perf_counter() - t0
+    n_tasks = plan.tasks.size
+    out_bytes = int(plan.out_len.sum())
+    comp_bytes = sum(it.enc.comp_bytes + it.enc.meta_bytes for it in items)
+
+    # parity of the benchmarked batch: every item bit-exact against the
+    # reference decoder (the oracle); that equals the input column except for
+    # containers the reference's own encoder writes wrongly (its RLE v2
+    # fixed-delta runs after short repeats), where both decoders agree
+    import concurrent.futures as cf
+    import oracle
+    B.launch(plan, None, dynamic=False, timing=False)
+    torch.cuda.synchronize()
+    out = plan.d_out.cpu().numpy()
+    bad = [i for i, (it, o, n) in enumerate(zip(items, plan.out_off, plan.out_len))
+           if not np.array_equal(out[o:o + n], it.raw)]
+    expect = {}
+    with cf.ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        for i, (rc, ref) in zip(bad, ex.map(lambda i: oracle.decode(items[i].enc), bad)):
+            if rc != 0:
+                raise RuntimeError(f"mixed batch item {i}: oracle status {rc}")
+            expect[i] = ref
+    if not B.verify(plan, expect):
+        raise RuntimeError("mixed batch: GPU output differs from the reference decoder")
+    n_quirk = len(expect)
+
+    # ---- training data: self-measured per-task times, random orders ----
+    X = B.task_features(plan)
+    t0 = time.perf_counter()
+    ys, samples = [], 0
+    seed = 0
+    while samples < 200_000 or len(ys) < 2:
+        ys.append(np.log(np.maximum(CM.measure_tasks(plan, seed=seed), 1.0)))
+        samples += n_tasks
+        seed += 1
+    model = CM.CostModel(seed=0, device=dev)
+    Xtr = np.concatenate([X] * len(ys))
+    ytr = np.concatenate(ys)
+    losses = model.train(Xtr, ytr, epochs=8, batch=256, lr=3e-3)
+    t_train = time.perf_counter() - t0
+    pred = model.predict(X)
+    corr = float(np.corrcoef(pred, ys[0])[0, 1])
+    graph = CM.GraphSchedule(plan, model, X)
+
+    flush = torch.empty(256 * MiB, dtype=torch.uint8, device=dev)
+    fifo = None
+
+    def run(kind):
+        if kind == "static":
+            B.launch(plan, None, dynamic=False, timing=False)
+        elif kind == "queue":
+            B.launch(plan, fifo, dynamic=True, timing=False)
+        else:
+            graph.replay()
+
+    for _ in range(args.warmup):
+        for kind in ("static", "queue", "learned"):
+            flush.zero_()
+            run(kind)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    K = args.steps
+    times = {"static": [], "queue": [], "learned": []}
+    with Clocks(local_rank) as clk:
+        for _ in range(K):
+            for kind in ("learned", "static", "queue"):
+                flush.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                run(kind)
+                b.record()
+                torch.cuda.synchronize()
+                times[kind].append(a.elapsed_time(b))
+    med = {k: statistics.median(v) for k, v in times.items()}
+    ms = med["learned"]
+    if world > 1:
+        t = torch.tensor([ms, med["static"], med["queue"]], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms, med["static"], med["queue"] = [float(x) for x in t.tolist()]
+    plan.d_out.zero_()
+    graph.replay()
+    torch.cuda.synchronize()
+    if not B.verify(plan, expect):
+        raise RuntimeError("mixed batch: learned schedule output differs")
+    value = out_bytes * world / (ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    alg = comp_bytes + out_bytes
+    ach = alg / (ms / 1e3) / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        # through the public batch API with host buffers: pinned payload and
+        # metadata arenas copied in, decode, output arena copied back
+        h_in = torch.empty(plan.d_in.numel(), dtype=torch.uint8, pin_memory=True)
+        h_in.copy_(plan.d_in)
+        h_meta = torch.empty(plan.d_meta.numel(), dtype=torch.uint8, pin_memory=True)
+        h_meta.copy_(plan.d_meta)
+        h_out = torch.empty(plan.d_out.numel(), dtype=torch.uint8, pin_memory=True)
+        ts = []
+        for i in range(4):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            plan.d_in.copy_(h_in, non_blocking=True)
+            plan.d_meta.copy_(h_meta, non_blocking=True)
+            graph.replay()
+            h_out.copy_(plan.d_out, non_blocking=True)
+            torch.cuda.synchronize()
+            if i:
+                ts.append(time.perf_counter() - t1)
+        e2e = {"value": round(out_bytes * world / statistics.median(ts) / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": int(h_in.numel() + h_meta.numel()), "d2h_bytes_per_step": int(h_out.numel()),
+               "path": "batch API: pinned arenas H2D, graph replay, output arena D2H"}
+
+    line = {
+        "metric": "mixed-batch decompressed GB/s (learned longest-first schedule)",
+        "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8/int32/int64", "data": "synthetic (seeded generators)",
+        "config": {"workload": f"mixed batch: {n_items} items log-uniform 4 KiB-2 MiB, "
+                               f"{out_bytes / GiB:.2f} GiB decompressed, 20/20/10/25/25% "
+                               "RLE v1/RLE v2/byte-RLE/LZSS/Deflate", "tasks": int(n_tasks),
+                   "warps": B.n_warps(plan), "l2": "flushed between timed launches (256 MiB write)",
+                   "parallelism": f"replicas x{world}"},
+        "makespan_ms": {"static": round(med["static"], 3), "queue_fifo": round(med["queue"], 3),
+                        "learned_lpt": round(ms, 3)},
+        "learned_gain_vs_static": round(1.0 - ms / med["static"], 4),
+        "cost_model": {"samples": int(len(ytr)), "epochs": 8, "final_loss": round(float(losses[-1]), 4),
+                       "corr_pred_measured": round(corr, 4), "train_s": round(t_train, 1)},
+        "roofline": {"bound": "hbm", "kernel": "batch", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(ach / peak, 4), "peak_source": peak_kind, "traffic": None},
+        "gpu_launches": 2 * K,
+        "clocks": clk.summary(),
+        "e2e": e2e,
+        "build_s": round(t_build, 1),
+        "parity": {"items": len(items), "checked_against": "input column; reference decoder (oracle) for "
+                   f"{n_quirk} RLE v2 items its own encoder does not round-trip"},
+    }
+    if rank == 0 and not args.no_cpu:
+        import concurrent.futures as cf
+        import oracle
+        threads = os.cpu_count() or 1
+        rng = np.random.default_rng(1)
+        pick = rng.permutation(len(items))
+        t1 = time.perf_counter()
+        done, nb = 0, 0
+        with cf.ThreadPoolExecutor(threads) as ex:
+            while time.perf_counter() - t1 < 10.0 and done < len(items):
+                batch = [items[i].enc for i in pick[done:done + 4 * threads]]
+                rcs = list(ex.map(lambda e: oracle.decode(e)[0], batch))
+                if any(rcs):
+                    raise RuntimeError("oracle failed on the mixed batch")
+                nb += sum(e.n_out for e in batch)
+                done += len(batch)
+        dt = time.perf_counter() - t1
+        line["cpu_baseline"] = {"value": round(nb / dt / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                                "sample": f"{done} random items, {nb / MiB:.0f} MiB out"}
+    return line
+
+
 def run_reference(args):
     """The reference's CPU decoders (oracle restatement where the reference
     has none that builds here) on all host cores."""
@@ -347,7 +538,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="brle_rlev2", choices=["brle_rlev2", "rlev1", "lzss", "deflate"])
+    ap.add_argument("--workload", default="brle_rlev2", choices=["brle_rlev2", "rlev1", "lzss", "deflate", "mixed"])
     ap.add_argument("--scale", type=float, default=1.0, help="workload size factor (1.0 = full size)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -368,7 +559,7 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    line = run_ours(args, rank, world, local_rank)
+    line = run_mixed(args, rank, world, local_rank) if args.workload == "mixed" else run_ours(args, rank, world, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -52,6 +52,7 @@ SIGNATURES = {
     "gd_lzss_decompress": (i32, [vp, u64, vp, vp, u64, C.POINTER(vp), u64p]),
     "gd_deflate_decompress": (i32, [vp, u64, vp, u64, vp, u64, u64, C.POINTER(vp), u64p]),
     "gd_lzss_contig_decompress": (i32, [vp, u64, vp, vp]),
+    "gd_inflate_decompress": (i32, [vp, u64, vp, vp, vp, u32, i32, vp, vp]),
     "gd_brle_trans_decompress": (i32, [vp, u64, vp, u64, vp, u64, vp, u64, u64, vp, vp]),
     "gd_brle_max_encoded_bytes": (u64, [u64, u64]),
     "gd_brle_encode": (u64, [vp, u64, u64, vp]),

@@ -212,14 +212,17 @@ def n_warps(plan: Plan, blocks_per_sm: int = 0) -> int:
     return int(lib().gd_batch_warps(plan.max_lane, blocks_per_sm))
 
 
-def verify(plan: Plan) -> bool:
-    """Every task OK and every item's output equal to its raw column."""
+def verify(plan: Plan, expect: dict | None = None) -> bool:
+    """Every task OK and every item's output equal to its raw column, or to
+    expect[item index] where given (the reference decoder's output for items
+    whose container does not round-trip in the reference itself)."""
     st = plan.d_status.cpu().numpy()
     if (st != 0).any():
         return False
     out = plan.d_out.cpu().numpy()
-    for it, o, n in zip(plan.items, plan.out_off, plan.out_len):
-        if not np.array_equal(out[o:o + n], it.raw):
+    for i, (it, o, n) in enumerate(zip(plan.items, plan.out_off, plan.out_len)):
+        want = expect[i] if expect and i in expect else it.raw
+        if not np.array_equal(out[o:o + n], want):
             return False
     return True
 
@@ -265,32 +268,52 @@ def task_features(plan: Plan) -> np.ndarray:
       14   log2 size of the whole item
       15   constant 1"""
     T = plan.tasks
-    F = np.zeros((T.size, N_FEATURES), np.float32)
+    n = T.size
+    F = np.zeros((n, N_FEATURES), np.float32)
     chunk = plan.extra["task_chunk"]
-    for i, rec in enumerate(T):
-        it = plan.items[plan.task_item[i]]
-        c = int(rec["codec"])
-        F[i, c] = 1.0
-        src_len = float(rec["src_len"])
-        dst_len = float(rec["dst_len"])
-        skew_max = skew_std = share = 1.0
-        if c in (1, 2, 3):
-            ll = it.enc.meta["col_len"].reshape(-1, 32)[chunk[i]].astype(np.float64)
-            m = max(ll.mean(), 1.0)
-            skew_max, skew_std = ll.max() / m, ll.std() / m
-            if c in (1, 2):
-                src_len = float(ll[int(rec["lane"])])
-                share = src_len / m
-                dst_len = dst_len / 32.0
-        F[i, 5] = np.log2(src_len + 1.0)
-        F[i, 6] = np.log2(dst_len + 1.0)
-        F[i, 7] = src_len / max(dst_len, 1.0)
-        F[i, 8] = skew_max
-        F[i, 9] = skew_std
-        F[i, 10] = share
-        F[i, 11] = np.log2(float(rec["chunk_size"] or rec["dst_len"]) + 1.0)
-        F[i, 12] = 1.0 if (c == 4 and it.enc.comp_bytes > 0.5 * it.enc.n_out) else 0.0
-        F[i, 13] = np.log2(src_len / max(dst_len, 1.0) * 65536.0 + 1.0)
-        F[i, 14] = np.log2(float(it.enc.n_out) + 1.0)
-        F[i, 15] = 1.0
+    item = plan.task_item
+    codec = T["codec"].astype(np.int64)
+    F[np.arange(n), codec] = 1.0
+    src_len = T["src_len"].astype(np.float64)
+    dst_len = T["dst_len"].astype(np.float64)
+    skew_max = np.ones(n)
+    skew_std = np.ones(n)
+    share = np.ones(n)
+    # lane-length statistics of every chunk of the RLE / LZSS items
+    lane_items = [i for i, it in enumerate(plan.items) if "col_len" in it.enc.meta]
+    if lane_items:
+        base = np.zeros(len(plan.items), np.int64)   # first chunk row of each item
+        rows, pos = [], 0
+        for i in lane_items:
+            cl = plan.items[i].enc.meta["col_len"].astype(np.float64).reshape(-1, 32)
+            base[i] = pos
+            rows.append(cl)
+            pos += cl.shape[0]
+        L = np.concatenate(rows)                     # (chunks, 32)
+        mean = np.maximum(L.mean(1), 1.0)
+        cmax, cstd = L.max(1) / mean, L.std(1) / mean
+        sel = np.isin(codec, (1, 2, 3))
+        r = base[item[sel]] + chunk[sel]
+        skew_max[sel] = cmax[r]
+        skew_std[sel] = cstd[r]
+        rle = np.isin(codec, (1, 2))
+        rr = base[item[rle]] + chunk[rle]
+        lane_len = L[rr, T["lane"][rle].astype(np.int64)]
+        share[rle] = lane_len / mean[rr]
+        src_len[rle] = lane_len
+        dst_len[rle] = dst_len[rle] / 32.0
+    comp_total = np.array([it.enc.comp_bytes for it in plan.items], np.float64)
+    out_total = np.array([it.enc.n_out for it in plan.items], np.float64)
+    F[:, 5] = np.log2(src_len + 1.0)
+    F[:, 6] = np.log2(dst_len + 1.0)
+    F[:, 7] = src_len / np.maximum(dst_len, 1.0)
+    F[:, 8] = skew_max
+    F[:, 9] = skew_std
+    F[:, 10] = share
+    cs = T["chunk_size"].astype(np.float64)
+    F[:, 11] = np.log2(np.where(cs > 0, cs, T["dst_len"].astype(np.float64)) + 1.0)
+    F[:, 12] = ((codec == 4) & (comp_total[item] > 0.5 * out_total[item])).astype(np.float32)
+    F[:, 13] = np.log2(src_len / np.maximum(dst_len, 1.0) * 65536.0 + 1.0)
+    F[:, 14] = np.log2(out_total[item] + 1.0)
+    F[:, 15] = 1.0
     return F

@@ -366,11 +366,18 @@ def decode_host(enc: Encoded, keep: bool = True) -> np.ndarray:
                                         _p(m["col_map"]), m["col_map"].nbytes, _p(m["blk_off"]), m["blk_off"].nbytes,
                                         enc.chunk_size, C.byref(out), C.byref(n))
     elif enc.codec == "deflate":
-        # reference triple: blk_offset = [total][0][cumulative], col_len = padded lengths
-        blk = np.concatenate([np.array([enc.n_out], dtype=np.uint64), m["comp_off"]])
-        cs = int(m["out_off"][1] - m["out_off"][0]) if enc.n_chunks > 0 else 1
-        rc = L.gd_deflate_decompress(_p(enc.data), enc.data.size, _p(m["comp_len"]), m["comp_len"].nbytes,
-                                     _p(blk), blk.nbytes, cs, C.byref(out), C.byref(n))
+        oo = m["out_off"]
+        cs = int(oo[1] - oo[0]) if enc.n_chunks > 0 else 1
+        uniform = enc.n_chunks > 0 and bool((np.diff(oo[:-1].astype(np.int64)) == cs).all()) and \
+            0 < int(oo[-1] - oo[-2]) <= cs and enc.params["zlib_header"] == 1
+        if uniform:
+            # reference triple: blk_offset = [total][0][cumulative], col_len = padded lengths
+            blk = np.concatenate([np.array([enc.n_out], dtype=np.uint64), m["comp_off"]])
+            rc = L.gd_deflate_decompress(_p(enc.data), enc.data.size, _p(m["comp_len"]), m["comp_len"].nbytes,
+                                         _p(blk), blk.nbytes, cs, C.byref(out), C.byref(n))
+        else:  # chunks of any size: the extension call with per-chunk output offsets
+            rc = L.gd_inflate_decompress(_p(enc.data), enc.data.size, _p(m["comp_off"]), _p(m["comp_len"]),
+                                         _p(oo), enc.n_chunks, enc.params["zlib_header"], C.byref(out), C.byref(n))
     else:
         raise ValueError(enc.codec)
     check(rc, f"{enc.codec} host decompress")

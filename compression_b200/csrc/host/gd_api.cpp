@@ -447,4 +447,46 @@ gd_status_t gd_brle_trans_decompress(const uint8_t* in, uint64_t in_n_bytes, con
     return GD_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Deflate chunks of any size (extension of deflate::decompress_gpu, which
+// assumes one uniform chunk size: zlib.h:966-1082).
+// ---------------------------------------------------------------------------
+gd_status_t gd_inflate_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* comp_off,
+                                  const uint64_t* comp_len, const uint64_t* out_off, uint32_t n_chunks,
+                                  int zlib_header, uint8_t** out, uint64_t* out_n_bytes) {
+    if (!in || !comp_off || !comp_len || !out_off || !out || !out_n_bytes || n_chunks == 0) return GD_ERR_INVALID_ARG;
+    const uint64_t n = n_chunks;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (comp_off[i] + comp_len[i] > in_n_bytes || out_off[i + 1] < out_off[i]) return GD_ERR_CORRUPT;
+    }
+    const uint64_t total = out_off[n];
+    *out = nullptr;
+    *out_n_bytes = 0;
+    cudaStream_t s = 0;
+    uint8_t* d_data = (uint8_t*)g_pool.get(0, in_n_bytes + 16);
+    uint64_t* d_meta = (uint64_t*)g_pool.get(1, 8 * (3 * n + 2));
+    uint8_t* d_out = (uint8_t*)g_pool.get(2, total ? total : 1);
+    uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
+    if (!d_data || !d_meta || !d_out || !d_st) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(d_data, in, in_n_bytes, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_meta, comp_off, 8 * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_meta + n + 1, comp_len, 8 * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_meta + 2 * n + 1, out_off, 8 * (n + 1), cudaMemcpyHostToDevice, s);
+    gd_status_t r = gd_inflate(d_data, d_meta, d_meta + n + 1, d_meta + 2 * n + 1, (uint32_t)n, zlib_header, d_out,
+                               d_st, s);
+    if (r != GD_OK) return r;
+    uint8_t* h = (uint8_t*)pinned().get(total ? total : 1);
+    if (!h) return GD_ERR_NOMEM;
+    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
+    r = collect(d_st, (uint32_t)n, s);
+    if (r != GD_OK) {
+        gd_free(h);
+        return r;
+    }
+    *out = h;
+    *out_n_bytes = total;
+    return GD_OK;
+}
+
 }  // extern "C"

@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(NW * 32) inflate_kernel(Chunks ch, uint32_t n_
     uint32_t err = ch.get(chunk, src, clen64, dst, olen64) ? ST_OK : ST_CORRUPT;
     if (olen64 > 0xffffffffull || clen64 > 0xffffffffull) err = ST_CORRUPT;
     uint32_t fin = 0;
-    if (err == ST_OK) err = stream_warp<WIN>(src, (uint32_t)clen64, dst, (uint32_t)olen64, zlib_hdr, S, &fin);
+    if (err == ST_OK) err = stream_warp_impl<WIN>(src, (uint32_t)clen64, dst, (uint32_t)olen64, zlib_hdr, S, &fin);
     if (err == ST_OK && Chunks::exact && fin != (uint32_t)olen64) err = ST_CORRUPT;
     if (lane_id() == 0) ch.put(chunk, err, err == ST_OK ? fin : 0);
 }

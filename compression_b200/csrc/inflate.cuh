@@ -61,12 +61,14 @@ enum : uint32_t { C_LIT = 0, C_COPY = 1, C_STORED = 2 };
 // already written to global memory (a smaller footprint, for kernels that
 // run other decoders beside this one).
 template <uint32_t WIN>
-struct WarpSmemT {
+struct alignas(16) WarpSmemT {
     uint8_t win[WIN ? WIN : 16];
     uint8_t ring[IRING];
     Huff lit;
     Huff dist;
     uint8_t lens[320];
+    uint8_t cl_tmp[320];   // code lengths while a dynamic header is read
+    uint16_t offs[16];     // canonical code offsets (build_huff)
     uint8_t lits[NLIT];
     uint32_t cmd_a[NCMD];  // C_LIT: literal buffer offset | C_COPY: distance | C_STORED: input offset
     uint32_t cmd_b[NCMD];  // length
@@ -79,11 +81,10 @@ using WarpSmem = WarpSmemT<0>;
 // Build `h` from code lengths lens[0..n).  Counting / offsets on lane 0, the
 // primary table fill spread over the warp.  Returns false (on every lane) for
 // an over-subscribed or otherwise unusable code.
-static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint32_t* sh_flag) {
+static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint32_t* sh_flag, uint16_t* offs) {
     const uint32_t lane = lane_id();
     for (uint32_t i = lane; i < (1u << LBITS); i += 32) h->lut[i] = 0xffffffffu;
     if (lane == 0) {
-        uint16_t offs[16];
         for (int i = 0; i < 16; ++i) h->count[i] = 0;
         for (uint32_t s = 0; s < n; ++s) h->count[lens[s]]++;
         int left = 1;
@@ -141,10 +142,13 @@ static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint
 // (the 16-byte-aligned span around them must be readable); dst: room for
 // olen bytes; hdr: 0 raw deflate, 1 zlib, 2 gzip; S: this warp's shared
 // state.  Returns a gd status (same on every lane); *written = bytes output.
+// stream_warp_impl is inlined into the caller, so the compiler sees that S is
+// shared memory and uses shared-memory loads and stores throughout;
+// stream_warp is the out-of-line form for kernels that run several decoders.
 template <uint32_t WIN>
-static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ src, uint32_t clen,
-                                                    uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
-                                                    WarpSmemT<WIN>& S, uint32_t* written) {
+static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __restrict__ src, uint32_t clen,
+                                                            uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
+                                                            WarpSmemT<WIN>& S, uint32_t* written) {
     static_assert(WIN == 0 || (WIN >= 32768 && (WIN & (WIN - 1)) == 0), "window: 0 or a power of two >= 32 KiB");
     const uint32_t lane = lane_id();
     uint32_t err = ST_OK;
@@ -230,8 +234,22 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
         }
         return true;
     };
+    // top up bitbuf: single bytes up to a 4-byte boundary of the stream,
+    // then one aligned 32-bit word per call (the ring is word aligned and
+    // IRING a multiple of 4), single bytes again at the end of the input
     auto fill_bits = [&]() {
-        while (bitcnt <= 56 && inpos < fill) {
+        while (bitcnt <= 56 && inpos < fill && (inpos & 3u)) {
+            bitbuf |= (uint64_t)S.ring[inpos & (IRING - 1)] << bitcnt;
+            ++inpos;
+            bitcnt += 8;
+        }
+        if (bitcnt <= 32 && (inpos & 3u) == 0 && inpos + 4 <= fill) {
+            const uint32_t w = *reinterpret_cast<const uint32_t*>(S.ring + (inpos & (IRING - 1)));
+            bitbuf |= (uint64_t)w << bitcnt;
+            inpos += 4;
+            bitcnt += 32;
+        }
+        while (bitcnt <= 56 && inpos < fill && inpos + 4 > fill) {
             bitbuf |= (uint64_t)S.ring[inpos & (IRING - 1)] << bitcnt;
             ++inpos;
             bitcnt += 8;
@@ -347,13 +365,13 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
             __syncwarp();
             err = S.status;
             if (err != ST_OK) break;
-            if (!build_huff(&S.lit, S.lens, 19, sflag)) {
+            if (!build_huff(&S.lit, S.lens, 19, sflag, S.offs)) {
                 err = ST_CORRUPT;
                 break;
             }
             if (lane == 0) {
                 // read nlen + ndist code lengths (lens[0..nlen) lit, [288..288+ndist) dist)
-                uint8_t tmp[320];
+                uint8_t* tmp = S.cl_tmp;
                 uint32_t i = 0;
                 const uint32_t tot = nlen + ndist;
                 while (i < tot && err == ST_OK) {
@@ -395,9 +413,9 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
             if (err != ST_OK) break;
         }
         if (hdr_state == 1 || hdr_state == 2) {
-            const bool ok1 = build_huff(&S.lit, S.lens, 288, sflag);
+            const bool ok1 = build_huff(&S.lit, S.lens, 288, sflag, S.offs);
             // a distance code with a single used symbol is allowed (incomplete)
-            const bool ok2 = ok1 && build_huff(&S.dist, S.lens + 288, 30, sflag);
+            const bool ok2 = ok1 && build_huff(&S.dist, S.lens + 288, 30, sflag, S.offs);
             if (!ok1 || !ok2) {
                 err = ST_CORRUPT;
                 break;
@@ -446,11 +464,20 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
                     opos += ln;
                 }
             } else {
-                // Huffman-coded symbols until the batch is full or the block ends
-                uint32_t lit_start = 0;
-                while (err == ST_OK && nc < NCMD - 1 && nl < NLIT && (fill - inpos >= 32 || fill >= span)) {
+                // Huffman-coded symbols until the batch is full or the block ends.
+                // Literals accumulate in a run that becomes one command when a
+                // copy or the end of the batch closes it.
+                uint32_t run = 0, run_start = nl;
+                while (err == ST_OK && nc < NCMD - 2 && nl < NLIT && (fill - inpos >= 32 || fill >= span)) {
+                    fill_bits();
                     uint32_t sym;
-                    if (!decode_sym(&S.lit, sym)) {
+                    const uint32_t e = S.lit.lut[bitbuf & ((1u << LBITS) - 1u)];
+                    if (e != 0xffffffffu && (e & 0xffu) != 0 && (e & 0xffu) <= bitcnt) {
+                        const uint32_t L = e & 0xffu;
+                        bitbuf >>= L;
+                        bitcnt -= L;
+                        sym = e >> 8;
+                    } else if (!decode_sym(&S.lit, sym)) {
                         err = ST_CORRUPT;
                         break;
                     }
@@ -459,18 +486,19 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
                             err = ST_OVERRUN;
                             break;
                         }
-                        if (nl == lit_start) {  // open a literal run
-                            S.cmd_t[nc] = C_LIT;
-                            S.cmd_a[nc] = nl;
-                            S.cmd_b[nc] = 0;
-                            ++nc;
-                        }
+                        if (run == 0) run_start = nl;
                         S.lits[nl++] = (uint8_t)sym;
-                        S.cmd_b[nc - 1]++;
+                        ++run;
                         ++opos;
                         continue;
                     }
-                    lit_start = nl;
+                    if (run) {
+                        S.cmd_t[nc] = C_LIT;
+                        S.cmd_a[nc] = run_start;
+                        S.cmd_b[nc] = run;
+                        ++nc;
+                        run = 0;
+                    }
                     if (sym == 256) {
                         in_block = 0;
                         break;
@@ -479,17 +507,17 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
                         err = ST_CORRUPT;
                         break;
                     }
-                    uint32_t x, len, dsym, dist;
+                    uint32_t x, dsym;
                     if (!get_bits(LEXT[sym - 257], x)) {
                         err = ST_CORRUPT;
                         break;
                     }
-                    len = LBASE[sym - 257] + x;
+                    const uint32_t len = LBASE[sym - 257] + x;
                     if (!decode_sym(&S.dist, dsym) || dsym > 29 || !get_bits(DEXT[dsym], x)) {
                         err = ST_CORRUPT;
                         break;
                     }
-                    dist = DBASE[dsym] + x;
+                    const uint32_t dist = DBASE[dsym] + x;
                     if (dist > opos) {
                         err = ST_CORRUPT;
                         break;
@@ -503,6 +531,12 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
                     S.cmd_b[nc] = len;
                     ++nc;
                     opos += len;
+                }
+                if (run) {
+                    S.cmd_t[nc] = C_LIT;
+                    S.cmd_a[nc] = run_start;
+                    S.cmd_b[nc] = run;
+                    ++nc;
                 }
             }
             S.n_cmd = nc;
@@ -598,6 +632,13 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
     const uint32_t fin = __shfl_sync(GD_FULL_MASK, opos, 0);
     *written = fin;
     return __shfl_sync(GD_FULL_MASK, err, 0);
+}
+
+template <uint32_t WIN>
+static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ src, uint32_t clen,
+                                                    uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
+                                                    WarpSmemT<WIN>& S, uint32_t* written) {
+    return stream_warp_impl<WIN>(src, clen, dst, olen, zlib_hdr, S, written);
 }
 
 }  // namespace infl

@@ -330,6 +330,14 @@ gd_status_t gd_deflate_decompress(const uint8_t* in, uint64_t in_n_bytes, const 
                                   uint64_t col_n_bytes, const uint64_t* blk_offset, uint64_t blk_n_bytes,
                                   uint64_t chunk_size, uint8_t** out, uint64_t* out_n_bytes);
 
+/* Deflate chunks of any size (an extension: deflate::decompress_gpu,
+ * include/zlib/zlib.h:966-1082, assumes one uniform chunk size).  in = the
+ * streams; comp_off[n] / comp_len[n] locate each; out_off[n+1] are the output
+ * offsets (out_off[n] = total); zlib_header as for gd_inflate. */
+gd_status_t gd_inflate_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* comp_off,
+                                  const uint64_t* comp_len, const uint64_t* out_off, uint32_t n_chunks,
+                                  int zlib_header, uint8_t** out, uint64_t* out_n_bytes);
+
 /* lzss::decompress_gpu_base (include/lzss/lzss.h:1126-1188): in = the whole
  * contiguous container [u64 in_n_bytes][u32 chunk_size][u32 n_chunks]
  * [u32 2048][u32 3][u32 34][u64 stream end per chunk][data]. */

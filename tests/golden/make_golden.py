@@ -87,6 +87,17 @@ def main():
         rv[f"dec{i}"] = np.fromfile(tmp / "vd", np.int64)
     np.savez_compressed(OUT / "rlev2_golden.npz", **rv)
 
+    # ---- an RLE v2 lane the reference's own encoder writes wrongly: a
+    # 12-value constant run after two short repeats becomes a fixed-delta run
+    # with a non-zero delta (lane 20 of a 5120-value generator column) ----
+    col = cc.gen_rlev2_ints(0xE0 * 100003 + 9149, 5120)
+    lane = col[20 * 32 + np.concatenate([np.arange(k * 1024, k * 1024 + 32) for k in range(5)])].astype(np.int64)
+    lane.tofile(tmp / "v")
+    run(REF / "ref_rlev2", "encode", tmp / "v", tmp / "vs")
+    run(REF / "ref_rlev2", "decode", tmp / "vs", lane.size, tmp / "vd")
+    np.savez_compressed(OUT / "rlev2_quirk.npz", raw=lane, enc=np.fromfile(tmp / "vs", np.uint8),
+                        dec=np.fromfile(tmp / "vd", np.int64))
+
     # ---- Deflate chunks (Python zlib, level 6 / 9 as orig_compressor.py) ----
     dz = {}
     raw = cc.gen_markov_copy(6, 300000, 32768)
