@@ -46,7 +46,9 @@ def test_training_learns_a_function(cuda):
 
 @pytest.fixture(scope="module")
 def batch(cuda):
-    items = B.make_mixed_batch(11, 400, 160 << 20)
+    # many items of moderate size: the total work per warp, not one long
+    # task, sets the makespan, which is where placement matters
+    items = B.make_mixed_batch(11, 2400, 480 << 20, 4096, 512 << 10)
     return B.build_plan(items, cuda)
 
 
@@ -56,7 +58,7 @@ def test_learned_lpt_beats_static_mapping(batch):
     X = B.task_features(plan)
     # self-measured training data: two randomly ordered runs of this batch
     # shape and one of a different batch
-    ys = [np.log(measure_tasks(plan, seed=s)) for s in (0, 1)]
+    ys = [np.log(np.maximum(measure_tasks(plan, seed=s), 1.0)) for s in (0, 1)]
     m = CostModel(seed=0)
     m.train(np.concatenate([X, X]), np.concatenate(ys), epochs=25, lr=3e-3)
     pred = m.predict(X)
@@ -67,7 +69,7 @@ def test_learned_lpt_beats_static_mapping(batch):
     print(f"\ncorr(pred, measured)={r:.3f}  static={static:.3f} ms  queue={queue:.3f} ms  "
           f"learned-LPT={learned:.3f} ms  gain vs static={(1 - learned / static) * 100:.1f}%")
     assert r > 0.8
-    assert learned < static
+    assert learned < 0.8 * static  # >= 20% shorter makespan than the static mapping
     plan.d_out.zero_()
     B.launch(plan, lpt_order(pred), dynamic=True)
     torch.cuda.synchronize()
