@@ -27,7 +27,8 @@
 //      control byte, run byte).
 //   6. Expansion: the tile's output is cut into 64-byte slices dealt round
 //      robin to all 256 threads.  A thread finds the token covering its slice
-//      by a fixed-step binary search of the list, then builds each aligned
+//      in a slice -> token index written with the list (a binary search of
+//      the list for tiles with more output than the index holds), builds each aligned
 //      16-byte vector by merging the pieces of the tokens that cover it (a run
 //      piece is a broadcast byte, a literal piece an unaligned 16-byte read
 //      of the staged tile), and stores it with one 16-byte store.  The few
@@ -57,6 +58,7 @@ constexpr uint32_t OFF_TBL = (TILE_BYTES + 15u) & ~15u;
 constexpr uint32_t OFF_LIST = OFF_TBL + TILE;
 constexpr uint32_t SMEM = OFF_LIST + MAXTOK * 8;
 static_assert(NWARP * 32 * 32 * 2 <= MAXTOK * 8, "region chains must fit in the token list space");
+constexpr uint32_t SLICE_CAP = TILE / 2;  // 64-byte slices indexed per tile (u16 entries in the exit tables)
 
 __device__ __forceinline__ uint32_t tok_in(uint32_t c) { return c > 127u ? c - 126u : 2u; }
 __device__ __forceinline__ uint32_t tok_out(uint32_t c) { return c > 127u ? c - 127u : c + 3u; }
@@ -221,12 +223,23 @@ __global__ void __launch_bounds__(NT, 4) decode_kernel(const uint8_t* __restrict
                 err = ST_OVERRUN;
                 break;
             }
+            // token list; and, for every 64-byte output slice that starts
+            // inside a token, that token's index (s_slice, in the exit-table
+            // space, which is free now) -- unless the tile's output has more
+            // slices than fit, in which case the expansion searches the list
+            const uint32_t sbase = opos >> 6;
+            const bool indexed = ((opos + total + 63u) >> 6) - sbase <= SLICE_CAP;
+            uint16_t* s_slice = reinterpret_cast<uint16_t*>(s_tbl);
             if (ntok) {
                 uint32_t j = (uint32_t)(ex >> 32), o = opos + (uint32_t)ex;
                 for (uint32_t p = ent; p < lim;) {
                     const uint32_t c = tb[p];
-                    s_list[j++] = make_uint2(o, p | (c << 16) | ((uint32_t)tb[p + 1] << 24));
-                    o += tok_out(c);
+                    s_list[j] = make_uint2(o, p | (c << 16) | ((uint32_t)tb[p + 1] << 24));
+                    const uint32_t oe_tok = o + tok_out(c);
+                    if (indexed)
+                        for (uint32_t b = (o + 63u) & ~63u; b < oe_tok; b += 64u) s_slice[(b >> 6) - sbase] = (uint16_t)j;
+                    ++j;
+                    o = oe_tok;
                     p += tok_in(c);
                 }
             }
@@ -239,10 +252,14 @@ __global__ void __launch_bounds__(NT, 4) decode_kernel(const uint8_t* __restrict
                 if (lo >= hi) continue;
                 // last token whose output starts at or before lo
                 uint32_t a = 0;
+                if (indexed) {
+                    if (lo > ob) a = s_slice[(lo >> 6) - sbase];  // lo is a slice start here
+                } else {
 #pragma unroll
-                for (uint32_t step = MAXTOK / 2; step; step >>= 1) {
-                    const uint32_t cand = a + step;
-                    if (cand < ntot && s_list[cand].x <= lo) a = cand;
+                    for (uint32_t step = MAXTOK / 2; step; step >>= 1) {
+                        const uint32_t cand = a + step;
+                        if (cand < ntot && s_list[cand].x <= lo) a = cand;
+                    }
                 }
                 uint32_t ks = s_list[a].x, info = s_list[a].y;
                 uint32_t ke = ks + tok_out((info >> 16) & 0xffu);
