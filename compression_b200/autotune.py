@@ -3,8 +3,9 @@
 Every knob of include/gd.h (gd_tune_key) selects among kernel variants that
 are compiled into libgd.so or sets a launch shape:
 
-  inflate  GD_TUNE_INFLATE_VARIANT        0: 32 KiB shared output window, 1 warp/block
-                                          1, 2: no window, 2 / 4 warps per block
+  inflate  GD_TUNE_INFLATE_VARIANT        0: decoder + writer warp per stream, 32 KiB window
+                                          1, 2: one warp per stream, no window, 2 / 4 per block
+                                          3: one warp per stream with the window
   brle     GD_TUNE_BRLE_BLOCKS_PER_SM     grid = value x SMs
   rlev1    GD_TUNE_RLEV1_LANES_PER_BLOCK  lane streams (warps) per block
   rlev2    GD_TUNE_RLEV2_LANES_PER_BLOCK  lane streams (warps) per block
@@ -41,7 +42,7 @@ TUNE_LZSS_WARPS_PER_BLOCK = 4
 
 # codec -> (knob, candidate values; the first is the built-in default)
 KNOBS = {
-    "deflate": (TUNE_INFLATE_VARIANT, [0, 1, 2]),
+    "deflate": (TUNE_INFLATE_VARIANT, [0, 1, 2, 3]),
     "brle": (TUNE_BRLE_BLOCKS_PER_SM, [8, 4, 16]),
     "rlev1": (TUNE_RLEV1_LANES_PER_BLOCK, [8, 4]),
     "rlev2": (TUNE_RLEV2_LANES_PER_BLOCK, [4, 8]),

@@ -67,6 +67,44 @@ __global__ void __launch_bounds__(NW * 32) inflate_kernel(Chunks ch, uint32_t n_
     if (lane_id() == 0) ch.put(chunk, err, err == ST_OK ? fin : 0);
 }
 
+// Reader/writer pairs: NP pairs per block, warps 2i (decoder) and 2i+1
+// (writer) share stream i's state and hand batches over through it.
+template <class Chunks, uint32_t WIN, int NP>
+__global__ void __launch_bounds__(NP * 64) inflate_pair_kernel(Chunks ch, uint32_t n_chunks, int zlib_hdr,
+                                                              const uint32_t* __restrict__ order) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    const uint32_t wid = threadIdx.x >> 5, pair = wid >> 1;
+    const uint32_t slot = blockIdx.x * NP + pair;
+    if (slot >= n_chunks) return;  // both warps of the pair leave together
+    const uint32_t chunk = order ? order[slot] : slot;
+    WarpSmemT<WIN, 2>& S = *reinterpret_cast<WarpSmemT<WIN, 2>*>(smem_raw + pair * sizeof(WarpSmemT<WIN, 2>));
+    const uint8_t* src;
+    uint8_t* dst;
+    uint64_t clen64, olen64;
+    uint32_t err = ch.get(chunk, src, clen64, dst, olen64) ? ST_OK : ST_CORRUPT;
+    if (olen64 > 0xffffffffull || clen64 > 0xffffffffull) err = ST_CORRUPT;
+    if (err != ST_OK) {  // decided identically by both warps: neither enters the hand-off
+        if ((wid & 1u) == 0 && lane_id() == 0) ch.put(chunk, err, 0);
+        return;
+    }
+    if (threadIdx.x == 64 * pair) {
+        S.produced = 0;
+        S.consumed = 0;
+    }
+    // counters cleared before either warp of the pair uses them: a barrier of
+    // the pair's 64 threads, reached unconditionally by both warps
+    asm volatile("bar.sync %0, 64;" ::"r"(1u + pair) : "memory");
+    if (wid & 1u) {
+        const uint32_t werr = stream_pair_writer<WIN>(S, src, dst);
+        if (werr != ST_OK && lane_id() == 0) ch.put(chunk, werr, 0);
+        return;
+    }
+    uint32_t fin = 0;
+    err = stream_warp_impl<WIN, 2>(src, (uint32_t)clen64, dst, (uint32_t)olen64, zlib_hdr, S, &fin);
+    if (err == ST_OK && Chunks::exact && fin != (uint32_t)olen64) err = ST_CORRUPT;
+    if (lane_id() == 0) ch.put(chunk, err, err == ST_OK ? fin : 0);
+}
+
 }  // namespace infl
 }  // namespace gd
 
@@ -96,14 +134,33 @@ gd_status_t launch_cfg(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32_
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
 }
 
-// Launch configuration (GD_TUNE_INFLATE_VARIANT): 0 = 32 KiB shared window,
-// one warp per block (default); 1 / 2 = no window, 2 / 4 warps per block.
+template <class Chunks, uint32_t WIN, int NP>
+gd_status_t launch_pair(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32_t* order, cudaStream_t s) {
+    using namespace gd::infl;
+    const uint32_t smem = NP * (uint32_t)sizeof(WarpSmemT<WIN, 2>);
+    static bool attr_set = false;  // benign race: the attribute call is idempotent
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(inflate_pair_kernel<Chunks, WIN, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem) != cudaSuccess)
+            return GD_ERR_CUDA;
+        attr_set = true;
+    }
+    const uint32_t grid = (n + NP - 1) / NP;
+    inflate_pair_kernel<Chunks, WIN, NP><<<grid, NP * 64, smem, s>>>(ch, n, zlib_hdr, order);
+    return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+}
+
+// Launch configuration (GD_TUNE_INFLATE_VARIANT): 0 = decoder/writer warp
+// pair per stream with a 32 KiB shared window (default); 1 / 2 = one warp per
+// stream without a window, 2 / 4 warps per block; 3 = one warp per stream
+// with a window.
 template <class Chunks>
 gd_status_t launch_inflate(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32_t* order, cudaStream_t s) {
     switch (gd_tune_get(GD_TUNE_INFLATE_VARIANT)) {
+        case 3: return launch_cfg<Chunks, 32768, 1>(ch, n, zlib_hdr, order, s);
         case 1: return launch_cfg<Chunks, 0, 2>(ch, n, zlib_hdr, order, s);
         case 2: return launch_cfg<Chunks, 0, 4>(ch, n, zlib_hdr, order, s);
-        default: return launch_cfg<Chunks, 32768, 1>(ch, n, zlib_hdr, order, s);
+        default: return launch_pair<Chunks, 32768, 1>(ch, n, zlib_hdr, order, s);
     }
 }
 }  // namespace

@@ -55,12 +55,24 @@ struct Huff {
 
 enum : uint32_t { C_LIT = 0, C_COPY = 1, C_STORED = 2 };
 
-// Per-warp shared state.  WIN > 0: the last WIN output bytes are kept in a
+// One batch of decoded commands: literal bytes, commands, and the output
+// position of its first byte.  last = no batch follows (pair hand-off).
+struct Batch {
+    uint8_t lits[NLIT];
+    uint32_t cmd_a[NCMD];  // C_LIT: literal buffer offset | C_COPY: distance | C_STORED: input offset
+    uint32_t cmd_b[NCMD];  // length
+    uint8_t cmd_t[NCMD];
+    uint32_t n_cmd, n_lit, pos0, last;
+};
+
+// Per-stream shared state.  WIN > 0: the last WIN output bytes are kept in a
 // shared-memory window (WIN a power of two >= 32768, the Deflate window), so
 // back-references never read global memory; WIN = 0: copies read the output
 // already written to global memory (a smaller footprint, for kernels that
-// run other decoders beside this one).
-template <uint32_t WIN>
+// run other decoders beside this one).  NB = 1: one warp decodes and
+// executes; NB = 2: a decoder warp fills batch k+1 while a writer warp
+// executes batch k.
+template <uint32_t WIN, int NB = 1>
 struct alignas(16) WarpSmemT {
     uint8_t win[WIN ? WIN : 16];
     uint8_t ring[IRING];
@@ -69,14 +81,121 @@ struct alignas(16) WarpSmemT {
     uint8_t lens[320];
     uint8_t cl_tmp[320];   // code lengths while a dynamic header is read
     uint16_t offs[16];     // canonical code offsets (build_huff)
-    uint8_t lits[NLIT];
-    uint32_t cmd_a[NCMD];  // C_LIT: literal buffer offset | C_COPY: distance | C_STORED: input offset
-    uint32_t cmd_b[NCMD];  // length
-    uint8_t cmd_t[NCMD];
+    Batch bt[NB];
     // decoder state shared between lane 0 and the warp
-    uint32_t n_cmd, n_lit, status, done;
+    uint32_t status, done;
+    uint32_t produced, consumed;  // pair hand-off counters
 };
-using WarpSmem = WarpSmemT<0>;
+using WarpSmem = WarpSmemT<0, 1>;
+
+// Write batch B (output starting at pos) with the calling warp.
+template <uint32_t WIN>
+static __device__ __forceinline__ void execute_batch(const Batch& B, uint32_t pos, uint8_t* win,
+                                                     const uint8_t* __restrict__ src, uint8_t* __restrict__ dst) {
+    const uint32_t lane = lane_id();
+    const uint32_t nc = B.n_cmd;
+    for (uint32_t c = 0; c < nc; ++c) {
+        const uint32_t t = B.cmd_t[c], a = B.cmd_a[c], n = B.cmd_b[c];
+        uint8_t* d = dst + pos;
+        if constexpr (WIN != 0) {
+            // every output byte also goes to the window; copies read it there
+            constexpr uint32_t M = WIN - 1;
+            if (t == C_LIT) {
+                for (uint32_t k = lane; k < n; k += 32) {
+                    const uint8_t v = B.lits[a + k];
+                    d[k] = v;
+                    win[(pos + k) & M] = v;
+                }
+            } else if (t == C_STORED) {
+                const uint8_t* s = src + a;
+                for (uint32_t k = lane; k < n; k += 32) {
+                    const uint8_t v = s[k];
+                    d[k] = v;
+                    win[(pos + k) & M] = v;
+                }
+            } else if (a >= 32) {
+                // 32-byte waves: a wave reads bytes written before it (earlier
+                // waves or earlier commands) and writes after every lane has read
+                const uint32_t sp = pos - a;
+                for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+                    const uint32_t k = k0 + lane;
+                    uint8_t v = 0;
+                    if (k < n) v = win[(sp + k) & M];
+                    __syncwarp();
+                    if (k < n) {
+                        d[k] = v;
+                        win[(pos + k) & M] = v;
+                    }
+                    __syncwarp();
+                }
+            } else {
+                // distance < 32: the copy repeats the a bytes before it
+                const uint32_t sp = pos - a;
+                for (uint32_t k = lane; k < n; k += 32) {
+                    const uint8_t v = win[(sp + k % a) & M];
+                    d[k] = v;
+                    win[(pos + k) & M] = v;
+                }
+            }
+        } else {
+            if (t == C_LIT) {
+                for (uint32_t k = lane; k < n; k += 32) d[k] = B.lits[a + k];
+            } else if (t == C_STORED) {
+                const uint8_t* s = src + a;
+                for (uint32_t k = lane; k < n; k += 32) d[k] = s[k];
+            } else {
+                const uint8_t* s = d - a;
+                if (a >= 32) {
+                    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+                        const uint32_t k = k0 + lane;
+                        uint8_t v = 0;
+                        if (k < n) v = s[k];
+                        __syncwarp();
+                        if (k < n) d[k] = v;
+                        __syncwarp();
+                    }
+                } else {
+                    for (uint32_t k = lane; k < n; k += 32) d[k] = s[k % a];
+                }
+            }
+        }
+        pos += n;
+        __syncwarp();
+    }
+}
+
+// Hand-off between the two warps of a pair: counters in shared memory.
+// produced = batches the decoder has filled, consumed = batches the writer
+// has executed.  Every wait is bounded (about a second): on expiry the waiter
+// reports GD_ERR_TIMEOUT and both warps still leave.
+constexpr uint32_t PAIR_SPIN_LIMIT = 1u << 25;
+
+// Wait (lane 0 spins, the warp follows) until *ctr >= target; false on expiry.
+__device__ __forceinline__ bool pair_wait(const uint32_t* ctr, uint32_t target) {
+    uint32_t ok = 1;
+    if (lane_id() == 0) {
+        uint32_t it = 0;
+        while (*reinterpret_cast<const volatile uint32_t*>(ctr) < target) {
+            if (++it > PAIR_SPIN_LIMIT) {
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence_block();  // the batch written before the counter is visible
+    }
+    return __shfl_sync(GD_FULL_MASK, ok, 0) != 0;
+}
+
+// Publish *ctr = value after this warp's earlier shared-memory writes.
+__device__ __forceinline__ void pair_post(uint32_t* ctr, uint32_t value) {
+    __syncwarp();
+    if (lane_id() == 0) {
+        __threadfence_block();
+        *reinterpret_cast<volatile uint32_t*>(ctr) = value;
+    }
+    __syncwarp();
+}
 
 // Build `h` from code lengths lens[0..n).  Counting / offsets on lane 0, the
 // primary table fill spread over the warp.  Returns false (on every lane) for
@@ -145,10 +264,12 @@ static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint
 // stream_warp_impl is inlined into the caller, so the compiler sees that S is
 // shared memory and uses shared-memory loads and stores throughout;
 // stream_warp is the out-of-line form for kernels that run several decoders.
-template <uint32_t WIN>
+// NB = 2 (decoder of a pair): instead of executing a batch, hand it to the
+// writer warp (see stream_pair_writer); S.produced / S.consumed must be 0.
+template <uint32_t WIN, int NB = 1>
 static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __restrict__ src, uint32_t clen,
                                                             uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
-                                                            WarpSmemT<WIN>& S, uint32_t* written) {
+                                                            WarpSmemT<WIN, NB>& S, uint32_t* written) {
     static_assert(WIN == 0 || (WIN >= 32768 && (WIN & (WIN - 1)) == 0), "window: 0 or a power of two >= 32 KiB");
     const uint32_t lane = lane_id();
     uint32_t err = ST_OK;
@@ -299,7 +420,16 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
 
     uint32_t* sflag = &S.done;  // scratch word for build_huff's broadcast (restored below)
     // main loop ------------------------------------------------------------
+    uint32_t kb = 0;  // batches handed off (pairs: the buffer is bt[kb & 1])
     while (err == ST_OK) {
+        Batch& BT = S.bt[NB == 2 ? (kb & 1u) : 0u];
+        // pairs: the buffer's previous batch (kb - 2) must have been executed
+        if constexpr (NB == 2) {
+            if (kb >= 2 && !pair_wait(&S.consumed, kb - 1)) {
+                err = ST_TIMEOUT;
+                break;
+            }
+        }
         // ---- refill input for the decoder (warp) ----
         uint32_t inpos_b = __shfl_sync(GD_FULL_MASK, inpos, 0);
         refill(inpos_b > 64 ? inpos_b - 64 : 0);
@@ -307,8 +437,8 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
         // ---- block header (table builds need the warp) ----
         uint32_t hdr_state = 0;  // 0 = none, 1 = fixed, 2 = dynamic lens ready, 3 = stored, 4 = end
         if (lane == 0) {
-            S.n_cmd = 0;
-            S.n_lit = 0;
+            BT.n_cmd = 0;
+            BT.n_lit = 0;
             if (!in_block) {
                 if (bfinal) {
                     hdr_state = 4;
@@ -439,14 +569,14 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                     if (opos + ln > olen) err = ST_OVERRUN;
                     const uint32_t from_buf = min(avail_bytes, ln);
                     for (uint32_t k = 0; k < from_buf && err == ST_OK; ++k) {
-                        S.lits[nl++] = (uint8_t)(bitbuf & 0xffu);
+                        BT.lits[nl++] = (uint8_t)(bitbuf & 0xffu);
                         bitbuf >>= 8;
                         bitcnt -= 8;
                     }
                     if (from_buf && err == ST_OK) {
-                        S.cmd_t[nc] = C_LIT;
-                        S.cmd_a[nc] = 0;
-                        S.cmd_b[nc] = from_buf;
+                        BT.cmd_t[nc] = C_LIT;
+                        BT.cmd_a[nc] = 0;
+                        BT.cmd_b[nc] = from_buf;
                         ++nc;
                     }
                     const uint32_t rest = ln - from_buf;
@@ -455,9 +585,9 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                         if (inpos + rest > span) err = ST_CORRUPT;
                         // the stored bytes are read from global: skip them in the ring
                         if (fill < inpos + rest) fill = max(fill, (inpos + rest) & ~15u);
-                        S.cmd_t[nc] = C_STORED;
-                        S.cmd_a[nc] = inpos - sh;
-                        S.cmd_b[nc] = rest;
+                        BT.cmd_t[nc] = C_STORED;
+                        BT.cmd_a[nc] = inpos - sh;
+                        BT.cmd_b[nc] = rest;
                         ++nc;
                         inpos += rest;
                     }
@@ -487,15 +617,15 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                             break;
                         }
                         if (run == 0) run_start = nl;
-                        S.lits[nl++] = (uint8_t)sym;
+                        BT.lits[nl++] = (uint8_t)sym;
                         ++run;
                         ++opos;
                         continue;
                     }
                     if (run) {
-                        S.cmd_t[nc] = C_LIT;
-                        S.cmd_a[nc] = run_start;
-                        S.cmd_b[nc] = run;
+                        BT.cmd_t[nc] = C_LIT;
+                        BT.cmd_a[nc] = run_start;
+                        BT.cmd_b[nc] = run;
                         ++nc;
                         run = 0;
                     }
@@ -526,21 +656,21 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                         err = ST_OVERRUN;
                         break;
                     }
-                    S.cmd_t[nc] = C_COPY;
-                    S.cmd_a[nc] = dist;
-                    S.cmd_b[nc] = len;
+                    BT.cmd_t[nc] = C_COPY;
+                    BT.cmd_a[nc] = dist;
+                    BT.cmd_b[nc] = len;
                     ++nc;
                     opos += len;
                 }
                 if (run) {
-                    S.cmd_t[nc] = C_LIT;
-                    S.cmd_a[nc] = run_start;
-                    S.cmd_b[nc] = run;
+                    BT.cmd_t[nc] = C_LIT;
+                    BT.cmd_a[nc] = run_start;
+                    BT.cmd_b[nc] = run;
                     ++nc;
                 }
             }
-            S.n_cmd = nc;
-            S.n_lit = nl;
+            BT.n_cmd = nc;
+            BT.n_lit = nl;
             S.status = err;
         }
         __syncwarp();
@@ -548,86 +678,35 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
         fill = __shfl_sync(GD_FULL_MASK, fill, 0);
         if (err != ST_OK) break;
 
-        // ---- execute the batch (all lanes) ----
-        const uint32_t nc = S.n_cmd;
+        // ---- execute the batch (all lanes), or hand it to the writer ----
+        const uint32_t nc = BT.n_cmd;
         uint32_t pos = __shfl_sync(GD_FULL_MASK, opos, 0);
         // pos is the end position after the batch; walk back to its start
         {
             uint32_t tot = 0;
-            for (uint32_t c = lane; c < nc; c += 32) tot += S.cmd_b[c];
+            for (uint32_t c = lane; c < nc; c += 32) tot += BT.cmd_b[c];
             for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(GD_FULL_MASK, tot, o);
             pos -= tot;
         }
-        for (uint32_t c = 0; c < nc; ++c) {
-            const uint32_t t = S.cmd_t[c], a = S.cmd_a[c], n = S.cmd_b[c];
-            uint8_t* d = dst + pos;
-            if constexpr (WIN != 0) {
-                // every output byte also goes to the window; copies read it there
-                constexpr uint32_t M = WIN - 1;
-                if (t == C_LIT) {
-                    for (uint32_t k = lane; k < n; k += 32) {
-                        const uint8_t v = S.lits[a + k];
-                        d[k] = v;
-                        S.win[(pos + k) & M] = v;
-                    }
-                } else if (t == C_STORED) {
-                    const uint8_t* s = src + a;
-                    for (uint32_t k = lane; k < n; k += 32) {
-                        const uint8_t v = s[k];
-                        d[k] = v;
-                        S.win[(pos + k) & M] = v;
-                    }
-                } else if (a >= 32) {
-                    // 32-byte waves: a wave reads bytes written before it (earlier
-                    // waves or earlier commands) and writes after every lane has read
-                    const uint32_t sp = pos - a;
-                    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
-                        const uint32_t k = k0 + lane;
-                        uint8_t v = 0;
-                        if (k < n) v = S.win[(sp + k) & M];
-                        __syncwarp();
-                        if (k < n) {
-                            d[k] = v;
-                            S.win[(pos + k) & M] = v;
-                        }
-                        __syncwarp();
-                    }
-                } else {
-                    // distance < 32: the copy repeats the a bytes before it
-                    const uint32_t sp = pos - a;
-                    for (uint32_t k = lane; k < n; k += 32) {
-                        const uint8_t v = S.win[(sp + k % a) & M];
-                        d[k] = v;
-                        S.win[(pos + k) & M] = v;
-                    }
-                }
-                pos += n;
-                __syncwarp();
-                continue;
+        if constexpr (NB == 2) {
+            if (lane == 0) {
+                BT.pos0 = pos;
+                BT.last = 0;
             }
-            if (t == C_LIT) {
-                for (uint32_t k = lane; k < n; k += 32) d[k] = S.lits[a + k];
-            } else if (t == C_STORED) {
-                const uint8_t* s = src + a;
-                for (uint32_t k = lane; k < n; k += 32) d[k] = s[k];
-            } else {
-                const uint8_t* s = d - a;
-                if (a >= 32) {
-                    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
-                        const uint32_t k = k0 + lane;
-                        uint8_t v = 0;
-                        if (k < n) v = s[k];
-                        __syncwarp();
-                        if (k < n) d[k] = v;
-                        __syncwarp();
-                    }
-                } else {
-                    for (uint32_t k = lane; k < n; k += 32) d[k] = s[k % a];
-                }
-            }
-            pos += n;
-            __syncwarp();
+            pair_post(&S.produced, kb + 1);
+            ++kb;
+        } else {
+            execute_batch<WIN>(BT, pos, S.win, src, dst);
         }
+    }
+    if constexpr (NB == 2) {  // the final (empty) hand-off
+        if (err != ST_TIMEOUT && kb >= 2 && !pair_wait(&S.consumed, kb - 1)) err = ST_TIMEOUT;
+        Batch& BT = S.bt[kb & 1u];
+        if (lane == 0) {
+            BT.n_cmd = 0;
+            BT.last = 1;
+        }
+        pair_post(&S.produced, kb + 1);
     }
     const uint32_t fin = __shfl_sync(GD_FULL_MASK, opos, 0);
     *written = fin;
@@ -639,6 +718,22 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
                                                     uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
                                                     WarpSmemT<WIN>& S, uint32_t* written) {
     return stream_warp_impl<WIN>(src, clen, dst, olen, zlib_hdr, S, written);
+}
+
+// Writer warp of a pair: executes batch k while the decoder warp (running
+// stream_warp_impl<WIN, 2> on the same S) decodes batch k+1.  The decoder's
+// last hand-off is an empty batch marked last (also after an error).
+// Returns GD_ERR_TIMEOUT if a wait expired, else OK.
+template <uint32_t WIN>
+static __device__ __forceinline__ uint32_t stream_pair_writer(WarpSmemT<WIN, 2>& S, const uint8_t* __restrict__ src,
+                                                              uint8_t* __restrict__ dst) {
+    for (uint32_t kb = 0;; ++kb) {
+        if (!pair_wait(&S.produced, kb + 1)) return ST_TIMEOUT;
+        const Batch& BT = S.bt[kb & 1u];
+        if (BT.last) return ST_OK;
+        execute_batch<WIN>(BT, BT.pos0, S.win, src, dst);
+        pair_post(&S.consumed, kb + 1);
+    }
 }
 
 }  // namespace infl
