@@ -197,10 +197,47 @@ __device__ __forceinline__ void pair_post(uint32_t* ctr, uint32_t value) {
     __syncwarp();
 }
 
-// Build `h` from code lengths lens[0..n).  Counting / offsets on lane 0, the
-// primary table fill spread over the warp.  Returns false (on every lane) for
-// an over-subscribed or otherwise unusable code.
-static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint32_t* sh_flag, uint16_t* offs) {
+// Lookup-table entries carry what the decoder needs next, so a length or
+// distance needs no second table lookup:
+//   bits 0-3 code length (0 = longer than LBITS: canonical walk), 4-7 extra
+//   bits, 8-23 value, 24-31 kind.
+// Table kinds: TK_PLAIN (code-length code: value = symbol), TK_LIT
+// (literal/length: E_LIT value = byte, E_LEN value = length base, E_EOB,
+// E_BAD), TK_DIST (E_DIST value = distance base, E_BAD).
+enum : uint32_t { TK_PLAIN = 0, TK_LIT = 1, TK_DIST = 2 };
+enum : uint32_t { E_LIT = 0, E_LEN = 1, E_EOB = 2, E_DIST = 3, E_BAD = 4 };
+
+__device__ __forceinline__ uint32_t make_entry(uint32_t tk, uint32_t sym, uint32_t L) {
+    uint32_t kind = E_LIT, value = sym, extra = 0;
+    if (tk == TK_LIT) {
+        if (sym == 256) {
+            kind = E_EOB;
+        } else if (sym > 256) {
+            if (sym > 285) {
+                kind = E_BAD;
+            } else {
+                kind = E_LEN;
+                value = LBASE[sym - 257];
+                extra = LEXT[sym - 257];
+            }
+        }
+    } else if (tk == TK_DIST) {
+        if (sym > 29) {
+            kind = E_BAD;
+        } else {
+            kind = E_DIST;
+            value = DBASE[sym];
+            extra = DEXT[sym];
+        }
+    }
+    return L | (extra << 4) | (value << 8) | (kind << 24);
+}
+
+// Build `h` from code lengths lens[0..n) for table kind tk.  Counting /
+// offsets on lane 0, the primary table fill spread over the warp.  Returns
+// false (on every lane) for an over-subscribed or otherwise unusable code.
+static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint32_t* sh_flag, uint16_t* offs,
+                                  uint32_t tk) {
     const uint32_t lane = lane_id();
     for (uint32_t i = lane; i < (1u << LBITS); i += 32) h->lut[i] = 0xffffffffu;
     if (lane == 0) {
@@ -235,7 +272,7 @@ static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint
             const uint32_t c = first + k;
             // deflate sends codes MSB first into an LSB-first stream: reverse
             const uint32_t rev = __brev(c) >> (32 - L);
-            const uint32_t entry = ((uint32_t)h->sym[idx + k] << 8) | L;
+            const uint32_t entry = make_entry(tk, h->sym[idx + k], L);
             for (uint32_t f = rev; f < (1u << LBITS); f += (1u << L)) h->lut[f] = entry;
         }
     }
@@ -384,19 +421,8 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
         return true;
     };
     // decode one symbol of code h; returns false on exhausted input / bad code
-    auto decode_sym = [&](const Huff* h, uint32_t& sym) -> bool {
-        fill_bits();
-        const uint32_t e = h->lut[bitbuf & ((1u << LBITS) - 1u)];
-        if (e != 0xffffffffu && (e & 0xffu) != 0) {
-            const uint32_t L = e & 0xffu;
-            if (L > bitcnt) return false;
-            bitbuf >>= L;
-            bitcnt -= L;
-            sym = e >> 8;
-            return true;
-        }
-        if (e == 0xffffffffu) return false;
-        // canonical walk (puff-style) for codes longer than LBITS
+    // canonical walk (puff-style) for codes longer than LBITS
+    auto walk = [&](const Huff* h, uint32_t& sym) -> bool {
         int code = 0, first = 0, index = 0;
         uint64_t bb = bitbuf;
         for (uint32_t L = 1; L < 16; ++L) {
@@ -416,6 +442,30 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
             code <<= 1;
         }
         return false;
+    };
+    // decode one entry of table h (kind tk); false on exhausted input / bad code
+    auto decode_ent = [&](const Huff* h, uint32_t tk, uint32_t& e) -> bool {
+        fill_bits();
+        e = h->lut[bitbuf & ((1u << LBITS) - 1u)];
+        const uint32_t L = e & 15u;
+        if (e != 0xffffffffu && L != 0) {
+            if (L > bitcnt) return false;
+            bitbuf >>= L;
+            bitcnt -= L;
+            return true;
+        }
+        if (e == 0xffffffffu) return false;
+        uint32_t sym;
+        if (!walk(h, sym)) return false;
+        e = make_entry(tk, sym, 0);
+        return true;
+    };
+    // one symbol of a plain table (the code-length code)
+    auto decode_sym = [&](const Huff* h, uint32_t& sym) -> bool {
+        uint32_t e;
+        if (!decode_ent(h, TK_PLAIN, e)) return false;
+        sym = (e >> 8) & 0xffffu;
+        return true;
     };
 
     uint32_t* sflag = &S.done;  // scratch word for build_huff's broadcast (restored below)
@@ -495,7 +545,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
             __syncwarp();
             err = S.status;
             if (err != ST_OK) break;
-            if (!build_huff(&S.lit, S.lens, 19, sflag, S.offs)) {
+            if (!build_huff(&S.lit, S.lens, 19, sflag, S.offs, TK_PLAIN)) {
                 err = ST_CORRUPT;
                 break;
             }
@@ -543,9 +593,9 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
             if (err != ST_OK) break;
         }
         if (hdr_state == 1 || hdr_state == 2) {
-            const bool ok1 = build_huff(&S.lit, S.lens, 288, sflag, S.offs);
+            const bool ok1 = build_huff(&S.lit, S.lens, 288, sflag, S.offs, TK_LIT);
             // a distance code with a single used symbol is allowed (incomplete)
-            const bool ok2 = ok1 && build_huff(&S.dist, S.lens + 288, 30, sflag, S.offs);
+            const bool ok2 = ok1 && build_huff(&S.dist, S.lens + 288, 30, sflag, S.offs, TK_DIST);
             if (!ok1 || !ok2) {
                 err = ST_CORRUPT;
                 break;
@@ -599,25 +649,19 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                 // copy or the end of the batch closes it.
                 uint32_t run = 0, run_start = nl;
                 while (err == ST_OK && nc < NCMD - 2 && nl < NLIT && (fill - inpos >= 32 || fill >= span)) {
-                    fill_bits();
-                    uint32_t sym;
-                    const uint32_t e = S.lit.lut[bitbuf & ((1u << LBITS) - 1u)];
-                    if (e != 0xffffffffu && (e & 0xffu) != 0 && (e & 0xffu) <= bitcnt) {
-                        const uint32_t L = e & 0xffu;
-                        bitbuf >>= L;
-                        bitcnt -= L;
-                        sym = e >> 8;
-                    } else if (!decode_sym(&S.lit, sym)) {
+                    uint32_t e;
+                    if (!decode_ent(&S.lit, TK_LIT, e)) {
                         err = ST_CORRUPT;
                         break;
                     }
-                    if (sym < 256) {
+                    const uint32_t kind = e >> 24;
+                    if (kind == E_LIT) {
                         if (opos >= olen) {
                             err = ST_OVERRUN;
                             break;
                         }
                         if (run == 0) run_start = nl;
-                        BT.lits[nl++] = (uint8_t)sym;
+                        BT.lits[nl++] = (uint8_t)(e >> 8);
                         ++run;
                         ++opos;
                         continue;
@@ -629,25 +673,25 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                         ++nc;
                         run = 0;
                     }
-                    if (sym == 256) {
+                    if (kind == E_EOB) {
                         in_block = 0;
                         break;
                     }
-                    if (sym > 285) {
+                    if (kind != E_LEN) {
                         err = ST_CORRUPT;
                         break;
                     }
-                    uint32_t x, dsym;
-                    if (!get_bits(LEXT[sym - 257], x)) {
+                    uint32_t x, ed;
+                    if (!get_bits((e >> 4) & 15u, x)) {
                         err = ST_CORRUPT;
                         break;
                     }
-                    const uint32_t len = LBASE[sym - 257] + x;
-                    if (!decode_sym(&S.dist, dsym) || dsym > 29 || !get_bits(DEXT[dsym], x)) {
+                    const uint32_t len = ((e >> 8) & 0xffffu) + x;
+                    if (!decode_ent(&S.dist, TK_DIST, ed) || (ed >> 24) != E_DIST || !get_bits((ed >> 4) & 15u, x)) {
                         err = ST_CORRUPT;
                         break;
                     }
-                    const uint32_t dist = DBASE[dsym] + x;
+                    const uint32_t dist = ((ed >> 8) & 0xffffu) + x;
                     if (dist > opos) {
                         err = ST_CORRUPT;
                         break;
