@@ -251,6 +251,25 @@ __global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
         if (tid < LANES_PER_BLOCK) {
             uint32_t nr = 0;
             while (p_err == ST_OK && p_g < nv && nr < (uint32_t)RCAP) {
+                // SHORT_REPEAT (most runs): length and size from the first byte
+                const uint32_t h0 = p_pos < plen ? psbuf[p_pos] : 0xffu;
+                if (h0 < 64u) {
+                    const uint32_t next = p_pos + 2u + ((h0 >> 3) & 7u), rl = (h0 & 7u) + 3u;
+                    if (next > plen) {
+                        p_err = ST_CORRUPT;
+                        break;
+                    }
+                    if (p_g + rl > nv) {
+                        p_err = ST_OVERRUN;
+                        break;
+                    }
+                    R.vs[tid][nr] = p_g;
+                    R.pos[tid][nr] = p_pos;
+                    ++nr;
+                    p_pos = next;
+                    p_g += rl;
+                    continue;
+                }
                 const Skip k = skip_run(psbuf, p_pos, plen);
                 if (k.err != ST_OK) {
                     p_err = k.err;
