@@ -170,6 +170,75 @@ def cpu_decode_sample(cols, threads: int, budget_s: float = 10.0):
     return out_bytes / t_total / 1e9, "; ".join(descr)
 
 
+REF_BIN = ROOT / "oracle" / "_ref"
+
+
+def _ref_container(name, enc, path):
+    """Write enc in the file format of the reference harness's bench mode;
+    returns the harness binary, or None when the codec has no compiled
+    reference CPU decoder."""
+    import oracle
+    m = enc.meta
+    if name == "brle" and (REF_BIN / "ref_brle").exists():
+        ptr = np.ascontiguousarray(m["ptr"], dtype=np.uint64)
+        with open(path, "wb") as f:
+            f.write(np.uint32(ptr.size).tobytes())
+            f.write(ptr.tobytes())
+            f.write(np.uint64(enc.n_out).tobytes())
+            f.write(enc.data.tobytes())
+        return REF_BIN / "ref_brle"
+    if name in ("rlev2", "lzss") and (REF_BIN / f"ref_{name}").exists():
+        lanes, off = oracle.export_lanes(enc)
+        per = enc.chunk_size // 256 if name == "rlev2" else enc.chunk_size // 32
+        with open(path, "wb") as f:
+            f.write(np.array([off.size - 1, per], dtype=np.uint64).tobytes())
+            f.write(off.tobytes())
+            f.write(lanes.tobytes())
+            f.write(bytes(64))
+        return REF_BIN / f"ref_{name}"
+    return None
+
+
+def ref_decode_sample(cols, threads: int, budget_s: float = 10.0, prepared=None):
+    """Decode rate of the reference's own CPU decoders on the host cores.
+
+    byte-RLE: brle::decode per 256 KiB chunk (brle.h:26-100); RLE v2:
+    rlev2::block_decode per lane stream (decoder.h:190); LZSS:
+    lzss::decompress_func per column stream (lzss_cpu.h:110) -- compiled from
+    the reference sources into oracle/_ref, run on `threads` host threads over
+    the whole column, repeated for the time budget.  Codecs without a compiled
+    reference decoder (RLE v1, whose decoders are GPU-only; Deflate, which the
+    reference decodes on the CPU with zlib) fall back to the oracle, whose
+    Deflate path is system zlib.  Returns (GB/s, description, kind,
+    prepared) where GB/s is the rate of decoding all columns one after the
+    other."""
+    prepared = prepared if prepared is not None else {}
+    t_total, b_total, descr, kinds = 0.0, 0, [], []
+    per = budget_s / len(cols)
+    for name, enc, raw in cols:
+        if name not in prepared:
+            path = Path(tempfile.mkdtemp()) / f"{name}.bin"
+            prepared[name] = (_ref_container(name, enc, path), path)
+        exe, path = prepared[name]
+        if exe is not None:
+            r = subprocess.run([str(exe), "bench", str(path), str(threads), str(per)], capture_output=True,
+                               text=True, check=True, timeout=120 + 4 * per)
+            nb, dt = r.stdout.split()
+            rate = int(nb) / float(dt)
+            kinds.append("reference")
+            descr.append(f"{name}: reference {exe.name} over the whole column ({enc.n_out / MiB:.0f} MiB), "
+                         f"repeated {int(nb) // max(enc.n_out, 1)}x")
+        else:
+            gbs, d = cpu_decode_sample([(name, enc, raw)], threads, budget_s=per)
+            rate = gbs * 1e9
+            kinds.append("reference" if name == "deflate" else "port")
+            descr.append(("zlib inflate: " if name == "deflate" else "oracle port: ") + d)
+        t_total += enc.n_out / rate
+        b_total += enc.n_out
+    kind = kinds[0] if len(set(kinds)) == 1 else "mixed"
+    return b_total / t_total / 1e9, "; ".join(descr), kind, prepared
+
+
 def _split(enc, take, threads):
     """Sub-containers of the first `take` chunks, split into `threads` parts."""
     import compression_b200.codecs as cc
@@ -322,8 +391,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        gbs, sample = cpu_decode_sample(cols, threads)
-        line["cpu_baseline"] = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+        gbs, sample, kind, _ = ref_decode_sample(cols, threads)
+        line["cpu_baseline"] = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
                                 "sample": sample}
     return line
 
@@ -490,44 +559,65 @@ def run_mixed(args, rank, world, local_rank):
                    f"{n_quirk} RLE v2 items its own encoder does not round-trip"},
     }
     if rank == 0 and not args.no_cpu:
-        import concurrent.futures as cf
-        import oracle
         threads = os.cpu_count() or 1
-        rng = np.random.default_rng(1)
-        pick = rng.permutation(len(items))
-        t1 = time.perf_counter()
-        done, nb = 0, 0
-        with cf.ThreadPoolExecutor(threads) as ex:
-            while time.perf_counter() - t1 < 10.0 and done < len(items):
-                batch = [items[i].enc for i in pick[done:done + 4 * threads]]
-                rcs = list(ex.map(lambda e: oracle.decode(e)[0], batch))
-                if any(rcs):
-                    raise RuntimeError("oracle failed on the mixed batch")
-                nb += sum(e.n_out for e in batch)
-                done += len(batch)
-        dt = time.perf_counter() - t1
-        line["cpu_baseline"] = {"value": round(nb / dt / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": "port",
-                                "sample": f"{done} random items, {nb / MiB:.0f} MiB out"}
+        gbs, sample = mixed_cpu_sample(items, threads, 10.0)
+        line["cpu_baseline"] = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                                "sample": sample}
     return line
 
 
+def mixed_cpu_sample(items, threads: int, budget_s: float):
+    """Oracle decode of random items of the mixed batch on the host cores
+    (the per-item containers have no single reference CPU entry point)."""
+    import concurrent.futures as cf
+    import oracle
+    rng = np.random.default_rng(1)
+    pick = rng.permutation(len(items))
+    t1 = time.perf_counter()
+    done, nb = 0, 0
+    with cf.ThreadPoolExecutor(threads) as ex:
+        while time.perf_counter() - t1 < budget_s and done < len(items):
+            batch = [items[i].enc for i in pick[done:done + 4 * threads]]
+            rcs = list(ex.map(lambda e: oracle.decode(e)[0], batch))
+            if any(rcs):
+                raise RuntimeError("oracle failed on the mixed batch")
+            nb += sum(e.n_out for e in batch)
+            done += len(batch)
+    dt = time.perf_counter() - t1
+    return nb / dt / 1e9, f"{done} random items, {nb / MiB:.0f} MiB out"
+
+
+
 def run_reference(args):
-    """The reference's CPU decoders (oracle restatement where the reference
-    has none that builds here) on all host cores."""
-    cols, cfg = make_workload(args.workload, args.scale)
+    """The reference's own CPU decoders (oracle/_ref, compiled from the
+    reference sources) on all host cores; the oracle port for codecs whose
+    reference decoders are GPU-only."""
     threads = os.cpu_count() or 1
-    vals = []
-    for _ in range(args.warmup):
-        cpu_decode_sample(cols, threads, budget_s=2.0)
-    for _ in range(args.steps):
-        gbs, sample = cpu_decode_sample(cols, threads, budget_s=6.0)
-        vals.append(gbs)
+    vals, prep = [], None
+    if args.workload == "mixed":
+        import compression_b200.batch as B
+        n_items = max(64, int(16384 * args.scale))
+        items = B.make_mixed_batch(0xE0, n_items, int(4 * GiB * args.scale), 4096, 2 * MiB)
+        cfg = {"workload": f"mixed-codec batch, {n_items} items, {4 * args.scale:g} GiB decompressed"}
+        for _ in range(args.warmup):
+            mixed_cpu_sample(items, threads, 1.0)
+        for _ in range(args.steps):
+            gbs, sample = mixed_cpu_sample(items, threads, 4.0)
+            vals.append(gbs)
+        kind = "port"
+    else:
+        cols, cfg = make_workload(args.workload, args.scale)
+        for _ in range(args.warmup):
+            _, _, _, prep = ref_decode_sample(cols, threads, budget_s=1.0, prepared=prep)
+        for _ in range(args.steps):
+            gbs, sample, kind, prep = ref_decode_sample(cols, threads, budget_s=4.0, prepared=prep)
+            vals.append(gbs)
     v = statistics.median(vals)
     return {"impl": "reference", "metric": "decompressed GB/s (byte-RLE + RLE v2 columns)"
             if args.workload == "brle_rlev2" else f"decompressed GB/s ({args.workload})",
             "value": round(v, 3), "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "config": cfg,
-            "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+            "ms_per_step": None, "higher_is_better": True, "config": cfg,
+            "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": kind,
                              "sample": sample},
             "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 

@@ -40,6 +40,8 @@ def lib():
         L.gdo_lzss_decode_stream.argtypes = [vp, u64, vp, u64]
         L.gdo_rlev2_decode_stream.restype = i32
         L.gdo_lzss_decode_stream.restype = i32
+        L.gdo_export_lanes.argtypes = [vp, u64, vp, vp, u32, vp, vp]
+        L.gdo_export_lanes.restype = i32
         L.gdo_version.restype = C.c_char_p
         _L = L
     return _L
@@ -92,3 +94,17 @@ def lzss_decode_stream(stream: np.ndarray, n_out: int) -> tuple[int, np.ndarray]
     s = np.ascontiguousarray(stream, dtype=np.uint8)
     out = np.zeros(n_out, dtype=np.uint8)
     return int(lib().gdo_lzss_decode_stream(_p(s), s.size, _p(out), n_out)), out
+
+
+def export_lanes(enc) -> tuple[np.ndarray, np.ndarray]:
+    """The 32 * n_chunks lane (or column) streams of an interleaved container
+    back to back, in slot order, and their offsets (32 * n_chunks + 1)."""
+    m = enc.meta
+    cl = np.ascontiguousarray(m["col_len"], dtype=np.uint64)
+    out = np.zeros(max(int(cl.sum()), 1), dtype=np.uint8)
+    off = np.zeros(cl.size + 1, dtype=np.uint64)
+    rc = lib().gdo_export_lanes(_p(enc.data), enc.data.size, _p(m["blk_off"]), _p(cl), enc.n_chunks,
+                                _p(out), _p(off))
+    if rc:
+        raise RuntimeError(f"export_lanes: status {rc}")
+    return out[: int(off[-1])], off

@@ -731,3 +731,35 @@ int gdo_rlev2_decode_stream(const uint8_t* s, uint64_t len, int64_t* vals, uint6
 int gdo_lzss_decode_stream(const uint8_t* s, uint64_t len, uint8_t* out, uint64_t n_out) {
     return lzss_decode_column(s, len, out, n_out);
 }
+
+/*
+ * Lane / column streams of an interleaved container (RLE v1, RLE v2, LZSS,
+ * byte-RLE transposed), written back to back in slot order: stream 32c+s is
+ * col_len[32c+s] bytes at out + out_off[32c+s], so that the reference's
+ * contiguous per-stream decoders (rlev2::block_decode, decoder.h:190;
+ * lzss::decompress_func, lzss_cpu.h:110) can be run on each one.
+ * out_off has 32*n_chunks + 1 entries.
+ */
+int gdo_export_lanes(const uint8_t* data, uint64_t data_len, const uint64_t* blk_off,
+                     const uint64_t* col_len, uint32_t n_chunks, uint8_t* out, uint64_t* out_off) {
+    uint8_t* lanes[32];
+    uint64_t cap = 0;
+    for (uint64_t i = 0; i < 32ull * n_chunks; ++i)
+        if (col_len[i] + 8 > cap) cap = col_len[i] + 8;
+    for (int t = 0; t < 32; ++t) lanes[t] = (uint8_t*)calloc(cap ? cap : 8, 1);
+    int rc = GDO_OK;
+    uint64_t pos = 0;
+    out_off[0] = 0;
+    for (uint32_t c = 0; c < n_chunks && rc == GDO_OK; ++c) {
+        if (blk_off[c] > data_len) { rc = GDO_CORRUPT; break; }
+        rc = deinterleave(data + blk_off[c], data_len - blk_off[c], col_len + 32ull * c, lanes);
+        for (int s = 0; s < 32 && rc == GDO_OK; ++s) {
+            uint64_t n = col_len[32ull * c + s];
+            memcpy(out + pos, lanes[s], n);
+            pos += n;
+            out_off[32ull * c + s + 1] = pos;
+        }
+    }
+    for (int t = 0; t < 32; ++t) free(lanes[t]);
+    return rc;
+}

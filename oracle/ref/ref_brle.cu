@@ -3,11 +3,18 @@
 //   ref_brle encode <raw> <container>   brle::encode per 256 KiB chunk, laid out
 //                                       as brle::compress_gpu does (brle.h:278-292)
 //   ref_brle decode <container> <raw>   brle::decode per chunk (brle.h:26-100)
+//   ref_brle bench <container> <threads> <seconds>
+//                                       brle::decode of every chunk on <threads>
+//                                       host threads, repeated for about <seconds>;
+//                                       prints "<bytes decoded> <seconds taken>"
 #include <brle/brle.h>
 
+#include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 static std::vector<uint8_t> slurp(const char* p) {
@@ -26,9 +33,38 @@ static void spit(const char* p, const void* d, size_t n) {
     fclose(f);
 }
 
+static int bench(const std::vector<uint8_t>& in, int threads, double budget) {
+    uint32_t n_ptr;
+    memcpy(&n_ptr, in.data(), 4);
+    std::vector<uint64_t> ptr(n_ptr);
+    memcpy(ptr.data(), in.data() + 4, 8 * n_ptr);
+    uint64_t total;
+    memcpy(&total, in.data() + 4 + 8 * n_ptr, 8);
+    const uint8_t* data = in.data() + 4 + 8 * n_ptr + 8;
+    const uint64_t nc = n_ptr - 1;
+    std::vector<uint8_t> out(nc * CHUNK_SIZE);
+    uint64_t bytes = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    double dt = 0;
+    do {
+        std::atomic<uint64_t> next{0};
+        std::vector<std::thread> th;
+        for (int t = 0; t < threads; ++t)
+            th.emplace_back([&]() {
+                for (uint64_t c; (c = next.fetch_add(1)) < nc;) brle::decode(data, out.data(), ptr.data(), c);
+            });
+        for (auto& x : th) x.join();
+        bytes += total;
+        dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    } while (dt < budget);
+    printf("%llu %.6f\n", (unsigned long long)bytes, dt);
+    return 0;
+}
+
 int main(int argc, char** argv) {
-    if (argc != 4) return 1;
+    if (argc < 4) return 1;
     std::vector<uint8_t> in = slurp(argv[2]);
+    if (!strcmp(argv[1], "bench")) return bench(in, atoi(argv[3]), argc > 4 ? atof(argv[4]) : 5.0);
     if (!strcmp(argv[1], "encode")) {
         const uint64_t n = in.size();
         const uint64_t nc = (n - 1) / CHUNK_SIZE + 1;

@@ -4,11 +4,18 @@
 // (lzss_gpu2.h:330-707), so one column = one call here.  Oracle tooling only.
 //   ref_lzss encode <raw> <stream>           lzss::compress_func, one chunk
 //   ref_lzss decode <stream> <n_out> <raw>    lzss::decompress_func
+//   ref_lzss bench <streams> <threads> <seconds>   lzss::decompress_func on every
+//       stream of a [u64 n][u64 bytes per stream][u64 offsets[n+1]][bytes] file
+//       on <threads> host threads, repeated for about <seconds>; prints
+//       "<bytes decoded> <seconds taken>"
 #include <lzss/lzss_cpu.h>
 
+#include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 static std::vector<uint8_t> slurp(const char* p) {
@@ -27,9 +34,39 @@ static void spit(const char* p, const void* d, size_t n) {
     fclose(f);
 }
 
+static int bench(const std::vector<uint8_t>& in, int threads, double budget) {
+    uint64_t n, nb;
+    memcpy(&n, in.data(), 8);
+    memcpy(&nb, in.data() + 8, 8);
+    std::vector<uint64_t> off(n + 1);
+    memcpy(off.data(), in.data() + 16, 8 * (n + 1));
+    const uint8_t* data = in.data() + 16 + 8 * (n + 1);
+    uint64_t bytes = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    double dt = 0;
+    do {
+        std::atomic<uint64_t> next{0};
+        std::vector<std::thread> th;
+        for (int t = 0; t < threads; ++t)
+            th.emplace_back([&]() {
+                std::vector<uint8_t> out(nb + 64);
+                for (uint64_t i; (i = next.fetch_add(1)) < n;) {
+                    const uint64_t lens[1] = {off[i + 1] - off[i]};
+                    lzss::decompress_func(data + off[i], out.data(), lens[0], nb, nb, 1, lens, 0);
+                }
+            });
+        for (auto& x : th) x.join();
+        bytes += n * nb;
+        dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    } while (dt < budget);
+    printf("%llu %.6f\n", (unsigned long long)bytes, dt);
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 4) return 1;
     std::vector<uint8_t> in = slurp(argv[2]);
+    if (!strcmp(argv[1], "bench")) return bench(in, atoi(argv[3]), argc > 4 ? atof(argv[4]) : 5.0);
     if (!strcmp(argv[1], "encode")) {
         const uint64_t n = in.size();
         const uint64_t oc = n + OVERHEAD_PER_CHUNK_((uint32_t)n) + 16;

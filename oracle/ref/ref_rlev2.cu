@@ -6,13 +6,20 @@
 // values (encoder_trans.h:9-289).  Oracle tooling only.
 //   ref_rlev2 encode <int64 raw> <stream>           block_encode, one chunk (<= 4096 values)
 //   ref_rlev2 decode <stream> <n_values> <int64 raw> block_decode
+//   ref_rlev2 bench <streams> <threads> <seconds>   block_decode of every stream
+//       of a [u64 n][u64 values per stream][u64 offsets[n+1]][bytes] file on
+//       <threads> host threads, repeated for about <seconds>; prints
+//       "<bytes decoded> <seconds taken>"
 #include <common.h>
 #include <rlev2/encoder.h>
 #include <rlev2/decoder.h>
 
+#include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 static std::vector<uint8_t> slurp(const char* p) {
@@ -31,9 +38,37 @@ static void spit(const char* p, const void* d, size_t n) {
     fclose(f);
 }
 
+static int bench(std::vector<uint8_t>& in, int threads, double budget) {
+    uint64_t n, nv;
+    memcpy(&n, in.data(), 8);
+    memcpy(&nv, in.data() + 8, 8);
+    std::vector<uint64_t> off(n + 1);
+    memcpy(off.data(), in.data() + 16, 8 * (n + 1));
+    uint8_t* data = in.data() + 16 + 8 * (n + 1);
+    uint64_t bytes = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    double dt = 0;
+    do {
+        std::atomic<uint64_t> next{0};
+        std::vector<std::thread> th;
+        for (int t = 0; t < threads; ++t)
+            th.emplace_back([&]() {
+                // decode_delta writes two values past a run (decoder.h:117-123): slack
+                std::vector<int64_t> out(CHUNK_SIZE / 8 + 16);
+                for (uint64_t i; (i = next.fetch_add(1)) < n;) rlev2::block_decode(0, data, off.data() + i, out.data());
+            });
+        for (auto& x : th) x.join();
+        bytes += n * nv * 8;
+        dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    } while (dt < budget);
+    printf("%llu %.6f\n", (unsigned long long)bytes, dt);
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 4) return 1;
     std::vector<uint8_t> in = slurp(argv[2]);
+    if (!strcmp(argv[1], "bench")) return bench(in, atoi(argv[3]), argc > 4 ? atof(argv[4]) : 5.0);
     if (!strcmp(argv[1], "encode")) {
         if (in.size() > CHUNK_SIZE) return 4;
         std::vector<uint8_t> out(OUTPUT_CHUNK_SIZE * 2, 0);
