@@ -3,6 +3,7 @@
 // and the per-thread device staging pool behind it.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -115,12 +116,95 @@ gd_status_t collect(const uint32_t* d_status, uint32_t n, cudaStream_t s) {
     return (gd_status_t)worst;
 }
 
+// Three non-blocking streams (host->device copies, decoding, device->host
+// copies) and their events, per host thread and device.
+constexpr int kMaxPieces = 32;
+struct Pipe {
+    int dev = -1;
+    cudaStream_t st[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t in_done[kMaxPieces], dec_done[kMaxPieces];
+    bool init() {
+        int d = 0;
+        cudaGetDevice(&d);
+        if (dev == d) return true;
+        if (dev >= 0) return false;  // one device per host thread for the pipelined path
+        for (auto& x : st)
+            if (cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking) != cudaSuccess) return false;
+        for (int i = 0; i < kMaxPieces; ++i)
+            if (cudaEventCreateWithFlags(&in_done[i], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&dec_done[i], cudaEventDisableTiming) != cudaSuccess)
+                return false;
+        dev = d;
+        return true;
+    }
+};
+thread_local Pipe g_pipe;
+
+// Host buffers in, host buffer out, in pieces of whole chunks: piece i's
+// host->device copy, its decode and its device->host copy run on three
+// streams, so copies in both directions (separate copy engines) overlap
+// decoding of the neighbouring pieces.  Chunk c's input is
+// h_in[in_at(c) .. in_at(c+1)) (copied to the same offset of d_in), its
+// output d_out[out_at(c) .. out_at(c+1)); both must be non-decreasing in c.
+// prologue(stream) issues the metadata copies (on the decode stream, before
+// the first decode); launch(a, b, stream) decodes chunks [a, b).  Decoders
+// read no input byte past their own chunks' streams that affects the
+// result, so a piece may decode while the next piece is still arriving.
+template <class InAt, class OutAt, class Prologue, class Launch>
+gd_status_t run_piped(uint64_t n, const uint8_t* h_in, uint8_t* d_in, InAt in_at, uint8_t* d_out, uint8_t* h_out,
+                      OutAt out_at, uint32_t* d_st, Prologue prologue, Launch launch, uint64_t pieces = 16) {
+    if (!g_pipe.init()) return GD_ERR_CUDA;
+    cudaStream_t si = g_pipe.st[0], sk = g_pipe.st[1], so = g_pipe.st[2];
+    const uint64_t total = out_at(n);
+    const uint64_t want = total / pieces > (4ull << 20) ? total / pieces : (4ull << 20);  // bytes out per piece
+    uint64_t cut[kMaxPieces + 1];
+    int np = 0;
+    cut[0] = 0;
+    for (uint64_t c = 0; c < n && np < kMaxPieces - 1;) {
+        uint64_t e = c + 1;
+        while (e < n && out_at(e) - out_at(c) < want) ++e;
+        cut[++np] = e;
+        c = e;
+    }
+    if (cut[np] != n) cut[++np] = n;
+    gd_status_t r = prologue(sk);
+    if (r != GD_OK) return r;
+    for (int i = 0; i < np; ++i) {
+        const uint64_t a = cut[i], b = cut[i + 1];
+        const uint64_t i0 = in_at(a), i1 = in_at(b);
+        if (i1 > i0 && cudaMemcpyAsync(d_in + i0, h_in + i0, i1 - i0, cudaMemcpyHostToDevice, si) != cudaSuccess)
+            return GD_ERR_CUDA;
+        cudaEventRecord(g_pipe.in_done[i], si);
+        cudaStreamWaitEvent(sk, g_pipe.in_done[i], 0);
+        r = launch(a, b, sk);
+        if (r != GD_OK) {
+            for (auto x : g_pipe.st) cudaStreamSynchronize(x);
+            return r;
+        }
+        cudaEventRecord(g_pipe.dec_done[i], sk);
+        cudaStreamWaitEvent(so, g_pipe.dec_done[i], 0);
+        const uint64_t o0 = out_at(a), o1 = out_at(b);
+        if (o1 > o0 && cudaMemcpyAsync(h_out + o0, d_out + o0, o1 - o0, cudaMemcpyDeviceToHost, so) != cudaSuccess)
+            return GD_ERR_CUDA;
+    }
+    if (cudaStreamSynchronize(so) != cudaSuccess) return GD_ERR_CUDA;
+    return collect(d_st, (uint32_t)n, sk);
+}
+
 template <typename T>
 T rd(const uint8_t* p) {
     T v;
     memcpy(&v, p, sizeof(T));
     return v;
 }
+
+// Deflate streams of chunk c: in[comp_off[c] .. + comp_len[c]), output
+// out[out_off[c] .. out_off[c+1]).  Pieced as run_piped when the streams lie
+// in chunk order; otherwise the whole input is copied with the first piece.
+// Fewer pieces than the other codecs: a piece ends with its longest stream.
+gd_status_t inflate_piped(const uint8_t* in, uint64_t in_n, const uint64_t* comp_off, const uint64_t* comp_len,
+                          const uint64_t* out_off, uint64_t n, int zlib_header, uint8_t* d_data, uint64_t* d_meta,
+                          uint8_t* d_out, uint8_t* h, uint32_t* d_st);
 
 }  // namespace
 
@@ -167,20 +251,26 @@ gd_status_t gd_brle_decompress(const uint8_t* in, uint64_t in_n_bytes, uint8_t**
         *out = (uint8_t*)malloc(1);
         return total == 0 ? GD_OK : GD_ERR_CORRUPT;
     }
-    cudaStream_t s = 0;
+    for (uint32_t c = 0; c < n_chunks; ++c)
+        if (ptr[c + 1] < ptr[c]) return GD_ERR_CORRUPT;
     uint8_t* d_data = (uint8_t*)g_pool.get(0, data_n);
     uint64_t* d_ptr = (uint64_t*)g_pool.get(1, 8ull * n_ptr);
     uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
     uint32_t* d_st = (uint32_t*)g_pool.get(3, 4ull * n_chunks);
     if (!d_data || !d_ptr || !d_out || !d_st) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(d_data, data, data_n, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_ptr, ptr.data(), 8ull * n_ptr, cudaMemcpyHostToDevice, s);
-    gd_status_t r = gd_brle_decode(d_data, d_ptr, n_chunks, chunk, d_out, total, d_st, s);
-    if (r != GD_OK) return r;
     uint8_t* h = (uint8_t*)pinned().get(total);
     if (!h) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
-    r = collect(d_st, n_chunks, s);
+    auto out_at = [&](uint64_t c) { return c * chunk < total ? c * chunk : total; };
+    gd_status_t r = run_piped(
+        n_chunks, data, d_data, [&](uint64_t c) { return ptr[c]; }, d_out, h, out_at, d_st,
+        [&](cudaStream_t st) {
+            return cudaMemcpyAsync(d_ptr, ptr.data(), 8ull * n_ptr, cudaMemcpyHostToDevice, st) == cudaSuccess
+                       ? GD_OK : GD_ERR_CUDA;
+        },
+        [&](uint64_t a, uint64_t b, cudaStream_t st) {
+            return gd_brle_decode(d_data, d_ptr + a, (uint32_t)(b - a), chunk, d_out + a * chunk,
+                                  out_at(b) - out_at(a), d_st + a, st);
+        });
     if (r != GD_OK) {
         gd_free(h);
         return r;
@@ -205,25 +295,30 @@ gd_status_t gd_rlev1_decompress(const uint8_t* in, uint64_t in_n_bytes, const ui
     if (blk_off[n] > data_n || total > n * chunk_size) return GD_ERR_CORRUPT;
     *out = nullptr;
     *out_n_bytes = 0;
-    cudaStream_t s = 0;
     uint8_t* d_data = (uint8_t*)g_pool.get(0, data_n);
     uint64_t* d_cl = (uint64_t*)g_pool.get(1, 8 * 32 * n);
     uint64_t* d_bo = (uint64_t*)g_pool.get(4, 8 * (n + 1));
     uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
     uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
     if (!d_data || !d_cl || !d_bo || !d_out || !d_st) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(d_data, data, data_n, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_cl, col_len, 8 * 32 * n, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_bo, blk_off, 8 * (n + 1), cudaMemcpyHostToDevice, s);
     uint64_t mx = 0;
     for (uint64_t i = 0; i < 32 * n; ++i) mx = col_len[i] > mx ? col_len[i] : mx;
-    gd_status_t r = gd_rlev1_decode(d_data, d_cl, d_bo, (uint32_t)n, chunk_size, comp_col_len, elem_bytes, d_out,
-                                    total, (uint32_t)(mx < 0xffffffffull ? mx : 0), d_st, s);
-    if (r != GD_OK) return r;
+    const bool mono = std::is_sorted(blk_off, blk_off + n + 1);
     uint8_t* h = (uint8_t*)pinned().get(total ? total : 1);
     if (!h) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
-    r = collect(d_st, (uint32_t)n, s);
+    auto out_at = [&](uint64_t c) { return c * chunk_size < total ? c * chunk_size : total; };
+    gd_status_t r = run_piped(
+        n, data, d_data, [&](uint64_t c) { return mono ? blk_off[c] : (c ? data_n : 0); }, d_out, h, out_at, d_st,
+        [&](cudaStream_t st) {
+            bool ok = cudaMemcpyAsync(d_cl, col_len, 8 * 32 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+            ok = ok && cudaMemcpyAsync(d_bo, blk_off, 8 * (n + 1), cudaMemcpyHostToDevice, st) == cudaSuccess;
+            return ok ? GD_OK : GD_ERR_CUDA;
+        },
+        [&](uint64_t a, uint64_t b, cudaStream_t st) {
+            return gd_rlev1_decode(d_data, d_cl + 32 * a, d_bo + a, (uint32_t)(b - a), chunk_size, comp_col_len,
+                                   elem_bytes, d_out + a * chunk_size, out_at(b) - out_at(a),
+                                   (uint32_t)(mx < 0xffffffffull ? mx : 0), d_st + a, st);
+        });
     if (r != GD_OK) {
         gd_free(h);
         return r;
@@ -244,25 +339,31 @@ gd_status_t gd_rlev2_decompress(const uint8_t* in, uint64_t in_n_bytes, uint64_t
     bo[n_chunks] = in_n_bytes;  // device API: last entry bounds the data
     *out = nullptr;
     *out_n_bytes = 0;
-    cudaStream_t s = 0;
     uint8_t* d_data = (uint8_t*)g_pool.get(0, in_n_bytes);
     uint64_t* d_cl = (uint64_t*)g_pool.get(1, 8 * 32 * n_chunks);
     uint64_t* d_bo = (uint64_t*)g_pool.get(4, 8 * (n_chunks + 1));
     uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
     uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n_chunks);
     if (!d_data || !d_cl || !d_bo || !d_out || !d_st) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(d_data, in, in_n_bytes, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_cl, col_len, 8 * 32 * n_chunks, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_bo, bo.data(), 8 * (n_chunks + 1), cudaMemcpyHostToDevice, s);
     uint64_t mx = 0;
     for (uint64_t i = 0; i < 32 * n_chunks; ++i) mx = col_len[i] > mx ? col_len[i] : mx;
-    gd_status_t r = gd_rlev2_decode(d_data, d_cl, d_bo, (uint32_t)n_chunks, chunk_size, read_unit, d_out, total,
-                                    (uint32_t)(mx < 0xffffffffull ? mx : 0), d_st, s);
-    if (r != GD_OK) return r;
+    const bool mono = std::is_sorted(bo.begin(), bo.end());
     uint8_t* h = (uint8_t*)pinned().get(total);
     if (!h) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
-    r = collect(d_st, (uint32_t)n_chunks, s);
+    auto out_at = [&](uint64_t c) { return c * chunk_size < total ? c * chunk_size : total; };
+    gd_status_t r = run_piped(
+        n_chunks, in, d_data, [&](uint64_t c) { return mono ? bo[c] : (c ? in_n_bytes : 0); }, d_out, h, out_at,
+        d_st,
+        [&](cudaStream_t st) {
+            bool ok = cudaMemcpyAsync(d_cl, col_len, 8 * 32 * n_chunks, cudaMemcpyHostToDevice, st) == cudaSuccess;
+            ok = ok && cudaMemcpyAsync(d_bo, bo.data(), 8 * (n_chunks + 1), cudaMemcpyHostToDevice, st) == cudaSuccess;
+            return ok ? GD_OK : GD_ERR_CUDA;
+        },
+        [&](uint64_t a, uint64_t b, cudaStream_t st) {
+            return gd_rlev2_decode(d_data, d_cl + 32 * a, d_bo + a, (uint32_t)(b - a), chunk_size, read_unit,
+                                   d_out + a * chunk_size, out_at(b) - out_at(a),
+                                   (uint32_t)(mx < 0xffffffffull ? mx : 0), d_st + a, st);
+        });
     if (r != GD_OK) {
         gd_free(h);
         return r;
@@ -286,7 +387,6 @@ int gd_lzss_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint8_t* co
     const uint64_t total = n * chunk;
     *out = nullptr;
     *out_n_bytes = 0;
-    cudaStream_t s = 0;
     uint8_t* d_data = (uint8_t*)g_pool.get(0, in_n_bytes);
     uint64_t* d_cl = (uint64_t*)g_pool.get(1, 8 * 32 * n);
     uint64_t* d_bo = (uint64_t*)g_pool.get(4, 8 * (n + 1));
@@ -294,16 +394,22 @@ int gd_lzss_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint8_t* co
     uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
     uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
     if (!d_data || !d_cl || !d_bo || !d_map || !d_out || !d_st) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(d_data, in, in_n_bytes, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_cl, meta[2], 8 * 32 * n, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_bo, bo.data(), 8 * (n + 1), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_map, meta[3], 32 * n, cudaMemcpyHostToDevice, s);
-    int r = gd_lzss_decode(d_data, d_bo, d_cl, d_map, (uint32_t)n, chunk, d_out, total, d_st, s);
-    if (r != GD_OK) return r;
+    const bool mono = std::is_sorted(bo.begin(), bo.end());
     uint8_t* h = (uint8_t*)pinned().get(total);
     if (!h) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
-    r = collect(d_st, (uint32_t)n, s);
+    int r = run_piped(
+        n, in, d_data, [&](uint64_t c) { return mono ? bo[c] : (c ? in_n_bytes : 0); }, d_out, h,
+        [&](uint64_t c) { return c * chunk; }, d_st,
+        [&](cudaStream_t st) {
+            bool ok = cudaMemcpyAsync(d_cl, meta[2], 8 * 32 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+            ok = ok && cudaMemcpyAsync(d_bo, bo.data(), 8 * (n + 1), cudaMemcpyHostToDevice, st) == cudaSuccess;
+            ok = ok && cudaMemcpyAsync(d_map, meta[3], 32 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+            return ok ? GD_OK : GD_ERR_CUDA;
+        },
+        [&](uint64_t a, uint64_t b, cudaStream_t st) {
+            return gd_lzss_decode(d_data, d_bo + a, d_cl + 32 * a, d_map + 32 * a, (uint32_t)(b - a), chunk,
+                                  d_out + a * chunk, (b - a) * chunk, d_st + a, st);
+        });
     if (r != GD_OK) {
         gd_free(h);
         return r;
@@ -333,22 +439,15 @@ gd_status_t gd_deflate_decompress(const uint8_t* in, uint64_t in_n_bytes, const 
     ooff[n] = total;
     *out = nullptr;
     *out_n_bytes = 0;
-    cudaStream_t s = 0;
     uint8_t* d_data = (uint8_t*)g_pool.get(0, in_n_bytes);
     uint64_t* d_meta = (uint64_t*)g_pool.get(1, 8 * (3 * n + 2));
     uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
     uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
     if (!d_data || !d_meta || !d_out || !d_st) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(d_data, in, in_n_bytes, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_meta, coff.data(), 8 * (n + 1), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_meta + n + 1, clen.data(), 8 * n, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_meta + 2 * n + 1, ooff.data(), 8 * (n + 1), cudaMemcpyHostToDevice, s);
-    gd_status_t r = gd_inflate(d_data, d_meta, d_meta + n + 1, d_meta + 2 * n + 1, (uint32_t)n, 1, d_out, d_st, s);
-    if (r != GD_OK) return r;
     uint8_t* h = (uint8_t*)pinned().get(total);
     if (!h) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
-    r = collect(d_st, (uint32_t)n, s);
+    gd_status_t r = inflate_piped(in, in_n_bytes, coff.data(), clen.data(), ooff.data(), n, 1, d_data, d_meta, d_out,
+                                  h, d_st);
     if (r != GD_OK) {
         gd_free(h);
         return r;
@@ -380,20 +479,25 @@ gd_status_t gd_lzss_contig_decompress(const uint8_t* in, uint64_t in_n_bytes, ui
     if (ends[n - 1] > dlen) return GD_ERR_CORRUPT;
     *out = nullptr;
     *out_n_bytes = 0;
-    cudaStream_t s = 0;
     uint8_t* d_data = (uint8_t*)g_pool.get(0, dlen + 16);
     uint64_t* d_ends = (uint64_t*)g_pool.get(1, 8 * n);
     uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
     uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
     if (!d_data || !d_ends || !d_out || !d_st) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(d_data, in + 28 + 8 * n, dlen, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_ends, ends.data(), 8 * n, cudaMemcpyHostToDevice, s);
-    gd_status_t r = gd_lzss_contig_decode(d_data, d_ends, (uint32_t)n, chunk, d_out, total, d_st, s);
-    if (r != GD_OK) return r;
     uint8_t* h = (uint8_t*)pinned().get(total);
     if (!h) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
-    r = collect(d_st, (uint32_t)n, s);
+    // one piece: a chunk's stream starts where the previous chunk's ends
+    gd_status_t r = run_piped(
+        n, in + 28 + 8 * n, d_data, [&](uint64_t c) { return c ? dlen : 0; }, d_out, h,
+        [&](uint64_t c) { return c * chunk < total ? c * chunk : total; }, d_st,
+        [&](cudaStream_t st) {
+            return cudaMemcpyAsync(d_ends, ends.data(), 8 * n, cudaMemcpyHostToDevice, st) == cudaSuccess
+                       ? GD_OK : GD_ERR_CUDA;
+        },
+        [&](uint64_t, uint64_t, cudaStream_t st) {
+            return gd_lzss_contig_decode(d_data, d_ends, (uint32_t)n, chunk, d_out, total, d_st, st);
+        },
+        1);
     if (r != GD_OK) {
         gd_free(h);
         return r;
@@ -420,7 +524,6 @@ gd_status_t gd_brle_trans_decompress(const uint8_t* in, uint64_t in_n_bytes, con
     const uint64_t total = n * chunk_size;
     *out = nullptr;
     *out_n_bytes = 0;
-    cudaStream_t s = 0;
     uint8_t* d_data = (uint8_t*)g_pool.get(0, in_n_bytes + 16);
     uint64_t* d_cl = (uint64_t*)g_pool.get(1, 8 * 32 * n);
     uint64_t* d_bo = (uint64_t*)g_pool.get(4, 8 * (n + 1));
@@ -428,16 +531,22 @@ gd_status_t gd_brle_trans_decompress(const uint8_t* in, uint64_t in_n_bytes, con
     uint8_t* d_out = (uint8_t*)g_pool.get(2, total);
     uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
     if (!d_data || !d_cl || !d_bo || !d_map || !d_out || !d_st) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(d_data, in, in_n_bytes, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_cl, col_len, 8 * 32 * n, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_bo, blk_off, 8 * (n + 1), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_map, col_map, 32 * n, cudaMemcpyHostToDevice, s);
-    gd_status_t r = gd_brle_trans_decode(d_data, d_bo, d_cl, d_map, (uint32_t)n, chunk_size, d_out, total, d_st, s);
-    if (r != GD_OK) return r;
+    const bool mono = std::is_sorted(blk_off, blk_off + n + 1);
     uint8_t* h = (uint8_t*)pinned().get(total);
     if (!h) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
-    r = collect(d_st, (uint32_t)n, s);
+    gd_status_t r = run_piped(
+        n, in, d_data, [&](uint64_t c) { return mono ? blk_off[c] : (c ? in_n_bytes : 0); }, d_out, h,
+        [&](uint64_t c) { return c * chunk_size; }, d_st,
+        [&](cudaStream_t st) {
+            bool ok = cudaMemcpyAsync(d_cl, col_len, 8 * 32 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+            ok = ok && cudaMemcpyAsync(d_bo, blk_off, 8 * (n + 1), cudaMemcpyHostToDevice, st) == cudaSuccess;
+            ok = ok && cudaMemcpyAsync(d_map, col_map, 32 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+            return ok ? GD_OK : GD_ERR_CUDA;
+        },
+        [&](uint64_t a, uint64_t b, cudaStream_t st) {
+            return gd_brle_trans_decode(d_data, d_bo + a, d_cl + 32 * a, d_map + 32 * a, (uint32_t)(b - a),
+                                        chunk_size, d_out + a * chunk_size, (b - a) * chunk_size, d_st + a, st);
+        });
     if (r != GD_OK) {
         gd_free(h);
         return r;
@@ -463,23 +572,15 @@ gd_status_t gd_inflate_decompress(const uint8_t* in, uint64_t in_n_bytes, const 
     const uint64_t total = out_off[n];
     *out = nullptr;
     *out_n_bytes = 0;
-    cudaStream_t s = 0;
     uint8_t* d_data = (uint8_t*)g_pool.get(0, in_n_bytes + 16);
     uint64_t* d_meta = (uint64_t*)g_pool.get(1, 8 * (3 * n + 2));
     uint8_t* d_out = (uint8_t*)g_pool.get(2, total ? total : 1);
     uint32_t* d_st = (uint32_t*)g_pool.get(3, 4 * n);
     if (!d_data || !d_meta || !d_out || !d_st) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(d_data, in, in_n_bytes, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_meta, comp_off, 8 * n, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_meta + n + 1, comp_len, 8 * n, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_meta + 2 * n + 1, out_off, 8 * (n + 1), cudaMemcpyHostToDevice, s);
-    gd_status_t r = gd_inflate(d_data, d_meta, d_meta + n + 1, d_meta + 2 * n + 1, (uint32_t)n, zlib_header, d_out,
-                               d_st, s);
-    if (r != GD_OK) return r;
     uint8_t* h = (uint8_t*)pinned().get(total ? total : 1);
     if (!h) return GD_ERR_NOMEM;
-    cudaMemcpyAsync(h, d_out, total, cudaMemcpyDeviceToHost, s);
-    r = collect(d_st, (uint32_t)n, s);
+    gd_status_t r = inflate_piped(in, in_n_bytes, comp_off, comp_len, out_off, n, zlib_header, d_data, d_meta, d_out,
+                                  h, d_st);
     if (r != GD_OK) {
         gd_free(h);
         return r;
@@ -490,3 +591,30 @@ gd_status_t gd_inflate_decompress(const uint8_t* in, uint64_t in_n_bytes, const 
 }
 
 }  // extern "C"
+
+namespace {
+gd_status_t inflate_piped(const uint8_t* in, uint64_t in_n, const uint64_t* comp_off, const uint64_t* comp_len,
+                          const uint64_t* out_off, uint64_t n, int zlib_header, uint8_t* d_data, uint64_t* d_meta,
+                          uint8_t* d_out, uint8_t* h, uint32_t* d_st) {
+    bool mono = true;
+    for (uint64_t i = 0; i + 1 < n && mono; ++i) mono = comp_off[i] + comp_len[i] <= comp_off[i + 1];
+    auto in_at = [&](uint64_t c) -> uint64_t {
+        if (!mono) return c ? in_n : 0;
+        return c < n ? comp_off[c] : in_n;
+    };
+    return run_piped(
+        n, in, d_data, in_at, d_out, h, [&](uint64_t c) { return out_off[c]; }, d_st,
+        [&](cudaStream_t st) {
+            bool ok = cudaMemcpyAsync(d_meta, comp_off, 8 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+            ok = ok && cudaMemcpyAsync(d_meta + n + 1, comp_len, 8 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+            ok = ok && cudaMemcpyAsync(d_meta + 2 * n + 1, out_off, 8 * (n + 1), cudaMemcpyHostToDevice, st) ==
+                           cudaSuccess;
+            return ok ? GD_OK : GD_ERR_CUDA;
+        },
+        [&](uint64_t a, uint64_t b, cudaStream_t st) {
+            return gd_inflate(d_data, d_meta + a, d_meta + n + 1 + a, d_meta + 2 * n + 1 + a, (uint32_t)(b - a),
+                              zlib_header, d_out, d_st + a, st);
+        },
+        4);
+}
+}  // namespace

@@ -5,7 +5,8 @@
 namespace gd {
 namespace lzss {
 
-// WPB: warps (chunks) per block, 4 by default (GD_TUNE_LZSS_WARPS_PER_BLOCK)
+// WPB: warps (chunks) per block (GD_TUNE_LZSS_WARPS_PER_BLOCK 2 / 4 / 8; also
+// the path for chunks too large to stage in shared memory)
 template <int WPB>
 __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restrict__ data,
                                                          const uint64_t* __restrict__ blk_off,
@@ -28,6 +29,49 @@ __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restr
     if (lane_id() == 0) put_status(status, chunk, err);
 }
 
+// One warp per block and chunk; the chunk's output is staged in shared memory
+// (chunk_warp_staged), so blocks per SM = shared memory / staged_smem(chunk).
+__global__ void __launch_bounds__(32) decode_staged_kernel(const uint8_t* __restrict__ data,
+                                                           const uint64_t* __restrict__ blk_off,
+                                                           const uint64_t* __restrict__ col_len,
+                                                           const uint8_t* __restrict__ col_map, uint32_t n_chunks,
+                                                           uint64_t chunk_size, uint8_t* out,
+                                                           uint32_t* __restrict__ status) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const uint32_t chunk = blockIdx.x;
+    if (chunk >= n_chunks) return;
+    const uint64_t b0 = blk_off[chunk], b1 = blk_off[chunk + 1];
+    uint32_t err;
+    if (b1 < b0) {
+        err = ST_CORRUPT;
+    } else {
+        err = chunk_warp_staged(data + b0, b1 - b0, col_len + 32ull * chunk, col_map + 32ull * chunk, chunk_size,
+                                out + (uint64_t)chunk * chunk_size, smem);
+    }
+    if (lane_id() == 0) put_status(status, chunk, err);
+}
+
+// One 256-thread block per chunk, 8 lanes per column (chunk_block_cols).
+__global__ void __launch_bounds__(256) decode_cols_kernel(const uint8_t* __restrict__ data,
+                                                          const uint64_t* __restrict__ blk_off,
+                                                          const uint64_t* __restrict__ col_len,
+                                                          const uint8_t* __restrict__ col_map, uint32_t n_chunks,
+                                                          uint64_t chunk_size, uint8_t* out,
+                                                          uint32_t* __restrict__ status) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const uint32_t chunk = blockIdx.x;
+    if (chunk >= n_chunks) return;  // block-uniform
+    const uint64_t b0 = blk_off[chunk], b1 = blk_off[chunk + 1];
+    uint32_t err;
+    if (b1 < b0) {
+        err = ST_CORRUPT;
+    } else {
+        err = chunk_block_cols(data + b0, b1 - b0, col_len + 32ull * chunk, col_map + 32ull * chunk, chunk_size,
+                               out + (uint64_t)chunk * chunk_size, smem);
+    }
+    if (threadIdx.x == 0) put_status(status, chunk, err);
+}
+
 }  // namespace lzss
 }  // namespace gd
 
@@ -43,7 +87,27 @@ extern "C" gd_status_t gd_lzss_decode(const uint8_t* d_data, const uint64_t* d_b
     if (out_n_bytes != chunk_size * (uint64_t)n_chunks) return GD_ERR_INVALID_ARG;
     if ((reinterpret_cast<uintptr_t>(d_out) & 3u) != 0) return GD_ERR_INVALID_ARG;
     using namespace gd::lzss;
+    // the staged decoder holds a whole chunk in shared memory; it needs
+    // 16-byte aligned output for its row stores
+    const uint32_t staged = staged_smem(chunk_size);
     const int k = gd_tune_get(GD_TUNE_LZSS_WARPS_PER_BLOCK);
+    const uint32_t cs = cols_smem(chunk_size);
+    if (k == 0 && cs <= 227u * 1024u) {
+        cudaFuncSetAttribute(decode_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cs);
+        cudaFuncSetAttribute(decode_cols_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+        decode_cols_kernel<<<n_chunks, 256, cs, (cudaStream_t)stream>>>(d_data, d_blk_off, d_col_len, d_col_map,
+                                                                       n_chunks, chunk_size, d_out, d_status);
+        return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+    }
+    if (k <= 1 && staged <= 227u * 1024u && (reinterpret_cast<uintptr_t>(d_out) & 15u) == 0) {
+        cudaFuncSetAttribute(decode_staged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, staged);
+        cudaFuncSetAttribute(decode_staged_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+        decode_staged_kernel<<<n_chunks, 32, staged, (cudaStream_t)stream>>>(d_data, d_blk_off, d_col_len, d_col_map,
+                                                                            n_chunks, chunk_size, d_out, d_status);
+        return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+    }
     const int wpb = (k == 2 || k == 8) ? k : 4;
     auto go = [&](auto kern) {
         const uint32_t smem = (uint32_t)wpb * WARP_SMEM;

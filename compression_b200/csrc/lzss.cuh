@@ -152,6 +152,389 @@ static __device__ __noinline__ uint32_t chunk_warp(const uint8_t* __restrict__ b
     return __reduce_max_sync(GD_FULL_MASK, err);
 }
 
+// ---------------------------------------------------------------------------
+// Staged decoder: the chunk's whole output lives in shared memory.
+//
+// The output is staged in its final layout (row k = the k-th 4-byte word of
+// all 32 columns, 128 bytes), so column q's words are all in bank q: the 32
+// lanes (one column each) never conflict, and a match source anywhere in the
+// column's history is a shared-memory read.  A lane handles one flag group
+// (8 tokens) per step: token positions follow from the flag byte alone, so
+// the 8 tokens' bytes and their match sources (8 bytes each, read before any
+// of the group's output is written) are loaded together; then the tokens are
+// appended in order through a register holding the column's partial word.
+// A source that reaches into the group's own output is re-read when its token
+// is appended; long (> 8 byte) and self-overlapping (offset < length)
+// matches take a 4- or 1-byte loop (byte-exact for every offset >= 1, as the
+// reference's byte-wise copy).  The compressed words of each lane stream are
+// prefetched into a per-lane ring with cp.async, well ahead of use.  When
+// every column is complete the warp writes the staged rows with 16-byte
+// stores.
+// ---------------------------------------------------------------------------
+constexpr uint32_t STAGE_PAD = 256;  // two rows past the chunk: 8-byte source reads and the carry word
+__host__ __device__ constexpr uint32_t staged_smem(uint64_t chunk_size) {
+    return (uint32_t)chunk_size + STAGE_PAD + 32u * RING_STRIDE + (uint32_t)sizeof(SegTable);
+}
+
+// Per-lane asynchronous ring over the lane's words: bytes [rd, arrived) are
+// readable, [arrived, fl) are in flight.
+__device__ __forceinline__ void ring_prefetch(LaneRing& r, LaneWords& w, const SegTable* T, const uint8_t* block,
+                                              uint32_t ltmask) {
+    uint32_t n = 0;
+    while (w.k < w.nw && r.fl - r.rd <= (uint32_t)RING - 4u) {
+        const uint32_t off = lw_addr(w, T, ltmask, w.k);
+        const uint32_t sa = (uint32_t)__cvta_generic_to_shared(r.buf + (r.fl & (RING - 1)));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(block + off) : "memory");
+        r.fl += 4;
+        ++w.k;
+        ++n;
+    }
+    if (n) asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+static __device__ __noinline__ uint32_t chunk_warp_staged(const uint8_t* __restrict__ block, uint64_t b_len,
+                                                         const uint64_t* __restrict__ col_len,
+                                                         const uint8_t* __restrict__ col_map, uint64_t chunk_size,
+                                                         uint8_t* __restrict__ cout, uint8_t* wsmem) {
+    const uint32_t lane = lane_id();
+    uint8_t* stage = wsmem;
+    uint8_t* ring = wsmem + chunk_size + STAGE_PAD;
+    SegTable* T_ = reinterpret_cast<SegTable*>(ring + 32 * RING_STRIDE);
+
+    uint32_t err = ST_OK;
+    const uint64_t len64 = col_len[lane];
+    const uint32_t len = len64 > 0x3fffffffull ? 0u : (uint32_t)len64;
+    if (len64 > 0x3fffffffull) err = ST_CORRUPT;
+    const uint32_t q = col_map[lane];
+    if (q >= 32) err = ST_CORRUPT;
+    {  // col_map must be a permutation of the 32 columns
+        uint32_t bits = 0;
+#pragma unroll
+        for (int o = 0; o < 32; ++o) bits |= 1u << (__shfl_sync(GD_FULL_MASK, q, o) & 31u);
+        if (bits != 0xffffffffu) err = ST_CORRUPT;
+    }
+    const uint32_t nw = (len + 3) >> 2;
+    uint32_t tot = warp_incl_scan(nw);
+    tot = __shfl_sync(GD_FULL_MASK, tot, 31);
+    if ((uint64_t)tot * 4 > b_len) err = ST_CORRUPT;
+    if ((reinterpret_cast<uintptr_t>(block) & 3u) != 0) err = ST_CORRUPT;  // words are 4-byte copies
+    if (chunk_size == 0 || chunk_size % 128 || chunk_size > (1ull << 31)) err = ST_INVALID;
+    if (__any_sync(GD_FULL_MASK, err != ST_OK)) return __reduce_max_sync(GD_FULL_MASK, err);
+    seg_build(T_, nw);
+    const uint32_t ltmask = (1u << lane) - 1u;
+    LaneWords lw;
+    lw_init(lw, T_, nw);
+    LaneRing r{ring + lane * RING_STRIDE, 0, 0, len};
+    uint32_t arrived = 0;
+    ring_prefetch(r, lw, T_, block, ltmask);
+
+    const uint32_t col_bytes = (uint32_t)(chunk_size / 32);
+    // column q's word k is stg[32k]
+    uint32_t* stg = reinterpret_cast<uint32_t*>(stage) + q;
+    uint32_t o = 0, acc = 0;  // column bytes produced; the bytes of the partial word o >> 2
+
+    // append the n (1..8) low bytes of x (zero above them): the partial word,
+    // the word after it and the one after that are stored unconditionally
+    // (bytes past o are rewritten before anything reads them)
+    auto put = [&](uint64_t x, uint32_t n) {
+        const uint32_t b = o & 3u, sh = b * 8u;
+        uint32_t* w = stg + 32u * (o >> 2);
+        const uint64_t v = (uint64_t)acc | (x << sh);
+        const uint32_t hi = sh ? (uint32_t)(x >> (64u - sh)) : 0u;
+        w[0] = (uint32_t)v;
+        w[32] = (uint32_t)(v >> 32);
+        w[64] = hi;
+        const uint32_t e = b + n;
+        acc = e < 4u ? (uint32_t)v : (e < 8u ? (uint32_t)(v >> 32) : hi);
+        o += n;
+    };
+    auto rd8 = [&](uint32_t sp) -> uint64_t {  // column bytes sp .. sp+7
+        const uint32_t* w = stg + 32u * (sp >> 2);
+        const uint32_t sh = (sp & 3u) * 8u, w1 = w[32];
+        return ((uint64_t)__funnelshift_r(w1, w[64], sh) << 32) | __funnelshift_r(w[0], w1, sh);
+    };
+    auto mask = [](uint32_t n) -> uint64_t { return n >= 8u ? ~0ull : ((1ull << (8u * n)) - 1ull); };
+
+    for (;;) {
+        const bool act = (o < col_bytes) && (err == ST_OK);
+        if (!__any_sync(GD_FULL_MASK, act)) break;
+        // top up every lane's ring together once any active lane is half empty
+        const bool low = act && (r.fl - r.rd <= (uint32_t)RING / 2) && (lw.k < lw.nw);
+        if (__any_sync(GD_FULL_MASK, low)) ring_prefetch(r, lw, T_, block, ltmask);
+        if (!act) continue;
+        // the group reads bytes rd .. rd+16
+        if (arrived < r.fl && arrived < r.rd + 17u) {
+            asm volatile("cp.async.wait_all;\n" ::: "memory");
+            arrived = r.fl;
+        }
+        if (r.rd >= r.len) {
+            err = ST_CORRUPT;
+            continue;
+        }
+        const uint32_t flag = ring_byte(r, r.rd);
+        // the group's tokens: first and second byte
+        uint32_t b0[8], b1[8];
+        {
+            uint32_t p = r.rd + 1u;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                b0[t] = ring_byte(r, p);
+                b1[t] = ring_byte(r, p + 1u);
+                p += 2u - ((flag >> t) & 1u);
+            }
+        }
+        // lengths and sources; a bad token ends the group (and the column)
+        uint32_t L[8], src[8];
+        uint32_t used = 1;  // group bytes consumed
+        {
+            uint32_t oo = o, p = r.rd + 1u;
+            bool stop = false;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                const bool lit = (flag >> t) & 1u;
+                const uint32_t v = b0[t] | (b1[t] << 8);
+                const uint32_t ml = lit ? 1u : (v & 31u) + 3u, off = lit ? 0u : v >> 5;
+                const bool live = !stop && oo < col_bytes;
+                const bool nobytes = p + (lit ? 0u : 1u) >= r.len;
+                const bool badoff = !lit && (off == 0 || off > oo);
+                const bool over = oo + ml > col_bytes;
+                if (live && (nobytes || badoff || over)) {
+                    err = (nobytes || badoff) ? ST_CORRUPT : ST_OVERRUN;
+                    stop = true;
+                }
+                const bool ok = live && !stop;
+                L[t] = ok ? ml : 0u;
+                src[t] = ok ? oo - off : 0u;
+                oo += ok ? ml : 0u;
+                used += ok ? (lit ? 1u : 2u) : 0u;
+                p += lit ? 1u : 2u;
+            }
+        }
+        // match sources as they are before this group writes anything
+        uint64_t x[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) x[t] = (L[t] && !((flag >> t) & 1u)) ? rd8(src[t]) : (uint64_t)b0[t];
+        const uint32_t o0 = o;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const uint32_t n = L[t];
+            if (n == 0) continue;
+            const uint32_t sp = src[t], off = o - sp;
+            const bool lit = (flag >> t) & 1u;
+            if (lit || (n <= 8u && off >= n)) {
+                // a source reaching into this group's output is re-read now
+                const uint64_t v = (!lit && sp + n > o0) ? rd8(sp) : x[t];
+                put(v & mask(n), n);
+            } else {
+                // long or self-overlapping match: each piece is read after the
+                // bytes before it are written
+                const uint32_t step = off >= 8u ? 8u : (off >= 4u ? 4u : 1u);
+                for (uint32_t j = 0; j < n; j += step) {
+                    const uint32_t m = min(step, n - j);
+                    put(rd8(sp + j) & mask(m), m);
+                }
+            }
+        }
+        r.rd += used;
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (err == ST_OK && o != col_bytes) err = ST_CORRUPT;
+    err = __reduce_max_sync(GD_FULL_MASK, err);
+    __syncwarp();
+    if (err == ST_OK) {
+        const uint4* s4 = reinterpret_cast<const uint4*>(stage);
+        uint4* d4 = reinterpret_cast<uint4*>(cout);
+        const uint32_t n16 = (uint32_t)(chunk_size / 16);
+        for (uint32_t i = lane; i < n16; i += 32) d4[i] = s4[i];
+    }
+    return err;
+}
+
+// ---------------------------------------------------------------------------
+// Column-group decoder: one block of 8 warps per chunk, 8 lanes per column.
+//
+// Lanes 8s..8s+7 of warp w decode column rank 4w+s, one flag group per step:
+// lane t takes token t of the group (its bytes follow from the flag byte
+// alone), the 8 lengths are prefix-summed across the lanes for the output
+// offsets, and every token is written at once -- literals and matches whose
+// source lies before the group (almost all) in one pass, the rest (source
+// inside the group, offset below the length) in token order afterwards.  The
+// chunk's output is staged column by column in shared memory (column q at
+// q*(col_bytes+4): 8-byte source reads are one funnel shift, and the final
+// row-major writes read the 32 columns of a row from 32 different banks).
+// Each column's compressed words arrive in a per-column ring by cp.async,
+// issued by the column's 8 lanes half a ring ahead of use.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr uint32_t cols_stride(uint64_t chunk_size) { return (uint32_t)(chunk_size / 32) + 4u; }
+__host__ __device__ constexpr uint32_t cols_smem(uint64_t chunk_size) {
+    return 32u * cols_stride(chunk_size) + 16u + 32u * RING_STRIDE + (uint32_t)sizeof(SegTable) + 32u * 8u + 16u;
+}
+
+// Must be called by all 256 threads of the block; returns the chunk status.
+static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __restrict__ block, uint64_t b_len,
+                                                           const uint64_t* __restrict__ col_len,
+                                                           const uint8_t* __restrict__ col_map,
+                                                           uint64_t chunk_size, uint8_t* __restrict__ cout,
+                                                           uint8_t* smem) {
+    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+    const uint32_t cstr = cols_stride(chunk_size);
+    uint8_t* stage = smem;
+    uint8_t* ring = smem + 32u * cstr + 16u;
+    SegTable* T_ = reinterpret_cast<SegTable*>(ring + 32 * RING_STRIDE);
+    uint32_t* s_q = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(T_) + sizeof(SegTable));
+    uint32_t* s_len = s_q + 32;
+    uint32_t* s_err = s_len + 32;
+
+    // ---- warp 0: metadata checks and the segment table ----
+    if (wid == 0) {
+        uint32_t err = ST_OK;
+        const uint64_t len64 = col_len[lane];
+        const uint32_t len = len64 > 0x3fffffffull ? 0u : (uint32_t)len64;
+        if (len64 > 0x3fffffffull) err = ST_CORRUPT;
+        const uint32_t q = col_map[lane];
+        if (q >= 32) err = ST_CORRUPT;
+        uint32_t bits = 0;
+#pragma unroll
+        for (int o = 0; o < 32; ++o) bits |= 1u << (__shfl_sync(GD_FULL_MASK, q, o) & 31u);
+        if (bits != 0xffffffffu) err = ST_CORRUPT;
+        const uint32_t nw = (len + 3) >> 2;
+        uint32_t tot = warp_incl_scan(nw);
+        tot = __shfl_sync(GD_FULL_MASK, tot, 31);
+        if ((uint64_t)tot * 4 > b_len) err = ST_CORRUPT;
+        if ((reinterpret_cast<uintptr_t>(block) & 3u) != 0) err = ST_CORRUPT;
+        if (chunk_size == 0 || chunk_size % 128 || chunk_size > (1ull << 31)) err = ST_INVALID;
+        err = __reduce_max_sync(GD_FULL_MASK, err);
+        if (err == ST_OK) seg_build(T_, nw);
+        s_q[lane] = q & 31u;
+        s_len[lane] = len;
+        if (lane == 0) *s_err = err;
+    }
+    __syncthreads();
+    if (*s_err != ST_OK) return *s_err;
+
+    const uint32_t sub = lane >> 3, t = lane & 7u;
+    const uint32_t rank = 4u * wid + sub;
+    const uint32_t seg0 = 8u * sub;  // first lane of this column's group
+    const uint32_t q = s_q[rank], len = s_len[rank];
+    const uint32_t nw = (len + 3) >> 2;
+    const uint32_t col_bytes = (uint32_t)(chunk_size / 32);
+    uint8_t* col = stage + q * cstr;
+    const uint8_t* rbuf = ring + rank * RING_STRIDE;
+    const uint32_t ltmask = (1u << rank) - 1u;
+    LaneWords lw;
+    lw.k = 0;
+    lw.nw = nw;
+    lw.j = 0;
+    lw_seek_seg(lw, T_, ltmask);
+    uint32_t nextk = t;  // this lane copies words t, t+8, t+16, ... of the stream
+
+    // column state, identical in the column's 8 lanes
+    uint32_t rd = 0, o = 0, fl = 0, arrived = 0, err = ST_OK;
+
+    auto prefetch = [&]() {  // top the ring up to 63 words past rd's word
+        const uint32_t tgt = min(nw, (rd >> 2) + 63u);
+        uint32_t n = 0;
+        for (; nextk < tgt; nextk += 8) {
+            const uint32_t off = lw_addr(lw, T_, ltmask, nextk);
+            const uint32_t sa = (uint32_t)__cvta_generic_to_shared(rbuf + ((4u * nextk) & (RING - 1)));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(block + off) : "memory");
+            ++n;
+        }
+        if (n) asm volatile("cp.async.commit_group;\n" ::: "memory");
+        fl = max(fl, 4u * tgt);
+    };
+    auto rb = [&](uint32_t p) -> uint32_t { return rbuf[p & (RING - 1)]; };
+    auto rd8 = [&](uint32_t sp) -> uint64_t {  // column bytes sp .. sp+7
+        const uint8_t* a = col + (sp & ~3u);
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(a);
+        const uint32_t sh = (sp & 3u) * 8u, w1 = w[1];
+        return ((uint64_t)__funnelshift_r(w1, w[2], sh) << 32) | __funnelshift_r(w[0], w1, sh);
+    };
+
+    prefetch();
+    for (;;) {
+        const bool act = (o < col_bytes) && (err == ST_OK);
+        if (!__any_sync(GD_FULL_MASK, act)) break;
+        if (act && fl - rd <= (uint32_t)RING / 2 && fl < 4u * nw) prefetch();
+        // the group reads bytes rd .. rd+16, copied by all 8 lanes of the column
+        const bool wait = act && arrived < fl && arrived < rd + 17u;
+        if (__any_sync(GD_FULL_MASK, wait)) {
+            asm volatile("cp.async.wait_all;\n" ::: "memory");
+            __syncwarp();
+            arrived = fl;
+        }
+        uint32_t L = 0, src = 0, ot = 0, lit = 0, code = ST_OK, flag = 0, b0 = 0;
+        const uint32_t o0 = o;  // the group's first output byte
+        bool exists = false;
+        if (act) {
+            if (rd >= len) code = ST_CORRUPT;
+            flag = rb(rd);
+            lit = (flag >> t) & 1u;
+            const uint32_t pos = rd + 1u + t + __popc(~flag & ((1u << t) - 1u));
+            b0 = rb(pos);
+            const uint32_t v = b0 | (rb(pos + 1u) << 8);
+            L = lit ? 1u : (v & 31u) + 3u;
+            uint32_t inc = L;
+#pragma unroll
+            for (uint32_t d = 1; d < 8; d <<= 1) {
+                const uint32_t n = __shfl_up_sync(0xffu << seg0, inc, d, 8);
+                if (t >= d) inc += n;
+            }
+            ot = o + inc - L;
+            exists = ot < col_bytes;
+            const uint32_t off = lit ? 0u : v >> 5;
+            if (exists && code == ST_OK) {
+                if (pos + (lit ? 0u : 1u) >= len || (!lit && (off == 0 || off > ot))) code = ST_CORRUPT;
+                else if (ot + L > col_bytes) code = ST_OVERRUN;
+            }
+            src = ot - off;
+            // the first bad token of the group decides the column's status
+            const uint32_t bad = __ballot_sync(0xffu << seg0, code != ST_OK) >> seg0;
+            if (bad) {
+                err = __shfl_sync(0xffu << seg0, code, seg0 + __ffs(bad) - 1u);
+            } else {
+                const uint32_t total = __shfl_sync(0xffu << seg0, inc, seg0 + 7u);
+                o = min(o + total, col_bytes);
+                rd += 17u - __popc(flag);
+            }
+            if (err != ST_OK) exists = false;
+        }
+        // pass 1: literals and matches whose source lies before the group
+        const bool dep = exists && !lit && src + L > o0;
+        if (exists && !dep) {
+            if (lit) {
+                col[ot] = (uint8_t)b0;
+            } else {
+                for (uint32_t j = 0; j < L; j += 8) {
+                    const uint64_t x = rd8(src + j);
+                    const uint32_t m = min(8u, L - j);
+                    for (uint32_t i = 0; i < m; ++i) col[ot + j + i] = (uint8_t)(x >> (8u * i));
+                }
+            }
+        }
+        // pass 2: the rest in token order, byte by byte
+        if (__any_sync(GD_FULL_MASK, dep)) {
+            for (uint32_t tt = 0; tt < 8; ++tt) {
+                __syncwarp();
+                if (dep && t == tt)
+                    for (uint32_t j = 0; j < L; ++j) col[ot + j] = col[src + j];
+            }
+        }
+        __syncwarp();
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (t == 0 && (err != ST_OK || o != col_bytes)) atomicMax(s_err, err != ST_OK ? err : (uint32_t)ST_CORRUPT);
+    __syncthreads();
+    const uint32_t e = *s_err;
+    if (e == ST_OK) {
+        // row k of the chunk = word k of columns 0..31
+        const uint32_t rows = col_bytes / 4u;
+        uint32_t* o32 = reinterpret_cast<uint32_t*>(cout);
+        for (uint32_t k = wid; k < rows; k += 8)
+            o32[32u * k + lane] = *reinterpret_cast<const uint32_t*>(stage + lane * cstr + 4u * k);
+    }
+    return e;
+}
 
 }  // namespace lzss
 }  // namespace gd

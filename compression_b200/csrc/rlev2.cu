@@ -3,12 +3,14 @@
 // A block of 4 (or 8) warps owns as many adjacent lane streams of one chunk and copies
 // them from the interleaved block into shared memory.  Then, in batches of
 // up to RCAP runs per stream:
-//   * parse: lanes 0..3 of warp 0 each walk one stream's run boundaries
-//     (the only serial part of the format: a run's byte length follows from
-//     its first header bytes), recording each run's header offset and first
-//     value index; then
-//     all threads decode the recorded headers -- kind, widths, bit offset of
-//     the packed data, base, delta -- into a shared-memory run table;
+//   * parse: lane 0 of warp w walks stream w's run boundaries (the only
+//     serial part of the format: a run's byte length follows from its first
+//     header bytes), recording each run's header offset and first value
+//     index; then the warp's lanes decode the recorded headers -- kind,
+//     widths, bit offset of the packed data, base, delta -- into the warp's
+//     shared-memory run table.  After the copy into shared memory the warps
+//     of a block never wait on each other, so one warp's walk overlaps the
+//     others' expansion;
 //   * expand: warp w produces the values of stream w, 32 consecutive values
 //     per round, one per lane.  A lane finds its run from a 32-bit map of the
 //     run starts inside the round (one shared load and one warp OR-reduce),
@@ -239,20 +241,21 @@ __global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
         return (uint64_t)t * ru + (uint64_t)(e / ru) * 32u * ru + (e % ru);
     };
 
-    // parser state: thread p < 8 parses stream p
+    // parser state: lane 0 of warp w walks stream w, so the walks of a
+    // block's streams run on different warps (no divergence between streams,
+    // no block barrier: after the copy above each warp runs on its own)
     uint32_t p_pos = 0, p_g = 0, p_err = ST_OK;
-    const uint32_t plen = tid < LANES_PER_BLOCK ? s_len[L0 + tid] : 0u;
-    const uint8_t* psbuf = smem + (tid < LANES_PER_BLOCK ? tid : 0u) * cap;
+    const uint32_t plen = s_len[t];
     uint32_t vbeg = 0;  // first value of this warp's current batch
     uint32_t werr = ST_OK;
 
     for (;;) {
-        // ---- parse 1: run boundaries, one thread per stream ----
-        if (tid < LANES_PER_BLOCK) {
+        // ---- parse 1: run boundaries (lane 0) ----
+        if (lane == 0) {
             uint32_t nr = 0;
             while (p_err == ST_OK && p_g < nv && nr < (uint32_t)RCAP) {
                 // SHORT_REPEAT (most runs): length and size from the first byte
-                const uint32_t h0 = p_pos < plen ? psbuf[p_pos] : 0xffu;
+                const uint32_t h0 = p_pos < plen ? sbuf[p_pos] : 0xffu;
                 if (h0 < 64u) {
                     const uint32_t next = p_pos + 2u + ((h0 >> 3) & 7u), rl = (h0 & 7u) + 3u;
                     if (next > plen) {
@@ -263,14 +266,14 @@ __global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
                         p_err = ST_OVERRUN;
                         break;
                     }
-                    R.vs[tid][nr] = p_g;
-                    R.pos[tid][nr] = p_pos;
+                    R.vs[wid][nr] = p_g;
+                    R.pos[wid][nr] = p_pos;
                     ++nr;
                     p_pos = next;
                     p_g += rl;
                     continue;
                 }
-                const Skip k = skip_run(psbuf, p_pos, plen);
+                const Skip k = skip_run(sbuf, p_pos, plen);
                 if (k.err != ST_OK) {
                     p_err = k.err;
                     break;
@@ -279,33 +282,33 @@ __global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
                     p_err = ST_OVERRUN;
                     break;
                 }
-                R.vs[tid][nr] = p_g;
-                R.pos[tid][nr] = p_pos;
+                R.vs[wid][nr] = p_g;
+                R.pos[wid][nr] = p_pos;
                 ++nr;
                 p_pos = k.next;
                 p_g += k.len;
             }
             // the stream must end exactly with its last run
             if (p_err == ST_OK && p_g == nv && p_pos != plen) p_err = ST_CORRUPT;
-            R.vs[tid][nr] = p_g;
-            R.nr[tid] = nr;
-            R.npr[tid] = 0;
-            R.err[tid] = p_err;
+            R.vs[wid][nr] = p_g;
+            R.nr[wid] = nr;
+            R.npr[wid] = 0;
+            R.err[wid] = p_err;
         }
-        __syncthreads();
-        // ---- parse 2: decode the recorded headers, all threads ----
-        for (uint32_t x = tid; x < (uint32_t)(LANES_PER_BLOCK * RCAP); x += blockDim.x) {
-            const uint32_t st = x / RCAP, ri = x % RCAP;
-            if (ri < R.nr[st]) {
-                const Run r = parse_fast(smem + st * cap, R.pos[st][ri], s_len[L0 + st]);
-                R.meta[st][ri] = r.kind | (r.fbw << 2) | (r.flags << 9) | (r.pll << 11) | (r.pw << 16) | (r.cfb << 23);
-                R.vbit[st][ri] = r.vbit;
-                R.base[st][ri] = r.base;
-                R.aux[st][ri] = r.kind == 2 ? (uint64_t)r.pbit : r.delta;
-                if (r.kind == 2 && r.pll) R.prun[st][atomicAdd(&R.npr[st], 1u)] = (uint8_t)ri;
+        __syncwarp();
+        // ---- parse 2: decode the recorded headers, one run per lane ----
+        {
+            const uint32_t nrp = R.nr[wid];
+            for (uint32_t ri = lane; ri < nrp; ri += 32) {
+                const Run r = parse_fast(sbuf, R.pos[wid][ri], plen);
+                R.meta[wid][ri] = r.kind | (r.fbw << 2) | (r.flags << 9) | (r.pll << 11) | (r.pw << 16) | (r.cfb << 23);
+                R.vbit[wid][ri] = r.vbit;
+                R.base[wid][ri] = r.base;
+                R.aux[wid][ri] = r.kind == 2 ? (uint64_t)r.pbit : r.delta;
+                if (r.kind == 2 && r.pll) R.prun[wid][atomicAdd(&R.npr[wid], 1u)] = (uint8_t)ri;
             }
         }
-        __syncthreads();
+        __syncwarp();
 
         // ---- expand: values [vbeg, vend) of stream t, 32 per round ----
         const uint32_t nr = R.nr[wid];
@@ -405,9 +408,9 @@ __global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
             }
         }
         vbeg = vend;
-        __syncthreads();  // the next batch rewrites the run tables
-        const bool more = tid < LANES_PER_BLOCK && p_err == ST_OK && p_g < nv;
-        if (!__syncthreads_or(more)) break;
+        __syncwarp();  // the next batch rewrites this warp's run tables
+        const bool more = lane == 0 && p_err == ST_OK && p_g < nv;
+        if (!__any_sync(GD_FULL_MASK, more)) break;
     }
     const uint32_t err = max(werr, R.err[wid]);
     if (lane == 0 && err != ST_OK && status) atomicMax(status + chunk, err);

@@ -257,3 +257,65 @@ def test_new_containers_corrupt(cuda):
     e4 = cc.brle_trans_encode(r2, 4096)
     e4.meta["col_len"][32] = 10_000  # longer than any valid column stream
     _expect_error(e4, cuda)
+
+
+def _lzss_token_column(rng, col_bytes):
+    """One LZSS column stream with every token shape the grammar allows:
+    literals, matches of length 3..34 at offsets 1..o, including offsets below
+    the length (the source overlaps the output, copied byte by byte)."""
+    toks, o = [], 0
+    while o < col_bytes:
+        if o == 0 or rng.random() < 0.35:
+            toks.append(("l", int(rng.integers(0, 256))))
+            o += 1
+            continue
+        ln = int(min(rng.integers(3, 35), col_bytes - o))
+        if ln < 3:
+            toks.append(("l", int(rng.integers(0, 256))))
+            o += 1
+            continue
+        r = rng.random()
+        off = int(rng.integers(1, 4)) if r < 0.25 else int(rng.integers(4, 9)) if r < 0.45 else \
+            int(rng.integers(1, o + 1))
+        off = min(off, o)
+        toks.append(("m", off, ln))
+        o += ln
+    out = bytearray()
+    for g in range(0, len(toks), 8):
+        grp = toks[g:g + 8]
+        out.append(sum(1 << i for i, t in enumerate(grp) if t[0] == "l"))
+        for t in grp:
+            if t[0] == "l":
+                out.append(t[1])
+            else:
+                v = (t[1] << 5) | (t[2] - 3)
+                out += bytes([v & 0xFF, v >> 8])
+    return np.frombuffer(bytes(out), np.uint8)
+
+
+@pytest.mark.parametrize("knob", [0, 1, 4])
+@pytest.mark.parametrize("chunk", [4096, 65536])
+def test_lzss_token_shapes(cuda, knob, chunk):
+    from test_golden import interleave_streams
+    import compression_b200.autotune as at
+    rng = np.random.default_rng(chunk + knob)
+    blocks, cls, maps = [], [], []
+    for c in range(3):
+        cols = [_lzss_token_column(rng, chunk // 32) for _ in range(32)]
+        order = sorted(range(32), key=lambda q: -cols[q].size)
+        blk, cl = interleave_streams([cols[q] for q in order])
+        blocks.append(blk)
+        cls.append(cl)
+        maps.append(np.array(order, np.uint8))
+    bo = np.concatenate([[0], np.cumsum([b.size for b in blocks])]).astype(np.uint64)
+    e = cc.Encoded("lzss", np.concatenate(blocks), 3 * chunk, 3, chunk,
+                   {"blk_off": bo, "col_len": np.concatenate(cls), "col_map": np.concatenate(maps)})
+    rc, ref = oracle.decode(e)
+    assert rc == 0
+    prev = at.set_knob(at.TUNE_LZSS_WARPS_PER_BLOCK, knob)
+    try:
+        st, out = _gpu(e, cuda)
+    finally:
+        at.set_knob(at.TUNE_LZSS_WARPS_PER_BLOCK, prev)
+    assert (st == 0).all(), np.unique(st)
+    assert np.array_equal(out, ref)
