@@ -262,6 +262,12 @@ class DeviceJob:
         self.out_n = out_n
         self.d_out = out if out is not None else torch.empty(max(out_n, 16), dtype=torch.uint8, device=self.dev)
         self.d_status = torch.zeros(max(enc.n_chunks, 1), dtype=torch.int32, device=self.dev)
+        self.d_order = None
+        if enc.codec == "deflate" and enc.n_chunks > 1:
+            # streams start longest first (the kernel hands them out in this order)
+            sizes = np.diff(enc.meta["out_off"].astype(np.int64))
+            order = np.argsort(-sizes, kind="stable").astype(np.uint32)
+            self.d_order = torch.from_numpy(order).to(self.dev)
 
     def launch(self, stream=None) -> None:
         L = lib()
@@ -290,6 +296,10 @@ class DeviceJob:
         elif e.codec == "brle_trans":
             rc = L.gd_brle_trans_decode(ptr(self.d_data), ptr(m["blk_off"]), ptr(m["col_len"]), ptr(m["col_map"]),
                                         e.n_chunks, e.chunk_size, ptr(self.d_out), e.n_out, ptr(self.d_status), s)
+        elif e.codec == "deflate" and self.d_order is not None:
+            rc = L.gd_inflate_ordered(ptr(self.d_data), ptr(m["comp_off"]), ptr(m["comp_len"]), ptr(m["out_off"]),
+                                      e.n_chunks, e.params["zlib_header"], ptr(self.d_out), ptr(self.d_status),
+                                      ptr(self.d_order), s)
         elif e.codec == "deflate":
             rc = L.gd_inflate(ptr(self.d_data), ptr(m["comp_off"]), ptr(m["comp_len"]), ptr(m["out_off"]),
                               e.n_chunks, e.params["zlib_header"], ptr(self.d_out), ptr(self.d_status), s)
@@ -320,7 +330,10 @@ def decode_host_pinned(enc: Encoded) -> np.ndarray:
     if "_pinned" not in enc.params:
         pm = {k: _pinned_copy(v) for k, v in enc.meta.items()}
         pd = _pinned_copy(enc.data)
-        pc = _pinned_copy(enc.params["container"]) if "container" in enc.params else None
+        cont = enc.params.get("container")
+        if cont is None and enc.codec == "rlev1":
+            cont = np.concatenate([np.array([enc.n_out], dtype=np.uint64).view(np.uint8), enc.data])
+        pc = _pinned_copy(cont) if cont is not None else None
         enc.params["_pinned"] = (pd, pm, pc)
     pd, pm, pc = enc.params["_pinned"]
     view = Encoded(enc.codec, pd, enc.n_out, enc.n_chunks, enc.chunk_size, pm,
@@ -343,7 +356,9 @@ def decode_host(enc: Encoded, keep: bool = True) -> np.ndarray:
         cont = enc.params["container"]
         rc = L.gd_brle_decompress(_p(cont), cont.size, C.byref(out), C.byref(n))
     elif enc.codec == "rlev1":
-        buf = np.concatenate([np.array([enc.n_out], dtype=np.uint64).view(np.uint8), enc.data])
+        buf = enc.params.get("container")  # [u64 decompressed size][blocks], as the reference reads it
+        if buf is None:
+            buf = np.concatenate([np.array([enc.n_out], dtype=np.uint64).view(np.uint8), enc.data])
         rc = L.gd_rlev1_decompress(_p(buf), buf.size, _p(m["col_len"]), m["col_len"].nbytes, _p(m["blk_off"]),
                                    m["blk_off"].nbytes, enc.params["comp_col_len"], enc.params["elem_bytes"],
                                    enc.chunk_size, C.byref(out), C.byref(n))

@@ -150,23 +150,30 @@ thread_local Pipe g_pipe;
 // the first decode); launch(a, b, stream) decodes chunks [a, b).  Decoders
 // read no input byte past their own chunks' streams that affects the
 // result, so a piece may decode while the next piece is still arriving.
+// Piece bounds: whole chunks, about total/pieces output bytes (at least
+// 4 MiB) each, at most kMaxPieces pieces.
+template <class OutAt>
+std::vector<uint64_t> piece_cuts(uint64_t n, OutAt out_at, uint64_t pieces) {
+    const uint64_t total = out_at(n);
+    const uint64_t want = total / pieces > (4ull << 20) ? total / pieces : (4ull << 20);
+    std::vector<uint64_t> cut{0};
+    for (uint64_t c = 0; c < n && cut.size() < (size_t)kMaxPieces;) {
+        uint64_t e = c + 1;
+        while (e < n && out_at(e) - out_at(c) < want) ++e;
+        cut.push_back(e);
+        c = e;
+    }
+    if (cut.back() != n) cut.push_back(n);
+    return cut;
+}
+
 template <class InAt, class OutAt, class Prologue, class Launch>
 gd_status_t run_piped(uint64_t n, const uint8_t* h_in, uint8_t* d_in, InAt in_at, uint8_t* d_out, uint8_t* h_out,
                       OutAt out_at, uint32_t* d_st, Prologue prologue, Launch launch, uint64_t pieces = 16) {
     if (!g_pipe.init()) return GD_ERR_CUDA;
     cudaStream_t si = g_pipe.st[0], sk = g_pipe.st[1], so = g_pipe.st[2];
-    const uint64_t total = out_at(n);
-    const uint64_t want = total / pieces > (4ull << 20) ? total / pieces : (4ull << 20);  // bytes out per piece
-    uint64_t cut[kMaxPieces + 1];
-    int np = 0;
-    cut[0] = 0;
-    for (uint64_t c = 0; c < n && np < kMaxPieces - 1;) {
-        uint64_t e = c + 1;
-        while (e < n && out_at(e) - out_at(c) < want) ++e;
-        cut[++np] = e;
-        c = e;
-    }
-    if (cut[np] != n) cut[++np] = n;
+    const std::vector<uint64_t> cut = piece_cuts(n, out_at, pieces);
+    const int np = (int)cut.size() - 1;
     gd_status_t r = prologue(sk);
     if (r != GD_OK) return r;
     for (int i = 0; i < np; ++i) {
@@ -602,19 +609,35 @@ gd_status_t inflate_piped(const uint8_t* in, uint64_t in_n, const uint64_t* comp
         if (!mono) return c ? in_n : 0;
         return c < n ? comp_off[c] : in_n;
     };
+    // inside every piece the streams start longest first: the piece ends
+    // with its longest stream, so that one must not start last
+    constexpr uint64_t kPieces = 4;
+    uint32_t* d_order = (uint32_t*)g_pool.get(6, 4 * n);
+    if (!d_order) return GD_ERR_NOMEM;
+    std::vector<uint32_t> order(n);
+    for (uint64_t i = 0; i < n; ++i) order[i] = (uint32_t)i;
+    auto out_at = [&](uint64_t c) { return out_off[c]; };
+    {
+        const std::vector<uint64_t> cuts = piece_cuts(n, out_at, kPieces);  // as run_piped cuts them
+        for (size_t i = 0; i + 1 < cuts.size(); ++i)
+            std::stable_sort(order.begin() + cuts[i], order.begin() + cuts[i + 1], [&](uint32_t x, uint32_t y) {
+                return out_off[x + 1] - out_off[x] > out_off[y + 1] - out_off[y];
+            });
+    }
     return run_piped(
-        n, in, d_data, in_at, d_out, h, [&](uint64_t c) { return out_off[c]; }, d_st,
+        n, in, d_data, in_at, d_out, h, out_at, d_st,
         [&](cudaStream_t st) {
             bool ok = cudaMemcpyAsync(d_meta, comp_off, 8 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
             ok = ok && cudaMemcpyAsync(d_meta + n + 1, comp_len, 8 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
             ok = ok && cudaMemcpyAsync(d_meta + 2 * n + 1, out_off, 8 * (n + 1), cudaMemcpyHostToDevice, st) ==
                            cudaSuccess;
+            ok = ok && cudaMemcpyAsync(d_order, order.data(), 4 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
             return ok ? GD_OK : GD_ERR_CUDA;
         },
         [&](uint64_t a, uint64_t b, cudaStream_t st) {
-            return gd_inflate(d_data, d_meta + a, d_meta + n + 1 + a, d_meta + 2 * n + 1 + a, (uint32_t)(b - a),
-                              zlib_header, d_out, d_st + a, st);
+            return gd_inflate_ordered(d_data, d_meta, d_meta + n + 1, d_meta + 2 * n + 1, (uint32_t)(b - a),
+                                      zlib_header, d_out, d_st, d_order + a, st);
         },
-        4);
+        kPieces);
 }
 }  // namespace

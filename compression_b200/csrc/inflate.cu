@@ -150,16 +150,29 @@ gd_status_t launch_pair(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
 }
 
-// Launch configuration (GD_TUNE_INFLATE_VARIANT): 0 = decoder/writer warp
-// pair per stream with a 32 KiB shared window (default); 1 / 2 = one warp per
+// Launch configuration (GD_TUNE_INFLATE_VARIANT): 1 / 2 = one warp per
 // stream without a window, 2 / 4 warps per block; 3 = one warp per stream
-// with a window.
+// with a window; 4 / 5 = decoder/writer warp pairs without a window (copies
+// read the output), 2 / 4 pairs per block; 6 = one decoder/writer pair per
+// block with a 32 KiB shared window; 0 (default) = 4 for at least 4 streams
+// per SM, else 6.
 template <class Chunks>
 gd_status_t launch_inflate(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32_t* order, cudaStream_t s) {
-    switch (gd_tune_get(GD_TUNE_INFLATE_VARIANT)) {
-        case 3: return launch_cfg<Chunks, 32768, 1>(ch, n, zlib_hdr, order, s);
+    int v = gd_tune_get(GD_TUNE_INFLATE_VARIANT);
+    if (v == 0) {
+        // many streams: throughput, i.e. more pairs per SM (no window); few:
+        // the fastest single stream (window)
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        v = n >= 4u * (uint32_t)sms ? 4 : 6;
+    }
+    switch (v) {
         case 1: return launch_cfg<Chunks, 0, 2>(ch, n, zlib_hdr, order, s);
         case 2: return launch_cfg<Chunks, 0, 4>(ch, n, zlib_hdr, order, s);
+        case 3: return launch_cfg<Chunks, 32768, 1>(ch, n, zlib_hdr, order, s);
+        case 4: return launch_pair<Chunks, 0, 2>(ch, n, zlib_hdr, order, s);
+        case 5: return launch_pair<Chunks, 0, 4>(ch, n, zlib_hdr, order, s);
         default: return launch_pair<Chunks, 32768, 1>(ch, n, zlib_hdr, order, s);
     }
 }

@@ -94,8 +94,15 @@ static __device__ __forceinline__ void execute_batch(const Batch& B, uint32_t po
                                                      const uint8_t* __restrict__ src, uint8_t* __restrict__ dst) {
     const uint32_t lane = lane_id();
     const uint32_t nc = B.n_cmd;
+    // the next command's fields are loaded before the current one is written
+    uint32_t tn = nc ? B.cmd_t[0] : 0u, an = nc ? B.cmd_a[0] : 0u, nn = nc ? B.cmd_b[0] : 0u;
     for (uint32_t c = 0; c < nc; ++c) {
-        const uint32_t t = B.cmd_t[c], a = B.cmd_a[c], n = B.cmd_b[c];
+        const uint32_t t = tn, a = an, n = nn;
+        if (c + 1 < nc) {
+            tn = B.cmd_t[c + 1];
+            an = B.cmd_a[c + 1];
+            nn = B.cmd_b[c + 1];
+        }
         uint8_t* d = dst + pos;
         if constexpr (WIN != 0) {
             // every output byte also goes to the window; copies read it there
@@ -112,6 +119,28 @@ static __device__ __forceinline__ void execute_batch(const Batch& B, uint32_t po
                     const uint8_t v = s[k];
                     d[k] = v;
                     win[(pos + k) & M] = v;
+                }
+            } else if (a >= 128) {
+                // 128-byte waves (four bytes a lane): with distance >= 128 a
+                // wave reads only bytes written before it
+                const uint32_t sp = pos - a;
+                for (uint32_t k0 = 0; k0 < n; k0 += 128) {
+                    uint8_t v[4];
+#pragma unroll
+                    for (uint32_t i = 0; i < 4; ++i) {
+                        const uint32_t k = k0 + lane + 32u * i;
+                        v[i] = k < n ? win[(sp + k) & M] : (uint8_t)0;
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (uint32_t i = 0; i < 4; ++i) {
+                        const uint32_t k = k0 + lane + 32u * i;
+                        if (k < n) {
+                            d[k] = v[i];
+                            win[(pos + k) & M] = v[i];
+                        }
+                    }
+                    __syncwarp();
                 }
             } else if (a >= 32) {
                 // 32-byte waves: a wave reads bytes written before it (earlier
@@ -648,6 +677,85 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                 // Literals accumulate in a run that becomes one command when a
                 // copy or the end of the batch closes it.
                 uint32_t run = 0, run_start = nl;
+                // fast loop while at least 16 input bytes are buffered: the bit
+                // buffer is topped up 32 bits at a time from two ring words,
+                // codes of <= LBITS bits decode with one lookup, the output
+                // bound is checked once per batch (below), and anything else
+                // (long codes, invalid entries) falls to the checked loop
+                {
+                    const uint32_t* r32 = reinterpret_cast<const uint32_t*>(S.ring);
+                    constexpr uint32_t RW = IRING / 4 - 1;
+                    auto top32 = [&]() {
+                        if (bitcnt <= 32) {
+                            const uint32_t k = inpos >> 2;
+                            const uint32_t w = __funnelshift_r(r32[k & RW], r32[(k + 1) & RW], (inpos & 3u) * 8u);
+                            bitbuf |= (uint64_t)w << bitcnt;
+                            bitcnt += 32;
+                            inpos += 4;
+                        }
+                    };
+                    while (nc < NCMD - 2 && nl < NLIT && fill - inpos >= 16) {
+                        top32();
+                        const uint32_t e = S.lit.lut[(uint32_t)bitbuf & ((1u << LBITS) - 1u)];
+                        const uint32_t L = e & 15u;
+                        if (L == 0 || e == 0xffffffffu) break;  // long code / bad entry: checked loop
+                        const uint32_t kind = e >> 24;
+                        if (kind == E_LIT) {
+                            bitbuf >>= L;
+                            bitcnt -= L;
+                            if (run == 0) run_start = nl;
+                            BT.lits[nl++] = (uint8_t)(e >> 8);
+                            ++run;
+                            ++opos;
+                            continue;
+                        }
+                        if (kind != E_LEN) break;  // end of block / bad symbol: checked loop
+                        // length: its extra bits are in the buffer (>= 33 - 10 bits left)
+                        const uint32_t ex = (e >> 4) & 15u;
+                        const uint64_t b1 = bitbuf >> L;
+                        const uint32_t len = ((e >> 8) & 0xffffu) + ((uint32_t)b1 & ((1u << ex) - 1u));
+                        uint64_t b2 = b1 >> ex;
+                        uint32_t c2 = bitcnt - L - ex;
+                        if (c2 <= 32) {
+                            const uint32_t k = inpos >> 2;
+                            const uint32_t w = __funnelshift_r(r32[k & RW], r32[(k + 1) & RW], (inpos & 3u) * 8u);
+                            b2 |= (uint64_t)w << c2;
+                            c2 += 32;
+                            inpos += 4;
+                        }
+                        const uint32_t ed = S.dist.lut[(uint32_t)b2 & ((1u << LBITS) - 1u)];
+                        const uint32_t Ld = ed & 15u;
+                        if (Ld == 0 || (ed >> 24) != E_DIST) {
+                            // long or bad distance code: undo to the length symbol
+                            // (bits re-read by the checked loop)
+                            if (c2 != bitcnt - L - ex) {
+                                inpos -= 4;
+                            }
+                            break;
+                        }
+                        const uint32_t exd = (ed >> 4) & 15u;
+                        const uint64_t b3 = b2 >> Ld;
+                        const uint32_t dist = ((ed >> 8) & 0xffffu) + ((uint32_t)b3 & ((1u << exd) - 1u));
+                        if (dist > opos) {
+                            err = ST_CORRUPT;
+                            break;
+                        }
+                        bitbuf = b3 >> exd;
+                        bitcnt = c2 - Ld - exd;
+                        if (run) {
+                            BT.cmd_t[nc] = C_LIT;
+                            BT.cmd_a[nc] = run_start;
+                            BT.cmd_b[nc] = run;
+                            ++nc;
+                            run = 0;
+                        }
+                        BT.cmd_t[nc] = C_COPY;
+                        BT.cmd_a[nc] = dist;
+                        BT.cmd_b[nc] = len;
+                        ++nc;
+                        opos += len;
+                    }
+                }
                 while (err == ST_OK && nc < NCMD - 2 && nl < NLIT && (fill - inpos >= 32 || fill >= span)) {
                     uint32_t e;
                     if (!decode_ent(&S.lit, TK_LIT, e)) {
@@ -712,6 +820,9 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                     BT.cmd_b[nc] = run;
                     ++nc;
                 }
+                // the fast loop does not bound the output per symbol: a batch
+                // that would write past the end is not executed
+                if (err == ST_OK && opos > olen) err = ST_OVERRUN;
             }
             BT.n_cmd = nc;
             BT.n_lit = nl;
@@ -773,7 +884,7 @@ static __device__ __forceinline__ uint32_t stream_pair_writer(WarpSmemT<WIN, 2>&
                                                               uint8_t* __restrict__ dst) {
     for (uint32_t kb = 0;; ++kb) {
         if (!pair_wait(&S.produced, kb + 1)) return ST_TIMEOUT;
-        const Batch& BT = S.bt[kb & 1u];
+        Batch& BT = S.bt[kb & 1u];
         if (BT.last) return ST_OK;
         execute_batch<WIN>(BT, BT.pos0, S.win, src, dst);
         pair_post(&S.consumed, kb + 1);

@@ -257,9 +257,12 @@ gd_status_t gd_batch_decode_lpt_noalloc(const gd_task* d_tasks, uint32_t n_tasks
  * autotuner, which times the choices on the device.
  * ------------------------------------------------------------------------ */
 typedef enum gd_tune_key {
-    GD_TUNE_INFLATE_VARIANT = 0, /* 0: decoder + writer warp per stream, 32 KiB shared output window;
-                                    1 / 2: one warp per stream, no window, 2 / 4 warps per block;
-                                    3: one warp per stream with the window */
+    GD_TUNE_INFLATE_VARIANT = 0, /* 1 / 2: one warp per stream, no window, 2 / 4 warps per block;
+                                    3: one warp per stream with a 32 KiB shared output window;
+                                    4 / 5: decoder + writer warp pair per stream, no window
+                                    (copies read the output), 2 / 4 pairs per block;
+                                    6: decoder + writer pair with the window, one per block;
+                                    0 (default): 4 for >= 4 streams per SM, else 6 */
     GD_TUNE_BRLE_BLOCKS_PER_SM = 1,   /* byte-RLE grid = value x SMs blocks (default 8) */
     GD_TUNE_RLEV1_LANES_PER_BLOCK = 2, /* 0/8: 8 lane streams per block; 4: 4 */
     GD_TUNE_RLEV2_LANES_PER_BLOCK = 3, /* 0/4: 4 lane streams per block; 8: 8 */

@@ -319,3 +319,20 @@ def test_lzss_token_shapes(cuda, knob, chunk):
         at.set_knob(at.TUNE_LZSS_WARPS_PER_BLOCK, prev)
     assert (st == 0).all(), np.unique(st)
     assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
+def test_inflate_variants(cuda, variant):
+    """Every inflate kernel shape on streams of mixed size with dynamic,
+    fixed-Huffman and stored blocks, against zlib."""
+    import compression_b200.autotune as at
+    raw = cc.gen_markov_copy(11, 3 << 20, 32768)
+    sizes = cc.loguniform_sizes(12, 40, 1024, 256 * 1024, raw.size)
+    oo = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    mode = (np.arange(40) % 7 == 3).astype(np.uint8) + 2 * (np.arange(40) % 11 == 5).astype(np.uint8)
+    enc = cc.deflate_encode(raw[: int(oo[-1])], oo, 6, mode, 1)
+    prev = at.set_knob(at.TUNE_INFLATE_VARIANT, variant)
+    try:
+        _parity(enc, raw[: int(oo[-1])], cuda)
+    finally:
+        at.set_knob(at.TUNE_INFLATE_VARIANT, prev)
