@@ -354,6 +354,12 @@ def run_ours(args, rank, world, local_rank):
                      "decomp_gbs": round(e.n_out / (kms / 1e3) / 1e9, 1),
                      "ratio": round(e.comp_bytes / max(e.n_out, 1), 4)})
     dom = max(kern, key=lambda k: k["ms"])
+    traffic = None
+    tp = ROOT / "profiles" / "dram_traffic.json"
+    if tp.exists() and args.scale == 1.0:
+        t = json.loads(tp.read_text()).get(args.workload, {}).get(dom["kernel"])
+        if t:
+            traffic = int(t["read"] + t["write"])
 
     # e2e: the reference-shaped host call (host buffers; H2D + decode + D2H inside)
     e2e = None
@@ -383,7 +389,9 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(cfg, l2="flushed between timed steps (256 MiB write)", parallelism=f"replicas x{world}"),
         "roofline": {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["gbs"], "peak": peak,
                      "unit": "GB/s", "frac": round(dom["gbs"] / peak, 4), "peak_source": peak_kind,
-                     "traffic": None},
+                     "traffic": traffic, "alg_bytes": dom["alg_bytes"],
+                     "traffic_source": "profiles/dram_traffic.json (ncu capture of this workload)" if traffic
+                     else None},
         "kernels": kern,
         "gpu_launches": len(jobs) * K,
         "clocks": clk.summary(),
