@@ -145,6 +145,29 @@ __device__ __forceinline__ void load_lane_streams(const SegTable& T, const uint3
     uint32_t maxw = 0;
 #pragma unroll
     for (int i = 0; i < NLANES; ++i) maxw = max(maxw, (s_len[L0 + i] + 3) >> 2);
+    // Rows every slot reaches (segment 0: [0, T.hi[0]), 128 bytes each) hold
+    // the group's words contiguously at 4*L0: with the block 16-byte aligned
+    // and NLANES, L0 multiples of 4, one 16-byte load fetches 4 lanes' words
+    // (a quarter of the memory requests of word copies).
+    uint32_t k0 = 0;
+    if constexpr (NLANES % 4 == 0) {
+        if ((reinterpret_cast<uintptr_t>(block) & 15u) == 0 && (L0 & 3u) == 0) {
+            constexpr uint32_t Q = NLANES / 4;
+            const uint32_t rows0 = min(T.hi[0], maxw);
+            const uint32_t cw = cap >> 2;
+#pragma unroll 4
+            for (uint32_t x = tid; x < rows0 * Q; x += blockDim.x) {
+                const uint32_t k = x / Q, q = x % Q;
+                const uint4 v = __ldg(reinterpret_cast<const uint4*>(block + k * 128u + 16u * ((L0 >> 2) + q)));
+                uint32_t* d0 = reinterpret_cast<uint32_t*>(dst + 4u * q * cap) + k;
+                d0[0] = v.x;
+                d0[cw] = v.y;
+                d0[2 * cw] = v.z;
+                d0[3 * cw] = v.w;
+            }
+            k0 = rows0;
+        }
+    }
     const uint32_t sub = tid % NLANES;
     const uint32_t l = L0 + sub;
     const uint32_t nwl = (s_len[l] + 3) >> 2;
@@ -152,7 +175,7 @@ __device__ __forceinline__ void load_lane_streams(const SegTable& T, const uint3
     uint32_t* d = reinterpret_cast<uint32_t*>(dst + sub * cap);
     // a thread's rows only grow, so its segment index is tracked, not searched
     uint32_t j = 0;
-    for (uint32_t k = tid / NLANES; k < maxw; k += blockDim.x / NLANES) {
+    for (uint32_t k = k0 + tid / NLANES; k < maxw; k += blockDim.x / NLANES) {
         if (k < nwl) {
             while (j < 31 && T.hi[j] <= k) ++j;
             const uint32_t lo = j ? T.hi[j - 1] : 0u;

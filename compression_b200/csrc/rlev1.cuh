@@ -54,16 +54,22 @@ template <typename T>
 static __device__ __noinline__ uint32_t lane_warp(const uint8_t* __restrict__ sbuf, uint32_t len, uint32_t nv, uint32_t t,
                                            uint32_t wil, T* __restrict__ outv, uint64_t want) {
     const uint32_t lane = lane_id();
+    // wil a power of two (COMP_COL_LEN / sizeof(T) always is in the
+    // reference's configurations): shifts instead of a division per value
+    const bool pow2 = (wil & (wil - 1u)) == 0u;
+    const uint32_t wsh = __ffs(wil) - 1u;
     auto put = [&](uint32_t e, uint64_t v) {
-        const uint64_t oe = (uint64_t)(e / wil) * 32u * wil + (uint64_t)t * wil + (e % wil);
+        const uint64_t oe = pow2 ? ((uint64_t)(e >> wsh) << (wsh + 5u)) + ((uint64_t)t << wsh) + (e & (wil - 1u))
+                                 : (uint64_t)(e / wil) * 32u * wil + (uint64_t)t * wil + (e % wil);
         if (oe < want) outv[oe] = (T)v;
     };
     uint32_t err = ST_OK, pos = 0, g = 0;
     while (g < nv) {
-        // ---- header (lane 0) ----
+        // ---- header: every lane parses it (shared-memory broadcast reads),
+        // so nothing needs to be shuffled ----
         uint32_t kind = 0, cnt = 0, next = 0, e = ST_OK;
         uint64_t base = 0, delta = 0;
-        if (lane == 0) {
+        {
             uint32_t p = pos;
             if (p >= len) {
                 e = ST_CORRUPT;
@@ -93,10 +99,6 @@ static __device__ __noinline__ uint32_t lane_warp(const uint8_t* __restrict__ sb
             }
             next = p;
         }
-        kind = __shfl_sync(GD_FULL_MASK, kind, 0);
-        cnt = __shfl_sync(GD_FULL_MASK, cnt, 0);
-        next = __shfl_sync(GD_FULL_MASK, next, 0);
-        e = __shfl_sync(GD_FULL_MASK, e, 0);
         if (e != ST_OK) {
             err = e;
             break;
@@ -106,10 +108,6 @@ static __device__ __noinline__ uint32_t lane_warp(const uint8_t* __restrict__ sb
             break;
         }
         if (kind == 0) {  // run: closed form
-            base = ((uint64_t)__shfl_sync(GD_FULL_MASK, (uint32_t)(base >> 32), 0) << 32) |
-                   __shfl_sync(GD_FULL_MASK, (uint32_t)base, 0);
-            delta = ((uint64_t)__shfl_sync(GD_FULL_MASK, (uint32_t)(delta >> 32), 0) << 32) |
-                    __shfl_sync(GD_FULL_MASK, (uint32_t)delta, 0);
             for (uint32_t i = lane; i < cnt; i += 32) put(g + i, base + (uint64_t)i * delta);
             g += cnt;
             pos = next;
@@ -131,16 +129,17 @@ static __device__ __noinline__ uint32_t lane_warp(const uint8_t* __restrict__ sb
                 break;
             }
             const uint32_t take = min(min(rem, nterm), 32u);
+            const uint32_t end = lane < take ? select128(m, lane) : 0u;
+            const uint32_t prev = __shfl_up_sync(GD_FULL_MASK, end, 1);  // the previous varint's last byte
             if (lane < take) {
-                const uint32_t end = select128(m, lane);
-                const uint32_t beg = lane ? select128(m, lane - 1) + 1 : 0;
+                const uint32_t beg = lane ? prev + 1 : 0;
                 uint64_t v = 0;
                 uint32_t sh = 0;
                 for (uint32_t k = beg; k <= end; ++k, sh += 7)
                     if (sh < 64) v |= (uint64_t)(sbuf[p + k] & 0x7fu) << sh;
                 put(g + lane, v);
             }
-            p += select128(m, take - 1) + 1;
+            p += __shfl_sync(GD_FULL_MASK, end, take - 1) + 1;
             g += take;
             rem -= take;
         }

@@ -62,9 +62,13 @@ __host__ __device__ constexpr uint32_t lane_cap(uint32_t n) { return ((n + 15u) 
 __device__ __forceinline__ uint64_t extract_msb(const uint8_t* buf, uint32_t bitpos, uint32_t w) {
     const uint32_t a = bitpos >> 3;
     const uint32_t* p = reinterpret_cast<const uint32_t*>(buf + (a & ~3u));
-    const uint32_t w0 = __byte_perm(p[0], 0, 0x0123), w1 = __byte_perm(p[1], 0, 0x0123),
-                   w2 = __byte_perm(p[2], 0, 0x0123);
     const uint32_t s = ((a & 3u) << 3) + (bitpos & 7u);  // 0..31
+    const uint32_t w0 = __byte_perm(p[0], 0, 0x0123), w1 = __byte_perm(p[1], 0, 0x0123);
+    if (w <= 32) {  // s + w <= 63: two big-endian words, 32-bit arithmetic
+        const uint32_t t = __funnelshift_l(w1, w0, s);
+        return (uint64_t)(t >> (32u - w));
+    }
+    const uint32_t w2 = __byte_perm(p[2], 0, 0x0123);
     const uint64_t hi = ((uint64_t)w0 << 32) | w1;
     const uint64_t t = (hi << s) | (((uint64_t)w2 << s) >> 32);
     return w >= 64 ? t : (t >> (64 - w));
