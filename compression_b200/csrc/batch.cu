@@ -20,10 +20,14 @@ namespace gd {
 namespace batch {
 
 constexpr int WPB = 4;  // warps per block
+// Deflate workspace of a batch warp: no window, a 2 KiB input ring (the
+// standalone kernels use 8 KiB); it sets every warp's workspace size, so it
+// is kept small for occupancy.
+using BatchInflSmem = infl::WarpSmemT<0, 1, 2048>;
 
 __host__ __device__ constexpr uint32_t warp_smem_bytes(uint32_t max_lane) {
     // union of the per-codec warp workspaces
-    uint32_t a = (uint32_t)sizeof(infl::WarpSmem);
+    uint32_t a = (uint32_t)sizeof(BatchInflSmem);
     uint32_t b = lzss::WARP_SMEM;
     uint32_t c = (uint32_t)sizeof(SegTable) + ((max_lane + 15u) & ~15u) + 160u;
     uint32_t d = brlew::WARP_SMEM;
@@ -110,8 +114,8 @@ __device__ uint32_t run_task(const gd_task& t, uint32_t max_lane, uint8_t* ws) {
         case GD_CODEC_DEFLATE: {
             if (t.src_len > 0xffffffffull || t.dst_len > 0xffffffffull) return ST_INVALID;
             uint32_t fin = 0;
-            const uint32_t e = infl::stream_warp<0>(t.src, (uint32_t)t.src_len, t.dst, (uint32_t)t.dst_len,
-                                                 (int)t.param, *reinterpret_cast<infl::WarpSmem*>(ws), &fin);
+            const uint32_t e = infl::stream_warp<0, 2048>(t.src, (uint32_t)t.src_len, t.dst, (uint32_t)t.dst_len,
+                                                       (int)t.param, *reinterpret_cast<BatchInflSmem*>(ws), &fin);
             return (e == ST_OK && fin != (uint32_t)t.dst_len) ? (uint32_t)ST_CORRUPT : e;
         }
         default:

@@ -72,10 +72,10 @@ struct Batch {
 // run other decoders beside this one).  NB = 1: one warp decodes and
 // executes; NB = 2: a decoder warp fills batch k+1 while a writer warp
 // executes batch k.
-template <uint32_t WIN, int NB = 1>
+template <uint32_t WIN, int NB = 1, uint32_t RB = IRING>
 struct alignas(16) WarpSmemT {
     uint8_t win[WIN ? WIN : 16];
-    uint8_t ring[IRING];
+    uint8_t ring[RB];
     Huff lit;
     Huff dist;
     uint8_t lens[320];
@@ -88,12 +88,120 @@ struct alignas(16) WarpSmemT {
 };
 using WarpSmem = WarpSmemT<0, 1>;
 
+// Windowless form: copies read the output already written (global memory).
+// Up to 4 consecutive commands whose sources all lie before the first of
+// them -- literal runs, and copies of at most 128 bytes whose distance
+// exceeds their offset into the group plus their length -- are executed
+// together: every lane issues all of its loads (4 bytes per command) before
+// any store, so the group pays one memory latency instead of one per
+// command.  Other commands run one at a time.
+static __device__ __forceinline__ void execute_batch_out(const Batch& B, uint32_t pos,
+                                                         const uint8_t* __restrict__ src,
+                                                         uint8_t* __restrict__ dst) {
+    const uint32_t lane = lane_id();
+    const uint32_t nc = B.n_cmd;
+    uint32_t c = 0;
+    while (c < nc) {
+        uint32_t tg[4], ag[4], ng[4];
+#pragma unroll
+        for (uint32_t i = 0; i < 4; ++i) {
+            const bool ok = c + i < nc;
+            tg[i] = ok ? B.cmd_t[c + i] : (uint32_t)C_STORED;
+            ag[i] = ok ? B.cmd_a[c + i] : 0u;
+            ng[i] = ok ? B.cmd_b[c + i] : 0u;
+        }
+        uint32_t g = 0, off = 0;
+#pragma unroll
+        for (uint32_t i = 0; i < 4; ++i) {
+            const bool fits = ng[i] <= 128u && (tg[i] == C_LIT || (tg[i] == C_COPY && ag[i] >= off + ng[i]));
+            if (g == i && fits) {
+                g = i + 1;
+                off += ng[i];
+            }
+        }
+        if (g >= 2) {
+            uint8_t v[4][4];
+            uint32_t o = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i) {
+#pragma unroll
+                for (uint32_t w = 0; w < 4; ++w) {
+                    const uint32_t k = lane + 32u * w;
+                    v[i][w] = 0;
+                    if (i < g && k < ng[i])
+                        v[i][w] = tg[i] == C_LIT ? B.lits[ag[i] + k] : dst[pos + o - ag[i] + k];
+                }
+                o += i < g ? ng[i] : 0u;
+            }
+            o = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i) {
+#pragma unroll
+                for (uint32_t w = 0; w < 4; ++w) {
+                    const uint32_t k = lane + 32u * w;
+                    if (i < g && k < ng[i]) dst[pos + o + k] = v[i][w];
+                }
+                o += i < g ? ng[i] : 0u;
+            }
+            pos += o;
+            c += g;
+            __syncwarp();
+            continue;
+        }
+        const uint32_t t = tg[0], a = ag[0], n = ng[0];
+        uint8_t* d = dst + pos;
+        if (t == C_LIT) {
+            for (uint32_t k = lane; k < n; k += 32) d[k] = B.lits[a + k];
+        } else if (t == C_STORED) {
+            const uint8_t* s = src + a;
+            for (uint32_t k = lane; k < n; k += 32) d[k] = s[k];
+        } else {
+            const uint8_t* s = d - a;
+            if (a >= 128) {  // 128-byte waves: one latency per 128 bytes
+                for (uint32_t k0 = 0; k0 < n; k0 += 128) {
+                    uint8_t v[4];
+#pragma unroll
+                    for (uint32_t w = 0; w < 4; ++w) {
+                        const uint32_t k = k0 + lane + 32u * w;
+                        v[w] = k < n ? s[k] : (uint8_t)0;
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (uint32_t w = 0; w < 4; ++w) {
+                        const uint32_t k = k0 + lane + 32u * w;
+                        if (k < n) d[k] = v[w];
+                    }
+                    __syncwarp();
+                }
+            } else if (a >= 32) {
+                for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+                    const uint32_t k = k0 + lane;
+                    uint8_t v = 0;
+                    if (k < n) v = s[k];
+                    __syncwarp();
+                    if (k < n) d[k] = v;
+                    __syncwarp();
+                }
+            } else {
+                for (uint32_t k = lane; k < n; k += 32) d[k] = s[k % a];
+            }
+        }
+        pos += n;
+        ++c;
+        __syncwarp();
+    }
+}
+
 // Write batch B (output starting at pos) with the calling warp.
 template <uint32_t WIN>
 static __device__ __forceinline__ void execute_batch(const Batch& B, uint32_t pos, uint8_t* win,
                                                      const uint8_t* __restrict__ src, uint8_t* __restrict__ dst) {
     const uint32_t lane = lane_id();
     const uint32_t nc = B.n_cmd;
+    if constexpr (WIN == 0) {
+        execute_batch_out(B, pos, src, dst);
+        return;
+    }
     // the next command's fields are loaded before the current one is written
     uint32_t tn = nc ? B.cmd_t[0] : 0u, an = nc ? B.cmd_a[0] : 0u, nn = nc ? B.cmd_b[0] : 0u;
     for (uint32_t c = 0; c < nc; ++c) {
@@ -164,27 +272,6 @@ static __device__ __forceinline__ void execute_batch(const Batch& B, uint32_t po
                     const uint8_t v = win[(sp + k % a) & M];
                     d[k] = v;
                     win[(pos + k) & M] = v;
-                }
-            }
-        } else {
-            if (t == C_LIT) {
-                for (uint32_t k = lane; k < n; k += 32) d[k] = B.lits[a + k];
-            } else if (t == C_STORED) {
-                const uint8_t* s = src + a;
-                for (uint32_t k = lane; k < n; k += 32) d[k] = s[k];
-            } else {
-                const uint8_t* s = d - a;
-                if (a >= 32) {
-                    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
-                        const uint32_t k = k0 + lane;
-                        uint8_t v = 0;
-                        if (k < n) v = s[k];
-                        __syncwarp();
-                        if (k < n) d[k] = v;
-                        __syncwarp();
-                    }
-                } else {
-                    for (uint32_t k = lane; k < n; k += 32) d[k] = s[k % a];
                 }
             }
         }
@@ -332,32 +419,33 @@ static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint
 // stream_warp is the out-of-line form for kernels that run several decoders.
 // NB = 2 (decoder of a pair): instead of executing a batch, hand it to the
 // writer warp (see stream_pair_writer); S.produced / S.consumed must be 0.
-template <uint32_t WIN, int NB = 1>
+template <uint32_t WIN, int NB = 1, uint32_t RB = IRING>
 static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __restrict__ src, uint32_t clen,
                                                             uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
-                                                            WarpSmemT<WIN, NB>& S, uint32_t* written) {
+                                                            WarpSmemT<WIN, NB, RB>& S, uint32_t* written) {
+    static_assert(RB >= 1024 && (RB & (RB - 1)) == 0, "input ring: a power of two >= 1 KiB");
     static_assert(WIN == 0 || (WIN >= 32768 && (WIN & (WIN - 1)) == 0), "window: 0 or a power of two >= 32 KiB");
     const uint32_t lane = lane_id();
     uint32_t err = ST_OK;
-    // input ring: compressed byte i (chunk-relative) at ring[(i + sh) % IRING];
+    // input ring: compressed byte i (chunk-relative) at ring[(i + sh) % RB];
     // fills are 16-byte aligned global loads.
     const uint32_t sh = (uint32_t)(reinterpret_cast<uintptr_t>(src) & 15u);
     const uint8_t* src_al = src - sh;
     const uint32_t span = clen + sh;  // bytes of the aligned view we may touch
     uint32_t fill = 0;                // aligned-view bytes loaded so far
     auto refill = [&](uint32_t consumed_al) {
-        // load the aligned view up to consumed_al + IRING (whole 16-byte words,
+        // load the aligned view up to consumed_al + RB (whole 16-byte words,
         // plus the ragged end of the chunk once it is reached)
-        uint32_t target = min(consumed_al + IRING, span);
+        uint32_t target = min(consumed_al + RB, span);
         if (target < span) target &= ~15u;
         if (target > fill) {
             const uint32_t a = fill, b = target & ~15u;
             for (uint32_t i = a + 16 * lane; i + 16 <= b; i += 512) {
                 const uint4 v = *reinterpret_cast<const uint4*>(src_al + i);
-                *reinterpret_cast<uint4*>(S.ring + (i & (IRING - 1))) = v;
+                *reinterpret_cast<uint4*>(S.ring + (i & (RB - 1))) = v;
             }
             for (uint32_t i = max(a, b) + lane; i < target; i += 32)
-                if (i >= sh) S.ring[i & (IRING - 1)] = src_al[i];
+                if (i >= sh) S.ring[i & (RB - 1)] = src_al[i];
             fill = target;
         }
         __syncwarp();
@@ -380,14 +468,14 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
         // zlib (RFC 1950): CMF, FLG; no preset dictionary
         if (clen < 2) err = ST_CORRUPT;
         else {
-            const uint32_t cmf = S.ring[(sh + 0) & (IRING - 1)], flg = S.ring[(sh + 1) & (IRING - 1)];
+            const uint32_t cmf = S.ring[(sh + 0) & (RB - 1)], flg = S.ring[(sh + 1) & (RB - 1)];
             if ((cmf & 15u) != 8u || ((cmf << 8) | flg) % 31u != 0 || (flg & 32u)) err = ST_CORRUPT;
             inpos += 2;
         }
         S.status = err;
     } else if (lane == 0 && err == ST_OK && zlib_hdr == 2) {
         // gzip (RFC 1952) member header; the 8-byte trailer is not read
-        auto at = [&](uint32_t i) -> uint32_t { return i < clen && sh + i < fill ? S.ring[(sh + i) & (IRING - 1)] : 0x100u; };
+        auto at = [&](uint32_t i) -> uint32_t { return i < clen && sh + i < fill ? S.ring[(sh + i) & (RB - 1)] : 0x100u; };
         uint32_t p = 10;
         if (at(0) != 0x1fu || at(1) != 0x8bu || at(2) != 8u || clen < 18) err = ST_CORRUPT;
         const uint32_t flg = at(3);
@@ -415,7 +503,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
     auto need_bits = [&](uint32_t n) -> bool {
         while (bitcnt < n) {
             if (inpos >= fill) return false;
-            bitbuf |= (uint64_t)S.ring[inpos & (IRING - 1)] << bitcnt;
+            bitbuf |= (uint64_t)S.ring[inpos & (RB - 1)] << bitcnt;
             ++inpos;
             bitcnt += 8;
         }
@@ -423,21 +511,21 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
     };
     // top up bitbuf: single bytes up to a 4-byte boundary of the stream,
     // then one aligned 32-bit word per call (the ring is word aligned and
-    // IRING a multiple of 4), single bytes again at the end of the input
+    // RB a multiple of 4), single bytes again at the end of the input
     auto fill_bits = [&]() {
         while (bitcnt <= 56 && inpos < fill && (inpos & 3u)) {
-            bitbuf |= (uint64_t)S.ring[inpos & (IRING - 1)] << bitcnt;
+            bitbuf |= (uint64_t)S.ring[inpos & (RB - 1)] << bitcnt;
             ++inpos;
             bitcnt += 8;
         }
         if (bitcnt <= 32 && (inpos & 3u) == 0 && inpos + 4 <= fill) {
-            const uint32_t w = *reinterpret_cast<const uint32_t*>(S.ring + (inpos & (IRING - 1)));
+            const uint32_t w = *reinterpret_cast<const uint32_t*>(S.ring + (inpos & (RB - 1)));
             bitbuf |= (uint64_t)w << bitcnt;
             inpos += 4;
             bitcnt += 32;
         }
         while (bitcnt <= 56 && inpos < fill && inpos + 4 > fill) {
-            bitbuf |= (uint64_t)S.ring[inpos & (IRING - 1)] << bitcnt;
+            bitbuf |= (uint64_t)S.ring[inpos & (RB - 1)] << bitcnt;
             ++inpos;
             bitcnt += 8;
         }
@@ -684,7 +772,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                 // (long codes, invalid entries) falls to the checked loop
                 {
                     const uint32_t* r32 = reinterpret_cast<const uint32_t*>(S.ring);
-                    constexpr uint32_t RW = IRING / 4 - 1;
+                    constexpr uint32_t RW = RB / 4 - 1;
                     auto top32 = [&]() {
                         if (bitcnt <= 32) {
                             const uint32_t k = inpos >> 2;
@@ -868,11 +956,11 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
     return __shfl_sync(GD_FULL_MASK, err, 0);
 }
 
-template <uint32_t WIN>
+template <uint32_t WIN, uint32_t RB = IRING>
 static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ src, uint32_t clen,
                                                     uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
-                                                    WarpSmemT<WIN>& S, uint32_t* written) {
-    return stream_warp_impl<WIN>(src, clen, dst, olen, zlib_hdr, S, written);
+                                                    WarpSmemT<WIN, 1, RB>& S, uint32_t* written) {
+    return stream_warp_impl<WIN, 1, RB>(src, clen, dst, olen, zlib_hdr, S, written);
 }
 
 // Writer warp of a pair: executes batch k while the decoder warp (running
