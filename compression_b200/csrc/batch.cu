@@ -20,10 +20,11 @@ namespace gd {
 namespace batch {
 
 constexpr int WPB = 4;  // warps per block
-// Deflate workspace of a batch warp: no window, a 2 KiB input ring (the
-// standalone kernels use 8 KiB); it sets every warp's workspace size, so it
-// is kept small for occupancy.
-using BatchInflSmem = infl::WarpSmemT<0, 1, 2048>;
+// Deflate workspace of a batch warp: no window, a 1 KiB input ring, an 8-bit
+// distance table and batches of 1024 literals / 128 commands (the standalone
+// kernels use 8 KiB, 10 bits, 2048 / 256); the largest codec workspace sets
+// every warp's, so it is kept small for occupancy.
+using BatchInflSmem = infl::WarpSmemT<0, 1, 1024, 8, 1024, 128>;
 
 __host__ __device__ constexpr uint32_t warp_smem_bytes(uint32_t max_lane) {
     // union of the per-codec warp workspaces
@@ -114,8 +115,9 @@ __device__ uint32_t run_task(const gd_task& t, uint32_t max_lane, uint8_t* ws) {
         case GD_CODEC_DEFLATE: {
             if (t.src_len > 0xffffffffull || t.dst_len > 0xffffffffull) return ST_INVALID;
             uint32_t fin = 0;
-            const uint32_t e = infl::stream_warp<0, 2048>(t.src, (uint32_t)t.src_len, t.dst, (uint32_t)t.dst_len,
-                                                       (int)t.param, *reinterpret_cast<BatchInflSmem*>(ws), &fin);
+            const uint32_t e = infl::stream_warp<0, 1024, 8, 1024, 128>(t.src, (uint32_t)t.src_len, t.dst,
+                                                                     (uint32_t)t.dst_len, (int)t.param,
+                                                                     *reinterpret_cast<BatchInflSmem*>(ws), &fin);
             return (e == ST_OK && fin != (uint32_t)t.dst_len) ? (uint32_t)ST_CORRUPT : e;
         }
         default:

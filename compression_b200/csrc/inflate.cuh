@@ -47,23 +47,28 @@ __device__ __constant__ uint8_t DEXT[30] = {0, 0, 0, 0, 1, 1, 2, 2,  3,  3,  4, 
 __device__ __constant__ uint8_t CLORDER[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
 
 // A canonical Huffman code: primary table + count/symbol arrays for the walk.
-struct Huff {
-    uint32_t lut[1 << LBITS];  // (sym << 8) | len, len 0 = longer than LBITS, 0xffffffff = invalid
+template <uint32_t BITS>
+struct HuffT {
+    uint32_t lut[1u << BITS];  // (sym << 8) | len, len 0 = longer than LBITS, 0xffffffff = invalid
     uint16_t count[16];
     uint16_t sym[320];
 };
+using Huff = HuffT<LBITS>;
 
 enum : uint32_t { C_LIT = 0, C_COPY = 1, C_STORED = 2 };
 
 // One batch of decoded commands: literal bytes, commands, and the output
 // position of its first byte.  last = no batch follows (pair hand-off).
-struct Batch {
-    uint8_t lits[NLIT];
-    uint32_t cmd_a[NCMD];  // C_LIT: literal buffer offset | C_COPY: distance | C_STORED: input offset
-    uint32_t cmd_b[NCMD];  // length
-    uint8_t cmd_t[NCMD];
+template <uint32_t NL, uint32_t NC>
+struct BatchT {
+    static constexpr uint32_t kLits = NL, kCmds = NC;
+    uint8_t lits[NL];
+    uint32_t cmd_a[NC];  // C_LIT: literal buffer offset | C_COPY: distance | C_STORED: input offset
+    uint32_t cmd_b[NC];  // length
+    uint8_t cmd_t[NC];
     uint32_t n_cmd, n_lit, pos0, last;
 };
+using Batch = BatchT<NLIT, NCMD>;
 
 // Per-stream shared state.  WIN > 0: the last WIN output bytes are kept in a
 // shared-memory window (WIN a power of two >= 32768, the Deflate window), so
@@ -72,16 +77,18 @@ struct Batch {
 // run other decoders beside this one).  NB = 1: one warp decodes and
 // executes; NB = 2: a decoder warp fills batch k+1 while a writer warp
 // executes batch k.
-template <uint32_t WIN, int NB = 1, uint32_t RB = IRING>
+// RB: input ring bytes; DB: distance lookup bits; NL / NC: literal bytes and
+// commands per batch (smaller values for kernels that run many warps).
+template <uint32_t WIN, int NB = 1, uint32_t RB = IRING, uint32_t DB = LBITS, uint32_t NL = NLIT, uint32_t NC = NCMD>
 struct alignas(16) WarpSmemT {
     uint8_t win[WIN ? WIN : 16];
     uint8_t ring[RB];
-    Huff lit;
-    Huff dist;
+    HuffT<LBITS> lit;
+    HuffT<DB> dist;
     uint8_t lens[320];
     uint8_t cl_tmp[320];   // code lengths while a dynamic header is read
     uint16_t offs[16];     // canonical code offsets (build_huff)
-    Batch bt[NB];
+    BatchT<NL, NC> bt[NB];
     // decoder state shared between lane 0 and the warp
     uint32_t status, done;
     uint32_t produced, consumed;  // pair hand-off counters
@@ -95,7 +102,8 @@ using WarpSmem = WarpSmemT<0, 1>;
 // together: every lane issues all of its loads (4 bytes per command) before
 // any store, so the group pays one memory latency instead of one per
 // command.  Other commands run one at a time.
-static __device__ __forceinline__ void execute_batch_out(const Batch& B, uint32_t pos,
+template <class BatchType>
+static __device__ __forceinline__ void execute_batch_out(const BatchType& B, uint32_t pos,
                                                          const uint8_t* __restrict__ src,
                                                          uint8_t* __restrict__ dst) {
     const uint32_t lane = lane_id();
@@ -193,8 +201,8 @@ static __device__ __forceinline__ void execute_batch_out(const Batch& B, uint32_
 }
 
 // Write batch B (output starting at pos) with the calling warp.
-template <uint32_t WIN>
-static __device__ __forceinline__ void execute_batch(const Batch& B, uint32_t pos, uint8_t* win,
+template <uint32_t WIN, class BatchType>
+static __device__ __forceinline__ void execute_batch(const BatchType& B, uint32_t pos, uint8_t* win,
                                                      const uint8_t* __restrict__ src, uint8_t* __restrict__ dst) {
     const uint32_t lane = lane_id();
     const uint32_t nc = B.n_cmd;
@@ -352,10 +360,11 @@ __device__ __forceinline__ uint32_t make_entry(uint32_t tk, uint32_t sym, uint32
 // Build `h` from code lengths lens[0..n) for table kind tk.  Counting /
 // offsets on lane 0, the primary table fill spread over the warp.  Returns
 // false (on every lane) for an over-subscribed or otherwise unusable code.
-static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint32_t* sh_flag, uint16_t* offs,
+template <uint32_t BITS>
+static __device__ bool build_huff(HuffT<BITS>* h, const uint8_t* lens, uint32_t n, uint32_t* sh_flag, uint16_t* offs,
                                   uint32_t tk) {
     const uint32_t lane = lane_id();
-    for (uint32_t i = lane; i < (1u << LBITS); i += 32) h->lut[i] = 0xffffffffu;
+    for (uint32_t i = lane; i < (1u << BITS); i += 32) h->lut[i] = 0xffffffffu;
     if (lane == 0) {
         for (int i = 0; i < 16; ++i) h->count[i] = 0;
         for (uint32_t s = 0; s < n; ++s) h->count[lens[s]]++;
@@ -376,7 +385,7 @@ static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint
     if (!*sh_flag) return false;
     // canonical codes in symbol order: code(s) = first(len) + rank among equal lengths
     // lane-parallel: every lane walks the sorted symbol list for a subset of lengths
-    for (uint32_t L = 1 + lane; L <= LBITS; L += 32) {
+    for (uint32_t L = 1 + lane; L <= BITS; L += 32) {
         uint32_t first = 0, idx = 0;
         uint32_t code = 0;
         for (uint32_t l = 1; l < L; ++l) {
@@ -389,12 +398,12 @@ static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint
             // deflate sends codes MSB first into an LSB-first stream: reverse
             const uint32_t rev = __brev(c) >> (32 - L);
             const uint32_t entry = make_entry(tk, h->sym[idx + k], L);
-            for (uint32_t f = rev; f < (1u << LBITS); f += (1u << L)) h->lut[f] = entry;
+            for (uint32_t f = rev; f < (1u << BITS); f += (1u << L)) h->lut[f] = entry;
         }
     }
     __syncwarp();
-    // prefixes of codes longer than LBITS: mark for the canonical walk
-    for (uint32_t L = LBITS + 1 + lane; L < 16; L += 32) {
+    // prefixes of codes longer than BITS: mark for the canonical walk
+    for (uint32_t L = BITS + 1 + lane; L < 16; L += 32) {
         uint32_t code = 0, idx = 0;
         for (uint32_t l = 1; l < L; ++l) {
             code = (code + h->count[l]) << 1;
@@ -402,7 +411,7 @@ static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint
         }
         for (uint32_t k = 0; k < h->count[L]; ++k) {
             const uint32_t c = code + k;
-            const uint32_t pre = __brev(c >> (L - LBITS)) >> (32 - LBITS);
+            const uint32_t pre = __brev(c >> (L - BITS)) >> (32 - BITS);
             atomicExch(&h->lut[pre], 0u);  // len 0: walk
         }
     }
@@ -419,10 +428,10 @@ static __device__ bool build_huff(Huff* h, const uint8_t* lens, uint32_t n, uint
 // stream_warp is the out-of-line form for kernels that run several decoders.
 // NB = 2 (decoder of a pair): instead of executing a batch, hand it to the
 // writer warp (see stream_pair_writer); S.produced / S.consumed must be 0.
-template <uint32_t WIN, int NB = 1, uint32_t RB = IRING>
+template <uint32_t WIN, int NB = 1, uint32_t RB = IRING, uint32_t DB = LBITS, uint32_t NL = NLIT, uint32_t NC = NCMD>
 static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __restrict__ src, uint32_t clen,
                                                             uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
-                                                            WarpSmemT<WIN, NB, RB>& S, uint32_t* written) {
+                                                            WarpSmemT<WIN, NB, RB, DB, NL, NC>& S, uint32_t* written) {
     static_assert(RB >= 1024 && (RB & (RB - 1)) == 0, "input ring: a power of two >= 1 KiB");
     static_assert(WIN == 0 || (WIN >= 32768 && (WIN & (WIN - 1)) == 0), "window: 0 or a power of two >= 32 KiB");
     const uint32_t lane = lane_id();
@@ -539,7 +548,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
     };
     // decode one symbol of code h; returns false on exhausted input / bad code
     // canonical walk (puff-style) for codes longer than LBITS
-    auto walk = [&](const Huff* h, uint32_t& sym) -> bool {
+    auto walk = [&](const auto* h, uint32_t& sym) -> bool {
         int code = 0, first = 0, index = 0;
         uint64_t bb = bitbuf;
         for (uint32_t L = 1; L < 16; ++L) {
@@ -561,9 +570,9 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
         return false;
     };
     // decode one entry of table h (kind tk); false on exhausted input / bad code
-    auto decode_ent = [&](const Huff* h, uint32_t tk, uint32_t& e) -> bool {
+    auto decode_ent = [&](const auto* h, uint32_t tk, uint32_t& e) -> bool {
         fill_bits();
-        e = h->lut[bitbuf & ((1u << LBITS) - 1u)];
+        e = h->lut[bitbuf & (uint64_t)(sizeof(h->lut) / 4 - 1)];
         const uint32_t L = e & 15u;
         if (e != 0xffffffffu && L != 0) {
             if (L > bitcnt) return false;
@@ -578,7 +587,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
         return true;
     };
     // one symbol of a plain table (the code-length code)
-    auto decode_sym = [&](const Huff* h, uint32_t& sym) -> bool {
+    auto decode_sym = [&](const auto* h, uint32_t& sym) -> bool {
         uint32_t e;
         if (!decode_ent(h, TK_PLAIN, e)) return false;
         sym = (e >> 8) & 0xffffu;
@@ -589,7 +598,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
     // main loop ------------------------------------------------------------
     uint32_t kb = 0;  // batches handed off (pairs: the buffer is bt[kb & 1])
     while (err == ST_OK) {
-        Batch& BT = S.bt[NB == 2 ? (kb & 1u) : 0u];
+        auto& BT = S.bt[NB == 2 ? (kb & 1u) : 0u];
         // pairs: the buffer's previous batch (kb - 2) must have been executed
         if constexpr (NB == 2) {
             if (kb >= 2 && !pair_wait(&S.consumed, kb - 1)) {
@@ -782,7 +791,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                             inpos += 4;
                         }
                     };
-                    while (nc < NCMD - 2 && nl < NLIT && fill - inpos >= 16) {
+                    while (nc < NC - 2 && nl < NL && fill - inpos >= 16) {
                         top32();
                         const uint32_t e = S.lit.lut[(uint32_t)bitbuf & ((1u << LBITS) - 1u)];
                         const uint32_t L = e & 15u;
@@ -811,7 +820,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                             c2 += 32;
                             inpos += 4;
                         }
-                        const uint32_t ed = S.dist.lut[(uint32_t)b2 & ((1u << LBITS) - 1u)];
+                        const uint32_t ed = S.dist.lut[(uint32_t)b2 & ((1u << DB) - 1u)];
                         const uint32_t Ld = ed & 15u;
                         if (Ld == 0 || (ed >> 24) != E_DIST) {
                             // long or bad distance code: undo to the length symbol
@@ -844,7 +853,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                         opos += len;
                     }
                 }
-                while (err == ST_OK && nc < NCMD - 2 && nl < NLIT && (fill - inpos >= 32 || fill >= span)) {
+                while (err == ST_OK && nc < NC - 2 && nl < NL && (fill - inpos >= 32 || fill >= span)) {
                     uint32_t e;
                     if (!decode_ent(&S.lit, TK_LIT, e)) {
                         err = ST_CORRUPT;
@@ -944,7 +953,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
     }
     if constexpr (NB == 2) {  // the final (empty) hand-off
         if (err != ST_TIMEOUT && kb >= 2 && !pair_wait(&S.consumed, kb - 1)) err = ST_TIMEOUT;
-        Batch& BT = S.bt[kb & 1u];
+        auto& BT = S.bt[kb & 1u];
         if (lane == 0) {
             BT.n_cmd = 0;
             BT.last = 1;
@@ -956,11 +965,11 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
     return __shfl_sync(GD_FULL_MASK, err, 0);
 }
 
-template <uint32_t WIN, uint32_t RB = IRING>
+template <uint32_t WIN, uint32_t RB = IRING, uint32_t DB = LBITS, uint32_t NL = NLIT, uint32_t NC = NCMD>
 static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ src, uint32_t clen,
                                                     uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
-                                                    WarpSmemT<WIN, 1, RB>& S, uint32_t* written) {
-    return stream_warp_impl<WIN, 1, RB>(src, clen, dst, olen, zlib_hdr, S, written);
+                                                    WarpSmemT<WIN, 1, RB, DB, NL, NC>& S, uint32_t* written) {
+    return stream_warp_impl<WIN, 1, RB, DB, NL, NC>(src, clen, dst, olen, zlib_hdr, S, written);
 }
 
 // Writer warp of a pair: executes batch k while the decoder warp (running
@@ -972,7 +981,7 @@ static __device__ __forceinline__ uint32_t stream_pair_writer(WarpSmemT<WIN, 2>&
                                                               uint8_t* __restrict__ dst) {
     for (uint32_t kb = 0;; ++kb) {
         if (!pair_wait(&S.produced, kb + 1)) return ST_TIMEOUT;
-        Batch& BT = S.bt[kb & 1u];
+        auto& BT = S.bt[kb & 1u];
         if (BT.last) return ST_OK;
         execute_batch<WIN>(BT, BT.pos0, S.win, src, dst);
         pair_post(&S.consumed, kb + 1);
