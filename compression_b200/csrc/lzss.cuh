@@ -455,7 +455,8 @@ static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __res
     for (;;) {
         const bool act = (o < col_bytes) && (err == ST_OK);
         if (!__any_sync(GD_FULL_MASK, act)) break;
-        if (act && fl - rd <= (uint32_t)RING / 2 && fl < 4u * nw) prefetch();
+        // rings are topped up together once any active column's is half empty
+        if (__any_sync(GD_FULL_MASK, act && fl - rd <= (uint32_t)RING / 2 && fl < 4u * nw) && act) prefetch();
         // the group reads bytes rd .. rd+16, copied by all 8 lanes of the column
         const bool wait = act && arrived < fl && arrived < rd + 17u;
         if (__any_sync(GD_FULL_MASK, wait)) {
@@ -502,14 +503,17 @@ static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __res
         // pass 1: literals and matches whose source lies before the group
         const bool dep = exists && !lit && src + L > o0;
         if (exists && !dep) {
-            if (lit) {
-                col[ot] = (uint8_t)b0;
-            } else {
-                for (uint32_t j = 0; j < L; j += 8) {
-                    const uint64_t x = rd8(src + j);
-                    const uint32_t m = min(8u, L - j);
-                    for (uint32_t i = 0; i < m; ++i) col[ot + j + i] = (uint8_t)(x >> (8u * i));
-                }
+            // the first 8 bytes (a literal: its byte) as predicated stores
+            const uint64_t x = lit ? (uint64_t)b0 : rd8(src);
+            const uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32);
+            uint8_t* d = col + ot;
+#pragma unroll
+            for (uint32_t i = 0; i < 8; ++i)
+                if (i < L) d[i] = (uint8_t)((i < 4 ? lo : hi) >> (8u * (i & 3u)));
+            for (uint32_t j = 8; j < L; j += 8) {  // matches longer than 8 bytes
+                const uint64_t y = rd8(src + j);
+                const uint32_t m = min(8u, L - j);
+                for (uint32_t i = 0; i < m; ++i) d[j + i] = (uint8_t)(y >> (8u * i));
             }
         }
         // pass 2: the rest in token order, byte by byte
