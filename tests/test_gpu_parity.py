@@ -336,3 +336,30 @@ def test_inflate_variants(cuda, variant):
         _parity(enc, raw[: int(oo[-1])], cuda)
     finally:
         at.set_knob(at.TUNE_INFLATE_VARIANT, prev)
+
+
+def test_host_calls_in_many_pieces(cuda):
+    """Host calls large enough to run as many overlapped pieces (each at
+    least 4 MiB of output): byte-exact, for every codec, with pinned and
+    pageable input; Deflate streams of uneven size (longest first inside each
+    piece) and a last chunk that is short."""
+    raw = cc.gen_brle_bytes(21, 40 * (1 << 20) + 12345)
+    assert np.array_equal(cc.decode_host(cc.brle_encode(raw)), raw)
+    v1 = cc.gen_rlev1_ints(22, 9 * (1 << 20) // 4)
+    e1 = cc.rlev1_encode(v1, 128 * 1024, 128, 4)
+    assert np.array_equal(cc.decode_host(e1), v1.view(np.uint8))
+    cc.decode_host_pinned(e1)  # the pinned path runs without error
+    v2 = cc.gen_rlev2_ints(23, 40 * (1 << 20) // 8)
+    assert np.array_equal(cc.decode_host(cc.rlev2_encode(v2, 256 * 1024, 32)), v2.view(np.uint8))
+    lz = cc.gen_markov_copy(24, 40 * (1 << 20), 4096)
+    assert np.array_equal(cc.decode_host(cc.lzss_encode(lz, 64 * 1024)), lz)
+    bt = cc.gen_brle_bytes(25, 20 * (1 << 20))
+    assert np.array_equal(cc.decode_host(cc.brle_trans_encode(bt, 4096)), bt)
+    d = cc.gen_markov_copy(26, 48 * (1 << 20), 32768)
+    sizes = cc.loguniform_sizes(27, 300, 4096, 1 << 20, d.size)
+    oo = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    ed = cc.deflate_encode(d[: int(oo[-1])], oo)
+    assert np.array_equal(cc.decode_host(ed), d[: int(oo[-1])])
+    n9 = 9 * (1 << 20) + 5  # uniform 1 MiB chunks (the reference's container) and a 5-byte last one
+    oo9 = np.array(list(range(0, 9 * (1 << 20) + 1, 1 << 20)) + [n9], dtype=np.uint64)
+    assert np.array_equal(cc.decode_host(cc.deflate_encode(d[:n9], oo9)), d[:n9])
