@@ -133,6 +133,28 @@ class Clocks:
 
 
 # --------------------------------------------------------------------------
+# ranks
+# --------------------------------------------------------------------------
+
+def max_over_ranks(values, world: int, device="cpu"):
+    """Element-wise maximum of per-rank timings over all ranks (every rank
+    gets the result); identity for one rank.  Device tensors for NCCL, CPU
+    tensors for gloo."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def job_rate(bytes_per_rank: int, world: int, ms: float) -> float:
+    """Whole-job GB/s: every rank decodes bytes_per_rank (weak scaling) and
+    the job takes the slowest rank's time."""
+    return bytes_per_rank * world / (ms / 1e3) / 1e9
+
+
+# --------------------------------------------------------------------------
 # CPU baselines (oracle restatement or the reference's own code)
 # --------------------------------------------------------------------------
 
@@ -334,13 +356,9 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
     per_kernel = [[evs[k][i][0].elapsed_time(evs[k][i][1]) for k in range(K)] for i in range(len(jobs))]
     step_ms = [sum(per_kernel[i][k] for i in range(len(jobs))) for k in range(K)]
-    ms = statistics.mean(step_ms)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks([statistics.mean(step_ms)], world, dev)[0]
     out_bytes = sum(e.n_out for _, e, _ in cols)
-    value = out_bytes * world / (ms / 1e3) / 1e9
+    value = job_rate(out_bytes, world, ms)
 
     # roofline of the dominant kernel: algorithmic bytes = compressed payload
     # + metadata read + decompressed bytes written, per launch
@@ -375,8 +393,8 @@ def run_ours(args, rank, world, local_rank):
             for _, e, _ in cols:
                 cc.decode_host_pinned(e)
             ts.append(time.perf_counter() - t0)
-        e2e_s = statistics.median(ts)
-        e2e = {"value": round(out_bytes * world / e2e_s / 1e9, 3), "unit": "GB/s",
+        e2e_s = max_over_ranks([statistics.median(ts)], world, dev)[0]
+        e2e = {"value": round(job_rate(out_bytes, world, e2e_s * 1e3), 3), "unit": "GB/s",
                "h2d_bytes_per_step": int(tot_h2d), "d2h_bytes_per_step": int(out_bytes),
                "path": "gd_*_decompress host C-ABI calls (pinned host buffers)"}
 
@@ -503,17 +521,13 @@ def run_mixed(args, rank, world, local_rank):
                 torch.cuda.synchronize()
                 times[kind].append(a.elapsed_time(b))
     med = {k: statistics.median(v) for k, v in times.items()}
-    ms = med["learned"]
-    if world > 1:
-        t = torch.tensor([ms, med["static"], med["queue"]], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms, med["static"], med["queue"] = [float(x) for x in t.tolist()]
+    ms, med["static"], med["queue"] = max_over_ranks([med["learned"], med["static"], med["queue"]], world, dev)
     plan.d_out.zero_()
     graph.replay()
     torch.cuda.synchronize()
     if not B.verify(plan, expect):
         raise RuntimeError("mixed batch: learned schedule output differs")
-    value = out_bytes * world / (ms / 1e3) / 1e9
+    value = job_rate(out_bytes, world, ms)
     peak, peak_kind = peaks()
     alg = comp_bytes + out_bytes
     ach = alg / (ms / 1e3) / 1e9
@@ -538,7 +552,8 @@ def run_mixed(args, rank, world, local_rank):
             torch.cuda.synchronize()
             if i:
                 ts.append(time.perf_counter() - t1)
-        e2e = {"value": round(out_bytes * world / statistics.median(ts) / 1e9, 3), "unit": "GB/s",
+        e2e_s = max_over_ranks([statistics.median(ts)], world, dev)[0]
+        e2e = {"value": round(job_rate(out_bytes, world, e2e_s * 1e3), 3), "unit": "GB/s",
                "h2d_bytes_per_step": int(h_in.numel() + h_meta.numel()), "d2h_bytes_per_step": int(h_out.numel()),
                "path": "batch API: pinned arenas H2D, graph replay, output arena D2H"}
 
