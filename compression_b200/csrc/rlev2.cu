@@ -437,7 +437,8 @@ extern "C" gd_status_t gd_rlev2_decode(const uint8_t* d_data, const uint64_t* d_
     // (a bound above the longest valid stream is clamped: longer lanes are
     // corrupt), plus 16 bytes for the header parser's 24-byte window reads
     const uint32_t cap = (max_lane_bytes ? min(lane_cap(max_lane_bytes), stream_cap(nv)) : stream_cap(nv)) + 16u;
-    const int lpb = gd_tune_get(GD_TUNE_RLEV2_LANES_PER_BLOCK) == 8 ? 8 : 4;
+    const int knob = gd_tune_get(GD_TUNE_RLEV2_LANES_PER_BLOCK);
+    const int lpb = knob == 8 ? 8 : 4;
     const uint32_t smem = (uint32_t)lpb * cap;
     if (smem > 200 * 1024) return GD_ERR_UNSUPPORTED;  // lane streams must fit in shared memory
     cudaStream_t s = (cudaStream_t)stream;

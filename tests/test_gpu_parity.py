@@ -363,3 +363,39 @@ def test_host_calls_in_many_pieces(cuda):
     n9 = 9 * (1 << 20) + 5  # uniform 1 MiB chunks (the reference's container) and a 5-byte last one
     oo9 = np.array(list(range(0, 9 * (1 << 20) + 1, 1 << 20)) + [n9], dtype=np.uint64)
     assert np.array_equal(cc.decode_host(cc.deflate_encode(d[:n9], oo9)), d[:n9])
+
+
+@pytest.mark.parametrize("knob", [4, 8])
+def test_rlev2_decoder_shapes(cuda, knob):
+    """Both RLE v2 kernel shapes (4 / 8 lane streams per block) on all four run kinds, signed and 64-bit-wide values, wide
+    patches, a short last chunk, READ_UNIT 8 / 32 / 64 and the reference
+    encoder's fixed-delta quirk, against the oracle; corrupt streams fail."""
+    import compression_b200.autotune as at
+    rng = np.random.default_rng(knob)
+    v = np.concatenate([rng.integers(-2**62, 2**62, 3000), -np.arange(3000), np.full(500, -7),
+                        rng.integers(0, 2**12, 3000) + (rng.random(3000) < 0.03) * 2**50,
+                        cc.gen_rlev2_ints(knob, 40000)]).astype(np.int64)
+    prev = at.set_knob(at.TUNE_RLEV2_LANES_PER_BLOCK, knob)
+    try:
+        for ru in (8, 32, 64):
+            enc = cc.rlev2_encode(v, 256 * ru * 4, ru)
+            rc, ref = oracle.decode(enc)
+            assert rc == 0
+            st, out = _gpu(enc, cuda)
+            assert (st == 0).all(), np.unique(st)
+            assert np.array_equal(out, ref)
+        quirk = cc.gen_rlev2_ints(0xE0 * 100003 + 9149, 5120 * 8)
+        enc = cc.rlev2_encode(quirk, 256 * 32, 32)
+        rc, ref = oracle.decode(enc)
+        st, out = _gpu(enc, cuda)
+        assert rc == 0 and (st == 0).all() and np.array_equal(out, ref)
+        bad = cc.rlev2_encode(cc.gen_rlev2_ints(5, 40000), 256 * 32, 32)
+        bad.meta["col_len"][0] += 1000000  # beyond the block
+        st, _ = _gpu(bad, cuda)
+        assert (st != 0).any()
+        bad2 = cc.rlev2_encode(cc.gen_rlev2_ints(6, 40000), 256 * 32, 32)
+        bad2.data[: bad2.data.size // 2] = 0xFF  # garbage headers
+        st, _ = _gpu(bad2, cuda)
+        assert (st != 0).any()
+    finally:
+        at.set_knob(at.TUNE_RLEV2_LANES_PER_BLOCK, prev)
