@@ -51,13 +51,14 @@ __global__ void __launch_bounds__(32) decode_staged_kernel(const uint8_t* __rest
     if (lane_id() == 0) put_status(status, chunk, err);
 }
 
-// One 256-thread block per chunk, 8 lanes per column (chunk_block_cols).
-__global__ void __launch_bounds__(256) decode_cols_kernel(const uint8_t* __restrict__ data,
-                                                          const uint64_t* __restrict__ blk_off,
-                                                          const uint64_t* __restrict__ col_len,
-                                                          const uint8_t* __restrict__ col_map, uint32_t n_chunks,
-                                                          uint64_t chunk_size, uint8_t* out,
-                                                          uint32_t* __restrict__ status) {
+// One block of 32*G threads per chunk, G lanes per column (chunk_block_cols).
+template <uint32_t G>
+__global__ void __launch_bounds__(32 * G) decode_cols_kernel(const uint8_t* __restrict__ data,
+                                                             const uint64_t* __restrict__ blk_off,
+                                                             const uint64_t* __restrict__ col_len,
+                                                             const uint8_t* __restrict__ col_map, uint32_t n_chunks,
+                                                             uint64_t chunk_size, uint8_t* out,
+                                                             uint32_t* __restrict__ status) {
     extern __shared__ __align__(16) uint8_t smem[];
     const uint32_t chunk = blockIdx.x;
     if (chunk >= n_chunks) return;  // block-uniform
@@ -66,8 +67,8 @@ __global__ void __launch_bounds__(256) decode_cols_kernel(const uint8_t* __restr
     if (b1 < b0) {
         err = ST_CORRUPT;
     } else {
-        err = chunk_block_cols(data + b0, b1 - b0, col_len + 32ull * chunk, col_map + 32ull * chunk, chunk_size,
-                               out + (uint64_t)chunk * chunk_size, smem);
+        err = chunk_block_cols<G>(data + b0, b1 - b0, col_len + 32ull * chunk, col_map + 32ull * chunk, chunk_size,
+                                  out + (uint64_t)chunk * chunk_size, smem);
     }
     if (threadIdx.x == 0) put_status(status, chunk, err);
 }
@@ -92,12 +93,15 @@ extern "C" gd_status_t gd_lzss_decode(const uint8_t* d_data, const uint64_t* d_b
     const uint32_t staged = staged_smem(chunk_size);
     const int k = gd_tune_get(GD_TUNE_LZSS_WARPS_PER_BLOCK);
     const uint32_t cs = cols_smem(chunk_size);
-    if (k == 0 && cs <= 227u * 1024u) {
-        cudaFuncSetAttribute(decode_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cs);
-        cudaFuncSetAttribute(decode_cols_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared);
-        decode_cols_kernel<<<n_chunks, 256, cs, (cudaStream_t)stream>>>(d_data, d_blk_off, d_col_len, d_col_map,
-                                                                       n_chunks, chunk_size, d_out, d_status);
+    if ((k == 0 || k == 256 || k == 512) && cs <= 227u * 1024u) {
+        auto go = [&](auto kern, uint32_t threads) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, cs);
+            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+            kern<<<n_chunks, threads, cs, (cudaStream_t)stream>>>(d_data, d_blk_off, d_col_len, d_col_map, n_chunks,
+                                                                 chunk_size, d_out, d_status);
+        };
+        if (k == 256) go(decode_cols_kernel<8>, 256);
+        else go(decode_cols_kernel<16>, 512);
         return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
     }
     if (k <= 1 && staged <= 227u * 1024u && (reinterpret_cast<uintptr_t>(d_out) & 15u) == 0) {

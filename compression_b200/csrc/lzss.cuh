@@ -351,26 +351,31 @@ static __device__ __noinline__ uint32_t chunk_warp_staged(const uint8_t* __restr
 }
 
 // ---------------------------------------------------------------------------
-// Column-group decoder: one block of 8 warps per chunk, 8 lanes per column.
+// Column-group decoder: one block per chunk, G = 8 or 16 lanes per column.
 //
-// Lanes 8s..8s+7 of warp w decode column rank 4w+s, one flag group per step:
-// lane t takes token t of the group (its bytes follow from the flag byte
-// alone), the 8 lengths are prefix-summed across the lanes for the output
-// offsets, and every token is written at once -- literals and matches whose
-// source lies before the group (almost all) in one pass, the rest (source
-// inside the group, offset below the length) in token order afterwards.  The
+// The G lanes of a column decode G/8 flag groups per step: lane t takes
+// token t (its bytes follow from the flag bytes alone; the second group's
+// flag byte sits 17 - popc(first flag) bytes after the first's), the G
+// lengths are prefix-summed across the lanes for the output offsets, and
+// every token is written at once -- literals and matches whose source lies
+// before the step's first output byte (almost all) in one pass, the rest
+// (source inside the step's output, offset below the length) in token order
+// afterwards.  The
 // chunk's output is staged column by column in shared memory (column q at
 // q*(col_bytes+4): 8-byte source reads are one funnel shift, and the final
 // row-major writes read the 32 columns of a row from 32 different banks).
 // Each column's compressed words arrive in a per-column ring by cp.async,
-// issued by the column's 8 lanes half a ring ahead of use.
+// issued by the column's G lanes half a ring ahead of use.
 // ---------------------------------------------------------------------------
 __host__ __device__ constexpr uint32_t cols_stride(uint64_t chunk_size) { return (uint32_t)(chunk_size / 32) + 4u; }
 __host__ __device__ constexpr uint32_t cols_smem(uint64_t chunk_size) {
     return 32u * cols_stride(chunk_size) + 16u + 32u * RING_STRIDE + (uint32_t)sizeof(SegTable) + 32u * 8u + 16u;
 }
 
-// Must be called by all 256 threads of the block; returns the chunk status.
+// G lanes per column (8: one flag group per step; 16: two, the second's flag
+// byte found from the first's).  Must be called by all 32*G threads of the
+// block; returns the chunk status.
+template <uint32_t G>
 static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __restrict__ block, uint64_t b_len,
                                                            const uint64_t* __restrict__ col_len,
                                                            const uint8_t* __restrict__ col_map,
@@ -412,9 +417,15 @@ static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __res
     __syncthreads();
     if (*s_err != ST_OK) return *s_err;
 
-    const uint32_t sub = lane >> 3, t = lane & 7u;
-    const uint32_t rank = 4u * wid + sub;
-    const uint32_t seg0 = 8u * sub;  // first lane of this column's group
+    static_assert(G == 8 || G == 16, "8 or 16 lanes per column");
+    constexpr uint32_t CPW = 32u / G;         // columns per warp
+    constexpr uint32_t NWARPS = G;            // warps per block (32 columns)
+    constexpr uint32_t GMASK = (1u << G) - 1u;
+    constexpr uint32_t NGRP = G / 8u;         // flag groups per step
+    const uint32_t sub = lane / G, t = lane % G;
+    const uint32_t rank = CPW * wid + sub;
+    const uint32_t seg0 = G * sub;  // first lane of this column's group
+    const uint32_t cmask = GMASK << seg0;
     const uint32_t q = s_q[rank], len = s_len[rank];
     const uint32_t nw = (len + 3) >> 2;
     const uint32_t col_bytes = (uint32_t)(chunk_size / 32);
@@ -426,7 +437,7 @@ static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __res
     lw.nw = nw;
     lw.j = 0;
     lw_seek_seg(lw, T_, ltmask);
-    uint32_t nextk = t;  // this lane copies words t, t+8, t+16, ... of the stream
+    uint32_t nextk = t;  // this lane copies words t, t+G, t+2G, ... of the stream
 
     // column state, identical in the column's 8 lanes
     uint32_t rd = 0, o = 0, fl = 0, arrived = 0, err = ST_OK;
@@ -434,7 +445,7 @@ static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __res
     auto prefetch = [&]() {  // top the ring up to 63 words past rd's word
         const uint32_t tgt = min(nw, (rd >> 2) + 63u);
         uint32_t n = 0;
-        for (; nextk < tgt; nextk += 8) {
+        for (; nextk < tgt; nextk += G) {
             const uint32_t off = lw_addr(lw, T_, ltmask, nextk);
             const uint32_t sa = (uint32_t)__cvta_generic_to_shared(rbuf + ((4u * nextk) & (RING - 1)));
             asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(block + off) : "memory");
@@ -457,8 +468,8 @@ static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __res
         if (!__any_sync(GD_FULL_MASK, act)) break;
         // rings are topped up together once any active column's is half empty
         if (__any_sync(GD_FULL_MASK, act && fl - rd <= (uint32_t)RING / 2 && fl < 4u * nw) && act) prefetch();
-        // the group reads bytes rd .. rd+16, copied by all 8 lanes of the column
-        const bool wait = act && arrived < fl && arrived < rd + 17u;
+        // a step reads bytes rd .. rd+17*NGRP-1, copied by all G lanes of the column
+        const bool wait = act && arrived < fl && arrived < rd + 17u * NGRP;
         if (__any_sync(GD_FULL_MASK, wait)) {
             asm volatile("cp.async.wait_all;\n" ::: "memory");
             __syncwarp();
@@ -468,35 +479,43 @@ static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __res
         const uint32_t o0 = o;  // the group's first output byte
         bool exists = false;
         if (act) {
-            if (rd >= len) code = ST_CORRUPT;
-            flag = rb(rd);
-            lit = (flag >> t) & 1u;
-            const uint32_t pos = rd + 1u + t + __popc(~flag & ((1u << t) - 1u));
+            // flag byte of each group of the step (the second follows the
+            // first group's 8 tokens: 17 - popc(flag) bytes after it)
+            const uint32_t f0 = rb(rd);
+            const uint32_t rd1 = rd + 17u - __popc(f0);
+            const uint32_t f1 = NGRP == 2 ? rb(rd1) : 0u;
+            const uint32_t gi = t >> 3, tb = t & 7u;
+            const uint32_t rdg = gi ? rd1 : rd;
+            flag = gi ? f1 : f0;
+            lit = (flag >> tb) & 1u;
+            const uint32_t pos = rdg + 1u + tb + __popc(~flag & ((1u << tb) - 1u));
             b0 = rb(pos);
             const uint32_t v = b0 | (rb(pos + 1u) << 8);
             L = lit ? 1u : (v & 31u) + 3u;
             uint32_t inc = L;
 #pragma unroll
-            for (uint32_t d = 1; d < 8; d <<= 1) {
-                const uint32_t n = __shfl_up_sync(0xffu << seg0, inc, d, 8);
+            for (uint32_t d = 1; d < G; d <<= 1) {
+                const uint32_t n = __shfl_up_sync(cmask, inc, d, G);
                 if (t >= d) inc += n;
             }
             ot = o + inc - L;
             exists = ot < col_bytes;
             const uint32_t off = lit ? 0u : v >> 5;
-            if (exists && code == ST_OK) {
-                if (pos + (lit ? 0u : 1u) >= len || (!lit && (off == 0 || off > ot))) code = ST_CORRUPT;
-                else if (ot + L > col_bytes) code = ST_OVERRUN;
+            if (exists) {
+                if (rdg >= len || pos + (lit ? 0u : 1u) >= len || (!lit && (off == 0 || off > ot)))
+                    code = ST_CORRUPT;
+                else if (ot + L > col_bytes)
+                    code = ST_OVERRUN;
             }
             src = ot - off;
-            // the first bad token of the group decides the column's status
-            const uint32_t bad = __ballot_sync(0xffu << seg0, code != ST_OK) >> seg0;
+            // the first bad token of the step decides the column's status
+            const uint32_t bad = __ballot_sync(cmask, code != ST_OK) >> seg0;
             if (bad) {
-                err = __shfl_sync(0xffu << seg0, code, seg0 + __ffs(bad) - 1u);
+                err = __shfl_sync(cmask, code, seg0 + __ffs(bad) - 1u);
             } else {
-                const uint32_t total = __shfl_sync(0xffu << seg0, inc, seg0 + 7u);
+                const uint32_t total = __shfl_sync(cmask, inc, seg0 + G - 1u);
                 o = min(o + total, col_bytes);
-                rd += 17u - __popc(flag);
+                rd = NGRP == 2 ? rd1 + 17u - __popc(f1) : rd1;
             }
             if (err != ST_OK) exists = false;
         }
@@ -518,7 +537,7 @@ static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __res
         }
         // pass 2: the rest in token order, byte by byte
         if (__any_sync(GD_FULL_MASK, dep)) {
-            for (uint32_t tt = 0; tt < 8; ++tt) {
+            for (uint32_t tt = 0; tt < G; ++tt) {
                 __syncwarp();
                 if (dep && t == tt)
                     for (uint32_t j = 0; j < L; ++j) col[ot + j] = col[src + j];
@@ -534,7 +553,7 @@ static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __res
         // row k of the chunk = word k of columns 0..31
         const uint32_t rows = col_bytes / 4u;
         uint32_t* o32 = reinterpret_cast<uint32_t*>(cout);
-        for (uint32_t k = wid; k < rows; k += 8)
+        for (uint32_t k = wid; k < rows; k += NWARPS)
             o32[32u * k + lane] = *reinterpret_cast<const uint32_t*>(stage + lane * cstr + 4u * k);
     }
     return e;

@@ -266,11 +266,13 @@ typedef enum gd_tune_key {
     GD_TUNE_BRLE_BLOCKS_PER_SM = 1,   /* byte-RLE grid = value x SMs blocks (default 8) */
     GD_TUNE_RLEV1_LANES_PER_BLOCK = 2, /* 0/8: 8 lane streams per block; 4: 4 */
     GD_TUNE_RLEV2_LANES_PER_BLOCK = 3, /* 0/4: 4 lane streams per block; 8: 8 */
-    GD_TUNE_LZSS_WARPS_PER_BLOCK = 4,  /* 0: one chunk per 8-warp block, 8 lanes per column, output
-                                          staged in shared memory; 1: one chunk per warp, one lane per
-                                          column, output staged; 2 / 4 / 8: that many chunks (warps)
-                                          per block, output written as decoded (also the path for
-                                          chunks too large to stage, > 200 KiB) */
+    GD_TUNE_LZSS_WARPS_PER_BLOCK = 4,  /* 0 / 512: one chunk per 512-thread block, 16 lanes per
+                                          column (two flag groups per step), output staged in shared
+                                          memory; 256: 8 lanes per column (one group per step);
+                                          1: one chunk per warp, one lane per column, output staged;
+                                          2 / 4 / 8: that many chunks (warps) per block, output
+                                          written as decoded (also the path for chunks too large to
+                                          stage, > 200 KiB) */
     GD_TUNE_COUNT = 5
 } gd_tune_key_t;
 
