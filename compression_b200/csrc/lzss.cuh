@@ -479,14 +479,25 @@ static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __res
         const uint32_t o0 = o;  // the group's first output byte
         bool exists = false;
         if (act) {
-            // flag byte of each group of the step (the second follows the
-            // first group's 8 tokens: 17 - popc(flag) bytes after it)
-            const uint32_t f0 = rb(rd);
-            const uint32_t rd1 = rd + 17u - __popc(f0);
-            const uint32_t f1 = NGRP == 2 ? rb(rd1) : 0u;
+            // flag byte of each group of the step (each follows the previous
+            // group's 8 tokens: 17 - popc(flag) bytes after its flag byte)
+            uint32_t rds[NGRP], fs[NGRP];
+            rds[0] = rd;
+            fs[0] = rb(rd);
+#pragma unroll
+            for (uint32_t gq = 1; gq < NGRP; ++gq) {
+                rds[gq] = rds[gq - 1] + 17u - __popc(fs[gq - 1]);
+                fs[gq] = rb(rds[gq]);
+            }
             const uint32_t gi = t >> 3, tb = t & 7u;
-            const uint32_t rdg = gi ? rd1 : rd;
-            flag = gi ? f1 : f0;
+            uint32_t rdg = rds[0];
+            flag = fs[0];
+#pragma unroll
+            for (uint32_t gq = 1; gq < NGRP; ++gq)
+                if (gi == gq) {
+                    rdg = rds[gq];
+                    flag = fs[gq];
+                }
             lit = (flag >> tb) & 1u;
             const uint32_t pos = rdg + 1u + tb + __popc(~flag & ((1u << tb) - 1u));
             b0 = rb(pos);
@@ -515,7 +526,7 @@ static __device__ __forceinline__ uint32_t chunk_block_cols(const uint8_t* __res
             } else {
                 const uint32_t total = __shfl_sync(cmask, inc, seg0 + G - 1u);
                 o = min(o + total, col_bytes);
-                rd = NGRP == 2 ? rd1 + 17u - __popc(f1) : rd1;
+                rd = rds[NGRP - 1] + 17u - __popc(fs[NGRP - 1]);
             }
             if (err != ST_OK) exists = false;
         }
