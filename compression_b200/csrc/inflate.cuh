@@ -774,84 +774,92 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                 // Literals accumulate in a run that becomes one command when a
                 // copy or the end of the batch closes it.
                 uint32_t run = 0, run_start = nl;
-                // fast loop while at least 16 input bytes are buffered: the bit
-                // buffer is topped up 32 bits at a time from two ring words,
-                // codes of <= LBITS bits decode with one lookup, the output
-                // bound is checked once per batch (below), and anything else
-                // (long codes, invalid entries) falls to the checked loop
+                // fast loop while enough input is buffered: the bit buffer is
+                // topped up from one aligned ring word at a time, codes of
+                // <= LBITS bits decode with one lookup (a literal entry is any
+                // nonzero value below 2^24), rounds of symbols run without
+                // per-symbol capacity checks (a symbol reads <= 6 input bytes
+                // and adds <= 2 commands and <= 1 literal), the output bound
+                // is checked once per batch (below), and anything else --
+                // long codes, end of block, invalid entries -- falls to the
+                // checked loop with the bit state untouched
                 {
                     const uint32_t* r32 = reinterpret_cast<const uint32_t*>(S.ring);
                     constexpr uint32_t RW = RB / 4 - 1;
-                    auto top32 = [&]() {
-                        if (bitcnt <= 32) {
-                            const uint32_t k = inpos >> 2;
-                            const uint32_t w = __funnelshift_r(r32[k & RW], r32[(k + 1) & RW], (inpos & 3u) * 8u);
-                            bitbuf |= (uint64_t)w << bitcnt;
-                            bitcnt += 32;
-                            inpos += 4;
-                        }
-                    };
-                    while (nc < NC - 2 && nl < NL && fill - inpos >= 16) {
-                        top32();
-                        const uint32_t e = S.lit.lut[(uint32_t)bitbuf & ((1u << LBITS) - 1u)];
-                        const uint32_t L = e & 15u;
-                        if (L == 0 || e == 0xffffffffu) break;  // long code / bad entry: checked loop
-                        const uint32_t kind = e >> 24;
-                        if (kind == E_LIT) {
-                            bitbuf >>= L;
-                            bitcnt -= L;
-                            if (run == 0) run_start = nl;
-                            BT.lits[nl++] = (uint8_t)(e >> 8);
-                            ++run;
-                            ++opos;
-                            continue;
-                        }
-                        if (kind != E_LEN) break;  // end of block / bad symbol: checked loop
-                        // length: its extra bits are in the buffer (>= 33 - 10 bits left)
-                        const uint32_t ex = (e >> 4) & 15u;
-                        const uint64_t b1 = bitbuf >> L;
-                        const uint32_t len = ((e >> 8) & 0xffffu) + ((uint32_t)b1 & ((1u << ex) - 1u));
-                        uint64_t b2 = b1 >> ex;
-                        uint32_t c2 = bitcnt - L - ex;
-                        if (c2 <= 32) {
-                            const uint32_t k = inpos >> 2;
-                            const uint32_t w = __funnelshift_r(r32[k & RW], r32[(k + 1) & RW], (inpos & 3u) * 8u);
-                            b2 |= (uint64_t)w << c2;
-                            c2 += 32;
-                            inpos += 4;
-                        }
-                        const uint32_t ed = S.dist.lut[(uint32_t)b2 & ((1u << DB) - 1u)];
-                        const uint32_t Ld = ed & 15u;
-                        if (Ld == 0 || (ed >> 24) != E_DIST) {
-                            // long or bad distance code: undo to the length symbol
-                            // (bits re-read by the checked loop)
-                            if (c2 != bitcnt - L - ex) {
-                                inpos -= 4;
-                            }
-                            break;
-                        }
-                        const uint32_t exd = (ed >> 4) & 15u;
-                        const uint64_t b3 = b2 >> Ld;
-                        const uint32_t dist = ((ed >> 8) & 0xffffu) + ((uint32_t)b3 & ((1u << exd) - 1u));
-                        if (dist > opos) {
-                            err = ST_CORRUPT;
-                            break;
-                        }
-                        bitbuf = b3 >> exd;
-                        bitcnt = c2 - Ld - exd;
-                        if (run) {
-                            BT.cmd_t[nc] = C_LIT;
-                            BT.cmd_a[nc] = run_start;
-                            BT.cmd_b[nc] = run;
-                            ++nc;
-                            run = 0;
-                        }
-                        BT.cmd_t[nc] = C_COPY;
-                        BT.cmd_a[nc] = dist;
-                        BT.cmd_b[nc] = len;
-                        ++nc;
-                        opos += len;
+                    // align the next ring load to a word
+                    while ((inpos & 3u) && bitcnt <= 56 && fill - inpos >= 16) {
+                        bitbuf |= (uint64_t)S.ring[inpos & (RB - 1)] << bitcnt;
+                        ++inpos;
+                        bitcnt += 8;
                     }
+                    bool fall = (inpos & 3u) != 0;
+                    while (!fall && err == ST_OK) {
+                        uint32_t budget = min((NC - 2 - nc) / 2, NL - nl);
+                        budget = min(budget, fill - inpos >= 24 ? (fill - inpos - 16) / 6 : 0u);
+                        if (budget == 0) break;
+                        for (; budget; --budget) {
+                            if (bitcnt <= 32) {
+                                bitbuf |= (uint64_t)r32[(inpos >> 2) & RW] << bitcnt;
+                                bitcnt += 32;
+                                inpos += 4;
+                            }
+                            const uint32_t e = S.lit.lut[(uint32_t)bitbuf & ((1u << LBITS) - 1u)];
+                            if (e - 1u < 0xffffffu) {  // literal
+                                const uint32_t L = e & 15u;
+                                bitbuf >>= L;
+                                bitcnt -= L;
+                                BT.lits[nl++] = (uint8_t)(e >> 8);
+                                ++run;
+                                ++opos;
+                                continue;
+                            }
+                            const uint32_t L = e & 15u;
+                            if ((e >> 24) != E_LEN || L == 0) {  // walk / end of block / bad: checked loop
+                                fall = true;
+                                break;
+                            }
+                            // length: its extra bits are in the buffer (>= 33 - 10 bits left)
+                            const uint32_t ex = (e >> 4) & 15u;
+                            const uint64_t b1 = bitbuf >> L;
+                            const uint32_t len = ((e >> 8) & 0xffffu) + ((uint32_t)b1 & ((1u << ex) - 1u));
+                            uint64_t b2 = b1 >> ex;
+                            uint32_t c2 = bitcnt - L - ex;
+                            const bool top = c2 <= 32;
+                            if (top) {
+                                b2 |= (uint64_t)r32[(inpos >> 2) & RW] << c2;
+                                c2 += 32;
+                            }
+                            const uint32_t ed = S.dist.lut[(uint32_t)b2 & ((1u << DB) - 1u)];
+                            const uint32_t Ld = ed & 15u;
+                            if (Ld == 0 || (ed >> 24) != E_DIST) {  // long / bad distance code: checked loop
+                                fall = true;
+                                break;
+                            }
+                            if (top) inpos += 4;
+                            const uint32_t exd = (ed >> 4) & 15u;
+                            const uint64_t b3 = b2 >> Ld;
+                            const uint32_t dist = ((ed >> 8) & 0xffffu) + ((uint32_t)b3 & ((1u << exd) - 1u));
+                            if (dist > opos) {
+                                err = ST_CORRUPT;
+                                break;
+                            }
+                            bitbuf = b3 >> exd;
+                            bitcnt = c2 - Ld - exd;
+                            if (run) {
+                                BT.cmd_t[nc] = C_LIT;
+                                BT.cmd_a[nc] = nl - run;
+                                BT.cmd_b[nc] = run;
+                                ++nc;
+                                run = 0;
+                            }
+                            BT.cmd_t[nc] = C_COPY;
+                            BT.cmd_a[nc] = dist;
+                            BT.cmd_b[nc] = len;
+                            ++nc;
+                            opos += len;
+                        }
+                    }
+                    run_start = nl - run;  // the open literal run, for the checked loop
                 }
                 while (err == ST_OK && nc < NC - 2 && nl < NL && (fill - inpos >= 32 || fill >= span)) {
                     uint32_t e;
