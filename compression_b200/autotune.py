@@ -7,7 +7,8 @@ are compiled into libgd.so or sets a launch shape:
                                           3: one warp per stream with a 32 KiB window
                                           4, 5: decoder + writer pair, no window, 2 / 4 per block
                                           6: decoder + writer pair with the window
-                                          0: 4 for >= 4 streams per SM, else 6
+                                          7-13: pairs with a 16 / 8 / 4 KiB window, smaller buffers
+                                          0: 12 for >= 4 streams per SM, else 6
   brle     GD_TUNE_BRLE_BLOCKS_PER_SM     grid = value x SMs
   rlev1    GD_TUNE_RLEV1_LANES_PER_BLOCK  lane streams (warps) per block
   rlev2    GD_TUNE_RLEV2_LANES_PER_BLOCK  lane streams (warps) per block
@@ -46,7 +47,7 @@ TUNE_LZSS_WARPS_PER_BLOCK = 4
 
 # codec -> (knob, candidate values; the first is the built-in default)
 KNOBS = {
-    "deflate": (TUNE_INFLATE_VARIANT, [0, 6, 4, 1]),
+    "deflate": (TUNE_INFLATE_VARIANT, [0, 6, 12, 10, 4]),
     "brle": (TUNE_BRLE_BLOCKS_PER_SM, [8, 4, 16]),
     "rlev1": (TUNE_RLEV1_LANES_PER_BLOCK, [8, 4]),
     "rlev2": (TUNE_RLEV2_LANES_PER_BLOCK, [4, 8]),

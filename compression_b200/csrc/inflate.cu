@@ -69,15 +69,17 @@ __global__ void __launch_bounds__(NW * 32) inflate_kernel(Chunks ch, uint32_t n_
 
 // Reader/writer pairs: NP pairs per block, warps 2i (decoder) and 2i+1
 // (writer) share stream i's state and hand batches over through it.
-template <class Chunks, uint32_t WIN, int NP>
+template <class Chunks, uint32_t WIN, int NP, uint32_t RB = IRING, uint32_t DB = LBITS, uint32_t NL = NLIT,
+          uint32_t NC = NCMD>
 __global__ void __launch_bounds__(NP * 64) inflate_pair_kernel(Chunks ch, uint32_t n_chunks, int zlib_hdr,
                                                               const uint32_t* __restrict__ order) {
+    using SmemT = WarpSmemT<WIN, 2, RB, DB, NL, NC>;
     extern __shared__ __align__(16) uint8_t smem_raw[];
     const uint32_t wid = threadIdx.x >> 5, pair = wid >> 1;
     const uint32_t slot = blockIdx.x * NP + pair;
     if (slot >= n_chunks) return;  // both warps of the pair leave together
     const uint32_t chunk = order ? order[slot] : slot;
-    WarpSmemT<WIN, 2>& S = *reinterpret_cast<WarpSmemT<WIN, 2>*>(smem_raw + pair * sizeof(WarpSmemT<WIN, 2>));
+    SmemT& S = *reinterpret_cast<SmemT*>(smem_raw + pair * sizeof(SmemT));
     const uint8_t* src;
     uint8_t* dst;
     uint64_t clen64, olen64;
@@ -95,12 +97,12 @@ __global__ void __launch_bounds__(NP * 64) inflate_pair_kernel(Chunks ch, uint32
     // the pair's 64 threads, reached unconditionally by both warps
     asm volatile("bar.sync %0, 64;" ::"r"(1u + pair) : "memory");
     if (wid & 1u) {
-        const uint32_t werr = stream_pair_writer<WIN>(S, src, dst);
+        const uint32_t werr = stream_pair_writer<WIN, RB, DB, NL, NC>(S, src, dst);
         if (werr != ST_OK && lane_id() == 0) ch.put(chunk, werr, 0);
         return;
     }
     uint32_t fin = 0;
-    err = stream_warp_impl<WIN, 2>(src, (uint32_t)clen64, dst, (uint32_t)olen64, zlib_hdr, S, &fin);
+    err = stream_warp_impl<WIN, 2, RB, DB, NL, NC>(src, (uint32_t)clen64, dst, (uint32_t)olen64, zlib_hdr, S, &fin);
     if (err == ST_OK && Chunks::exact && fin != (uint32_t)olen64) err = ST_CORRUPT;
     if (lane_id() == 0) ch.put(chunk, err, err == ST_OK ? fin : 0);
 }
@@ -134,19 +136,20 @@ gd_status_t launch_cfg(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32_
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
 }
 
-template <class Chunks, uint32_t WIN, int NP>
+template <class Chunks, uint32_t WIN, int NP, uint32_t RB = gd::infl::IRING, uint32_t DB = gd::infl::LBITS,
+          uint32_t NL = gd::infl::NLIT, uint32_t NC = gd::infl::NCMD>
 gd_status_t launch_pair(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32_t* order, cudaStream_t s) {
     using namespace gd::infl;
-    const uint32_t smem = NP * (uint32_t)sizeof(WarpSmemT<WIN, 2>);
+    const uint32_t smem = NP * (uint32_t)sizeof(WarpSmemT<WIN, 2, RB, DB, NL, NC>);
+    auto kern = inflate_pair_kernel<Chunks, WIN, NP, RB, DB, NL, NC>;
     static bool attr_set = false;  // benign race: the attribute call is idempotent
     if (!attr_set) {
-        if (cudaFuncSetAttribute(inflate_pair_kernel<Chunks, WIN, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 smem) != cudaSuccess)
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
             return GD_ERR_CUDA;
         attr_set = true;
     }
     const uint32_t grid = (n + NP - 1) / NP;
-    inflate_pair_kernel<Chunks, WIN, NP><<<grid, NP * 64, smem, s>>>(ch, n, zlib_hdr, order);
+    kern<<<grid, NP * 64, smem, s>>>(ch, n, zlib_hdr, order);
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
 }
 
@@ -154,8 +157,10 @@ gd_status_t launch_pair(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32
 // stream without a window, 2 / 4 warps per block; 3 = one warp per stream
 // with a window; 4 / 5 = decoder/writer warp pairs without a window (copies
 // read the output), 2 / 4 pairs per block; 6 = one decoder/writer pair per
-// block with a 32 KiB shared window; 0 (default) = 4 for at least 4 streams
-// per SM, else 6.
+// block with a 32 KiB shared window; 7 - 13 = pairs with a 16 / 8 / 4 KiB
+// window (nearer copies from shared memory, farther ones from the output)
+// and smaller rings, distance tables and batches, so that 7 to 15 pairs fit
+// on an SM; 0 (default) = 12 for at least 4 streams per SM, else 6.
 template <class Chunks>
 gd_status_t launch_inflate(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32_t* order, cudaStream_t s) {
     int v = gd_tune_get(GD_TUNE_INFLATE_VARIANT);
@@ -165,7 +170,7 @@ gd_status_t launch_inflate(const Chunks& ch, uint32_t n, int zlib_hdr, const uin
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        v = n >= 4u * (uint32_t)sms ? 4 : 6;
+        v = n >= 4u * (uint32_t)sms ? 12 : 6;
     }
     switch (v) {
         case 1: return launch_cfg<Chunks, 0, 2>(ch, n, zlib_hdr, order, s);
@@ -173,6 +178,13 @@ gd_status_t launch_inflate(const Chunks& ch, uint32_t n, int zlib_hdr, const uin
         case 3: return launch_cfg<Chunks, 32768, 1>(ch, n, zlib_hdr, order, s);
         case 4: return launch_pair<Chunks, 0, 2>(ch, n, zlib_hdr, order, s);
         case 5: return launch_pair<Chunks, 0, 4>(ch, n, zlib_hdr, order, s);
+        case 7: return launch_pair<Chunks, 16384, 1, 2048, 8, 1024, 128>(ch, n, zlib_hdr, order, s);
+        case 8: return launch_pair<Chunks, 16384, 2, 2048, 8, 1024, 128>(ch, n, zlib_hdr, order, s);
+        case 9: return launch_pair<Chunks, 8192, 1, 2048, 8, 1024, 128>(ch, n, zlib_hdr, order, s);
+        case 10: return launch_pair<Chunks, 4096, 1, 2048, 8, 1024, 128>(ch, n, zlib_hdr, order, s);
+        case 11: return launch_pair<Chunks, 8192, 1, 1024, 8, 512, 64>(ch, n, zlib_hdr, order, s);
+        case 12: return launch_pair<Chunks, 4096, 1, 1024, 8, 512, 64>(ch, n, zlib_hdr, order, s);
+        case 13: return launch_pair<Chunks, 4096, 2, 1024, 8, 512, 64>(ch, n, zlib_hdr, order, s);
         default: return launch_pair<Chunks, 32768, 1>(ch, n, zlib_hdr, order, s);
     }
 }

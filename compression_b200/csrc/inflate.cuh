@@ -71,10 +71,10 @@ struct BatchT {
 using Batch = BatchT<NLIT, NCMD>;
 
 // Per-stream shared state.  WIN > 0: the last WIN output bytes are kept in a
-// shared-memory window (WIN a power of two >= 32768, the Deflate window), so
-// back-references never read global memory; WIN = 0: copies read the output
-// already written to global memory (a smaller footprint, for kernels that
-// run other decoders beside this one).  NB = 1: one warp decodes and
+// shared-memory window (a power of two; with 32768, the Deflate window, no
+// back-reference reads global memory, with less only the farther ones do);
+// WIN = 0: copies read the output already written to global memory (a
+// smaller footprint, for kernels that run other decoders beside this one).  NB = 1: one warp decodes and
 // executes; NB = 2: a decoder warp fills batch k+1 while a writer warp
 // executes batch k.
 // RB: input ring bytes; DB: distance lookup bits; NL / NC: literal bytes and
@@ -235,6 +235,28 @@ static __device__ __forceinline__ void execute_batch(const BatchType& B, uint32_
                     const uint8_t v = s[k];
                     d[k] = v;
                     win[(pos + k) & M] = v;
+                }
+            } else if (WIN < 32768u && a > WIN) {
+                // a window smaller than the Deflate window: farther sources
+                // are read from the output (written long before this wave)
+                const uint8_t* s = d - a;
+                for (uint32_t k0 = 0; k0 < n; k0 += 128) {
+                    uint8_t v[4];
+#pragma unroll
+                    for (uint32_t i = 0; i < 4; ++i) {
+                        const uint32_t k = k0 + lane + 32u * i;
+                        v[i] = k < n ? s[k] : (uint8_t)0;
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (uint32_t i = 0; i < 4; ++i) {
+                        const uint32_t k = k0 + lane + 32u * i;
+                        if (k < n) {
+                            d[k] = v[i];
+                            win[(pos + k) & M] = v[i];
+                        }
+                    }
+                    __syncwarp();
                 }
             } else if (a >= 128) {
                 // 128-byte waves (four bytes a lane): with distance >= 128 a
@@ -433,7 +455,9 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
                                                             uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
                                                             WarpSmemT<WIN, NB, RB, DB, NL, NC>& S, uint32_t* written) {
     static_assert(RB >= 1024 && (RB & (RB - 1)) == 0, "input ring: a power of two >= 1 KiB");
-    static_assert(WIN == 0 || (WIN >= 32768 && (WIN & (WIN - 1)) == 0), "window: 0 or a power of two >= 32 KiB");
+    // a window below the Deflate window's 32 KiB serves the nearer copies;
+    // the executor reads farther ones from the output
+    static_assert(WIN == 0 || (WIN >= 4096 && (WIN & (WIN - 1)) == 0), "window: 0 or a power of two >= 4 KiB");
     const uint32_t lane = lane_id();
     uint32_t err = ST_OK;
     // input ring: compressed byte i (chunk-relative) at ring[(i + sh) % RB];
@@ -984,8 +1008,9 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
 // stream_warp_impl<WIN, 2> on the same S) decodes batch k+1.  The decoder's
 // last hand-off is an empty batch marked last (also after an error).
 // Returns GD_ERR_TIMEOUT if a wait expired, else OK.
-template <uint32_t WIN>
-static __device__ __forceinline__ uint32_t stream_pair_writer(WarpSmemT<WIN, 2>& S, const uint8_t* __restrict__ src,
+template <uint32_t WIN, uint32_t RB = IRING, uint32_t DB = LBITS, uint32_t NL = NLIT, uint32_t NC = NCMD>
+static __device__ __forceinline__ uint32_t stream_pair_writer(WarpSmemT<WIN, 2, RB, DB, NL, NC>& S,
+                                                              const uint8_t* __restrict__ src,
                                                               uint8_t* __restrict__ dst) {
     for (uint32_t kb = 0;; ++kb) {
         if (!pair_wait(&S.produced, kb + 1)) return ST_TIMEOUT;

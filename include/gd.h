@@ -262,7 +262,12 @@ typedef enum gd_tune_key {
                                     4 / 5: decoder + writer warp pair per stream, no window
                                     (copies read the output), 2 / 4 pairs per block;
                                     6: decoder + writer pair with the window, one per block;
-                                    0 (default): 4 for >= 4 streams per SM, else 6 */
+                                    7 / 8: pairs with a 16 KiB window, 1 / 2 per block;
+                                    9 / 10: 8 / 4 KiB window; 11 / 12: 8 / 4 KiB window with a
+                                    1 KiB ring and batches of 512 literals / 64 commands;
+                                    13: as 12, 2 pairs per block (copies beyond the window
+                                    read the output);
+                                    0 (default): 12 for >= 4 streams per SM, else 6 */
     GD_TUNE_BRLE_BLOCKS_PER_SM = 1,   /* byte-RLE grid = value x SMs blocks (default 8) */
     GD_TUNE_RLEV1_LANES_PER_BLOCK = 2, /* 0/8: 8 lane streams per block; 4: 4 */
     GD_TUNE_RLEV2_LANES_PER_BLOCK = 3, /* 0/4: 4 lane streams per block; 8: 8 */
