@@ -20,11 +20,12 @@ namespace gd {
 namespace batch {
 
 constexpr int WPB = 4;  // warps per block
-// Deflate workspace of a batch warp: no window, a 1 KiB input ring, an 8-bit
-// distance table and batches of 1024 literals / 128 commands (the standalone
-// kernels use 8 KiB, 10 bits, 2048 / 256); the largest codec workspace sets
-// every warp's, so it is kept small for occupancy.
-using BatchInflSmem = infl::WarpSmemT<0, 1, 1024, 8, 1024, 128>;
+// Deflate workspace of a batch warp: a 4 KiB output window (nearer copies
+// from shared memory, farther ones from the output), a 1 KiB input ring, an
+// 8-bit distance table and batches of 512 literals / 64 commands (the
+// standalone kernels use up to 32 KiB, 8 KiB, 10 bits, 2048 / 256); the
+// largest codec workspace sets every warp's, so it is kept small.
+using BatchInflSmem = infl::WarpSmemT<4096, 1, 1024, 8, 512, 64>;
 
 __host__ __device__ constexpr uint32_t warp_smem_bytes(uint32_t max_lane) {
     // union of the per-codec warp workspaces
@@ -115,7 +116,7 @@ __device__ uint32_t run_task(const gd_task& t, uint32_t max_lane, uint8_t* ws) {
         case GD_CODEC_DEFLATE: {
             if (t.src_len > 0xffffffffull || t.dst_len > 0xffffffffull) return ST_INVALID;
             uint32_t fin = 0;
-            const uint32_t e = infl::stream_warp<0, 1024, 8, 1024, 128>(t.src, (uint32_t)t.src_len, t.dst,
+            const uint32_t e = infl::stream_warp<4096, 1024, 8, 512, 64>(t.src, (uint32_t)t.src_len, t.dst,
                                                                      (uint32_t)t.dst_len, (int)t.param,
                                                                      *reinterpret_cast<BatchInflSmem*>(ws), &fin);
             return (e == ST_OK && fin != (uint32_t)t.dst_len) ? (uint32_t)ST_CORRUPT : e;
