@@ -10,7 +10,8 @@ A step decodes both columns from HBM to HBM.  Synthetic seeded data stands in
 for the reference's datasets, which are not available.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload brle_rlev2|rlev1|lzss|deflate|mixed] [--scale F]
+                    [--workload brle_rlev2|rlev1|lzss|deflate|mixed|rlev1_encode|rlev2_encode]
+                    [--scale F]
 
 Multi-GPU (torchrun, one process per GPU): every rank decodes its own copy of
 the workload (independent chunks, no exchange step), weak scaling, time = max
@@ -681,6 +682,139 @@ def mixed_cpu_sample(items, threads: int, budget_s: float):
 
 
 
+# --------------------------------------------------------------------------
+# device encoders (RLE v1 / RLE v2 containers written on the GPU)
+# --------------------------------------------------------------------------
+
+def encode_column(workload: str, scale: float):
+    """The decode workloads' columns: (codec, raw bytes, encoder kwargs, chunk, label)."""
+    import compression_b200.codecs as cc
+    if workload == "rlev1_encode":
+        v = cc.gen_rlev1_ints(0xA0, int(64 * MiB * scale) // 4)
+        return ("rlev1", v.view(np.uint8), dict(comp_col_len=128, elem_bytes=4), 128 * 1024,
+                f"RLE v1 encode of {64 * scale:g} MiB int32, 128 KiB chunks, COMP_COL_LEN 128")
+    v = cc.gen_rlev2_ints(0xB1, int(256 * MiB * scale) // 8)
+    return ("rlev2", v.view(np.uint8), dict(read_unit=32), 256 * 1024,
+            f"RLE v2 encode of {256 * scale:g} MiB int64, 256 KiB chunks, READ_UNIT 32")
+
+
+def host_encode(codec, raw, chunk, kw):
+    import compression_b200.codecs as cc
+    if codec == "rlev1":
+        return cc.rlev1_encode(raw, chunk, kw["comp_col_len"], kw["elem_bytes"])
+    return cc.rlev2_encode(raw, chunk, kw["read_unit"])
+
+
+def host_encode_rate(codec, raw, chunk, kw, budget_s: float):
+    """The host encoder (one std::thread per core over chunks) on the whole
+    column, repeated for the time budget.  Returns (GB/s of column bytes, reps)."""
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        host_encode(codec, raw, chunk, kw)
+        reps += 1
+        dt = time.perf_counter() - t0
+        if dt >= budget_s:
+            return raw.size * reps / dt / 1e9, reps
+
+
+def run_encode(args, rank, world, local_rank):
+    import torch
+    import compression_b200.codecs as cc
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    codec, raw, kw, chunk, label = encode_column(args.workload, args.scale)
+    host = host_encode(codec, raw, chunk, kw)
+    d_col = torch.from_numpy(raw.copy()).to(dev)
+    stream = torch.cuda.current_stream(dev)
+
+    # parity: the device container is the host encoder's, and decodes back
+    bufs = cc.encode_device(codec, d_col, chunk, **kw)
+    torch.cuda.synchronize()
+    blk = bufs["blk_off"].cpu().numpy().view(np.uint64)
+    size = int(blk[-1])
+    ok = ((bufs["status"].cpu().numpy() == 0).all() and np.array_equal(blk, host.meta["blk_off"])
+          and np.array_equal(bufs["col_len"].cpu().numpy().view(np.uint64), host.meta["col_len"])
+          and np.array_equal(bufs["data"][:size].cpu().numpy(), host.data))
+    if not ok:
+        raise RuntimeError(f"{codec} device encoder differs from the host encoder")
+    job = cc.DeviceJob(host, dev)
+    job.launch()
+    torch.cuda.synchronize()
+    if not ((job.status() == 0).all() and np.array_equal(job.output(), raw)):
+        raise RuntimeError(f"{codec} container does not decode back to the column")
+
+    flush = torch.empty(256 * MiB, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        flush.zero_()
+        cc.encode_device(codec, d_col, chunk, bufs=bufs, **kw)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    K = args.steps
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    with Clocks(local_rank) as clk:
+        for k in range(K):
+            flush.zero_()
+            evs[k][0].record(stream)
+            cc.encode_device(codec, d_col, chunk, bufs=bufs, **kw)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+    ms = max_over_ranks([statistics.mean(a.elapsed_time(b) for a, b in evs)], world, dev)[0]
+    value = job_rate(raw.size, world, ms)
+    nc = blk.size - 1
+    alg = raw.size + size + 8 * (nc + 1) + 8 * 32 * nc  # column in; container, blk_off, col_len out
+    peak, peak_kind = peaks()
+    gbs = alg / (ms / 1e3) / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        h_col = torch.from_numpy(raw.copy()).pin_memory()
+        h_data = torch.empty(bufs["data"].numel(), dtype=torch.uint8).pin_memory()
+        h_meta = torch.empty(nc + 1 + 32 * nc, dtype=torch.int64).pin_memory()
+        d_in = torch.empty_like(d_col)
+
+        def host_call():
+            d_in.copy_(h_col, non_blocking=True)
+            cc.encode_device(codec, d_in, chunk, bufs=bufs, **kw)
+            h_meta[:nc + 1].copy_(bufs["blk_off"], non_blocking=True)
+            h_meta[nc + 1:].copy_(bufs["col_len"], non_blocking=True)
+            torch.cuda.synchronize()
+            n = int(h_meta[nc])
+            h_data[:n].copy_(bufs["data"][:n])
+            return n
+
+        for _ in range(2):
+            host_call()
+        ts = []
+        for _ in range(max(3, min(K, 5))):
+            t0 = time.perf_counter()
+            host_call()
+            ts.append(time.perf_counter() - t0)
+        e2e_s = max_over_ranks([statistics.median(ts)], world, dev)[0]
+        e2e = {"value": round(job_rate(raw.size, world, e2e_s * 1e3), 3), "unit": "GB/s",
+               "h2d_bytes_per_step": int(raw.size), "d2h_bytes_per_step": int(size + 8 * (nc + 1 + 32 * nc)),
+               "path": "pinned column H2D, gd_*_encode_device, container D2H"}
+
+    line = {
+        "metric": f"encoded GB/s ({codec} device encoder, column bytes in)", "value": round(value, 2),
+        "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32" if codec == "rlev1" else "int64", "data": "synthetic (seeded generators)",
+        "config": {"workload": label, "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}", "ratio": round(size / raw.size, 4)},
+        "roofline": {"bound": "hbm", "kernel": f"{codec} encode (lane encode + offsets + interleave)",
+                     "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s", "frac": round(gbs / peak, 4),
+                     "peak_source": peak_kind, "traffic": None, "alg_bytes": alg},
+        "gpu_launches": 3 * K, "step": "one column encoded", "clocks": clk.summary(), "e2e": e2e,
+    }
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        gbs_cpu, reps = host_encode_rate(codec, raw, chunk, kw, 10.0)
+        line["cpu_baseline"] = {"value": round(gbs_cpu, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                                "sample": f"host encoder on the whole column, {reps} passes"}
+    return line
+
+
 def run_reference(args):
     """The reference's own CPU decoders (oracle/_ref, compiled from the
     reference sources) on all host cores; the oracle port for codecs whose
@@ -698,6 +832,16 @@ def run_reference(args):
             gbs, sample = mixed_cpu_sample(items, threads, 4.0)
             vals.append(gbs)
         kind = "port"
+    elif args.workload.endswith("_encode"):
+        codec, raw, kw, chunk, label = encode_column(args.workload, args.scale)
+        cfg = {"workload": label}
+        for _ in range(args.warmup):
+            host_encode_rate(codec, raw, chunk, kw, 0.5)
+        for _ in range(args.steps):
+            gbs, reps = host_encode_rate(codec, raw, chunk, kw, 4.0)
+            vals.append(gbs)
+            sample = f"host encoder on the whole column, {reps} passes"
+        kind = "port"
     else:
         cols, cfg = make_workload(args.workload, args.scale)
         for _ in range(args.warmup):
@@ -706,8 +850,10 @@ def run_reference(args):
             gbs, sample, kind, prep = ref_decode_sample(cols, threads, budget_s=4.0, prepared=prep)
             vals.append(gbs)
     v = statistics.median(vals)
-    return {"impl": "reference", "metric": "decompressed GB/s (byte-RLE + RLE v2 columns)"
-            if args.workload == "brle_rlev2" else f"decompressed GB/s ({args.workload})",
+    metric = ("decompressed GB/s (byte-RLE + RLE v2 columns)" if args.workload == "brle_rlev2"
+              else f"encoded GB/s ({args.workload[:5]} device encoder, column bytes in)"
+              if args.workload.endswith("_encode") else f"decompressed GB/s ({args.workload})")
+    return {"impl": "reference", "metric": metric,
             "value": round(v, 3), "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": None, "higher_is_better": True, "config": cfg,
             "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": kind,
@@ -721,7 +867,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="brle_rlev2", choices=["brle_rlev2", "rlev1", "lzss", "deflate", "mixed"])
+    ap.add_argument("--workload", default="brle_rlev2", choices=["brle_rlev2", "rlev1", "lzss", "deflate", "mixed",
+                                                                 "rlev1_encode", "rlev2_encode"])
     ap.add_argument("--scale", type=float, default=1.0, help="workload size factor (1.0 = full size)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -742,7 +889,12 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    line = run_mixed(args, rank, world, local_rank) if args.workload == "mixed" else run_ours(args, rank, world, local_rank)
+    if args.workload == "mixed":
+        line = run_mixed(args, rank, world, local_rank)
+    elif args.workload.endswith("_encode"):
+        line = run_encode(args, rank, world, local_rank)
+    else:
+        line = run_ours(args, rank, world, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

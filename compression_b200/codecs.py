@@ -234,6 +234,71 @@ def deflate_encode(raw, out_off: np.ndarray, level: int = 6, mode: np.ndarray | 
 
 
 # --------------------------------------------------------------------------
+# device encoders (RLE v1 / RLE v2 containers written on the GPU)
+# --------------------------------------------------------------------------
+
+def encode_device(codec: str, d_col, chunk_size: int, *, comp_col_len: int = 128, elem_bytes: int = 4,
+                  read_unit: int = 32, stream=None, bufs: dict | None = None) -> dict:
+    """Enqueue gd_rlev1_encode_device / gd_rlev2_encode_device on `d_col`, a
+    CUDA uint8 tensor holding the column.  Returns the device tensors
+    {"data", "blk_off", "col_len", "status", "scratch"}; "data" is sized to
+    the bound and the container's length is blk_off[-1].  `bufs` (a previous
+    return value) reuses its buffers."""
+    import torch
+    n = int(d_col.numel())
+    L = lib()
+    if codec == "rlev1":
+        bound = L.gd_rlev1_encode_bound(n, chunk_size, elem_bytes)
+    elif codec == "rlev2":
+        bound = L.gd_rlev2_encode_bound(n, chunk_size)
+    else:
+        raise ValueError(f"no device encoder for {codec}")
+    if bound == 0:
+        raise ValueError("bad encoder arguments")
+    nc = (n + chunk_size - 1) // chunk_size
+    dev = d_col.device
+    if bufs is None or bufs["data"].numel() < bound or bufs["blk_off"].numel() != nc + 1:
+        bufs = {"scratch": torch.empty(bound, dtype=torch.uint8, device=dev),
+                "data": torch.empty(bound, dtype=torch.uint8, device=dev),
+                "blk_off": torch.empty(nc + 1, dtype=torch.int64, device=dev),
+                "col_len": torch.empty(32 * nc, dtype=torch.int64, device=dev),
+                "status": torch.empty(nc, dtype=torch.int32, device=dev)}
+    s = (stream or torch.cuda.current_stream()).cuda_stream
+    p = lambda t: C.c_void_p(t.data_ptr())
+    if codec == "rlev1":
+        rc = L.gd_rlev1_encode_device(p(d_col), n, chunk_size, comp_col_len, elem_bytes, p(bufs["scratch"]),
+                                      p(bufs["data"]), p(bufs["blk_off"]), p(bufs["col_len"]), p(bufs["status"]),
+                                      C.c_void_p(s))
+    else:
+        rc = L.gd_rlev2_encode_device(p(d_col), n, chunk_size, read_unit, p(bufs["scratch"]), p(bufs["data"]),
+                                      p(bufs["blk_off"]), p(bufs["col_len"]), p(bufs["status"]), C.c_void_p(s))
+    check(rc, f"gd_{codec}_encode_device")
+    return bufs
+
+
+def encode_gpu(codec: str, raw, chunk_size: int, *, comp_col_len: int = 128, elem_bytes: int = 4,
+               read_unit: int = 32) -> Encoded:
+    """The device encoder from host memory: the same Encoded as rlev1_encode /
+    rlev2_encode (rle_v1::compress_gpu, include/rle_v1/rlev1.h:25-97;
+    rlev2::compress_gpu_transpose, include/rlev2/encoder_trans.h:428-537)."""
+    import torch
+    b = _as_u8(raw)
+    d = torch.from_numpy(b.copy()).cuda()
+    r = encode_device(codec, d, chunk_size, comp_col_len=comp_col_len, elem_bytes=elem_bytes, read_unit=read_unit)
+    torch.cuda.synchronize()
+    st = r["status"].cpu().numpy()
+    if (st != 0).any():
+        raise DecodeError(int(st[st != 0][0]), f"gd_{codec}_encode_device")
+    blk = r["blk_off"].cpu().numpy().view(np.uint64)
+    col = r["col_len"].cpu().numpy().view(np.uint64)
+    data = r["data"][:int(blk[-1])].cpu().numpy()
+    nc = blk.size - 1
+    params = ({"comp_col_len": comp_col_len, "elem_bytes": elem_bytes} if codec == "rlev1"
+              else {"read_unit": read_unit})
+    return Encoded(codec, data, b.size, nc, chunk_size, {"blk_off": blk, "col_len": col}, params)
+
+
+# --------------------------------------------------------------------------
 # device jobs
 # --------------------------------------------------------------------------
 

@@ -388,6 +388,31 @@ uint64_t gd_rlev2_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uin
 /* rlev2::block_encode on one stream (include/rlev2/encoder.h:795-969). */
 uint64_t gd_rlev2_encode_stream(const int64_t* vals, uint64_t n, uint8_t* out, uint64_t cap);
 
+/* ------------------------------------------------------------------------
+ * Device encoders (sm_100a) for the RLE v1 and RLE v2 containers: the same
+ * bytes as gd_rlev1_encode / gd_rlev2_encode, written from a column already
+ * in device memory.  Asynchronous on `stream`.
+ *
+ * d_scratch and d_data each hold gd_*_encode_bound(n_bytes, ...) bytes (4-byte
+ * aligned); d_blk_off holds n_chunks + 1 and d_col_len 32 * n_chunks values;
+ * d_status (optional) n_chunks words (GD_ERR_OVERRUN if a lane outgrew its
+ * scratch slot, which the bound rules out).  The encoded size is
+ * d_blk_off[n_chunks].  n_bytes must be a multiple of the value size and
+ * d_in aligned to it; the last chunk is zero-padded as the host encoders do.
+ * ------------------------------------------------------------------------ */
+/* rle_v1::compress_gpu (include/rle_v1/rlev1.h:25-97); elem_bytes 4 or 8. */
+uint64_t gd_rlev1_encode_bound(uint64_t n_bytes, uint64_t chunk_size, uint32_t elem_bytes);
+gd_status_t gd_rlev1_encode_device(const uint8_t* d_in, uint64_t n_bytes, uint64_t chunk_size,
+                                   uint32_t comp_col_len, uint32_t elem_bytes, uint8_t* d_scratch,
+                                   uint8_t* d_data, uint64_t* d_blk_off, uint64_t* d_col_len,
+                                   uint32_t* d_status, gd_stream_t stream);
+/* rlev2::compress_gpu_transpose (include/rlev2/encoder_trans.h:428-537). */
+uint64_t gd_rlev2_encode_bound(uint64_t n_bytes, uint64_t chunk_size);
+gd_status_t gd_rlev2_encode_device(const uint8_t* d_in, uint64_t n_bytes, uint64_t chunk_size,
+                                   uint32_t read_unit, uint8_t* d_scratch, uint8_t* d_data,
+                                   uint64_t* d_blk_off, uint64_t* d_col_len, uint32_t* d_status,
+                                   gd_stream_t stream);
+
 uint64_t gd_lzss_max_encoded_bytes(uint64_t n, uint64_t chunk_size);
 /* lzss::compress_gpu (include/lzss/lzss_gpu2.h:1915-2127). */
 uint64_t gd_lzss_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* data,

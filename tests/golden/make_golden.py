@@ -33,6 +33,21 @@ def run(*args):
     subprocess.run([str(a) for a in args], check=True, stdout=subprocess.DEVNULL)
 
 
+def negative_constant_run(tmp: Path):
+    """An RLE v2 lane the reference's own encoder writes as a corrupt stream:
+    128 equal negative values reach determineEncoding through the fixed-run
+    path (var_runlen 0), is_safe_subtract's `smaller - INT64_MIN` wraps and
+    calls the run unsafe, and write_direct stores var_runlen - 1 = 0xffff as
+    the length field (a DIRECT run claiming 512 values).  Only the encoder
+    output is stored: the reference decoder would read past its run.  The
+    lane is lane 0 of the last chunk of a 70000-value constant -5 column in
+    256 KiB chunks, READ_UNIT 32 (160 values, then the zero padding)."""
+    lane = np.concatenate([np.full(160, -5, np.int64), np.zeros(864, np.int64)])
+    lane.tofile(tmp / "v")
+    run(REF / "ref_rlev2", "encode", tmp / "v", tmp / "vs")
+    np.savez_compressed(OUT / "rlev2_negconst.npz", raw=lane, enc=np.fromfile(tmp / "vs", np.uint8))
+
+
 def main():
     tmp = Path(tempfile.mkdtemp())
     rng = np.random.default_rng(20261203)
@@ -97,6 +112,8 @@ def main():
     run(REF / "ref_rlev2", "decode", tmp / "vs", lane.size, tmp / "vd")
     np.savez_compressed(OUT / "rlev2_quirk.npz", raw=lane, enc=np.fromfile(tmp / "vs", np.uint8),
                         dec=np.fromfile(tmp / "vd", np.int64))
+
+    negative_constant_run(tmp)
 
     # ---- Deflate chunks (Python zlib, level 6 / 9 as orig_compressor.py) ----
     dz = {}

@@ -33,6 +33,16 @@ def test_device_api_rejects_bad_arguments_without_gpu():
     assert L.gd_rlev2_decode(1, 1, 1, 1, 256 * 1024, 0, 1, 10, 0, None, None) == 5
     assert L.gd_lzss_decode(1, 1, 1, 1, 2, 65536, 16, 1000, None, None) == 1  # out != n*chunk
     assert L.gd_inflate(3, 1, 1, 1, 1, 1, 1, None, None) == 1  # unaligned data
+    # device encoders: partial values, chunk not a multiple of 32 slices, unaligned input
+    assert L.gd_rlev1_encode_device(4, 999, 4096, 128, 4, 4, 4, 8, 8, None, None) == 1
+    assert L.gd_rlev1_encode_device(4, 1000, 4000, 128, 4, 4, 4, 8, 8, None, None) == 1
+    assert L.gd_rlev1_encode_device(2, 1000, 4096, 128, 4, 4, 4, 8, 8, None, None) == 1
+    assert L.gd_rlev2_encode_device(8, 996, 8192, 1, 4, 4, 8, 8, None, None) == 1
+    assert L.gd_rlev2_encode_device(8, 1000, 8192, 3, 4, 4, 8, 8, None, None) == 1
+    assert L.gd_rlev1_encode_device(None, 0, 4096, 128, 4, None, None, None, None, None, None) == 0  # empty
+    # bounds: 32 lane slots per chunk, each holding the longest lane stream
+    assert L.gd_rlev1_encode_bound(128 * 1024, 128 * 1024, 4) == 32 * ((1024 * 5 + 1024 // 64 + 16 + 3) & ~3)
+    assert L.gd_rlev2_encode_bound(2 * 256 * 1024, 256 * 1024) == 2 * 32 * ((1024 * 11 + 64 + 3) & ~3)
 
 
 def test_compat_header_compiles_and_links(tmp_path):
