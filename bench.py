@@ -10,7 +10,7 @@ A step decodes both columns from HBM to HBM.  Synthetic seeded data stands in
 for the reference's datasets, which are not available.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload brle_rlev2|rlev1|lzss|deflate|mixed|rlev1_encode|rlev2_encode]
+                    [--workload brle_rlev2|rlev1|lzss|deflate|mixed|brle_encode|rlev1_encode|rlev2_encode]
                     [--scale F]
 
 Multi-GPU (torchrun, one process per GPU): every rank decodes its own copy of
@@ -689,6 +689,9 @@ def mixed_cpu_sample(items, threads: int, budget_s: float):
 def encode_column(workload: str, scale: float):
     """The decode workloads' columns: (codec, raw bytes, encoder kwargs, chunk, label)."""
     import compression_b200.codecs as cc
+    if workload == "brle_encode":
+        a = cc.gen_brle_bytes(0xB0, int(256 * MiB * scale))
+        return ("brle", a, {}, 256 * 1024, f"byte-RLE encode of {256 * scale:g} MiB uint8, 256 KiB chunks")
     if workload == "rlev1_encode":
         v = cc.gen_rlev1_ints(0xA0, int(64 * MiB * scale) // 4)
         return ("rlev1", v.view(np.uint8), dict(comp_col_len=128, elem_bytes=4), 128 * 1024,
@@ -700,6 +703,8 @@ def encode_column(workload: str, scale: float):
 
 def host_encode(codec, raw, chunk, kw):
     import compression_b200.codecs as cc
+    if codec == "brle":
+        return cc.brle_encode(raw, chunk)
     if codec == "rlev1":
         return cc.rlev1_encode(raw, chunk, kw["comp_col_len"], kw["elem_bytes"])
     return cc.rlev2_encode(raw, chunk, kw["read_unit"])
@@ -730,11 +735,19 @@ def run_encode(args, rank, world, local_rank):
     # parity: the device container is the host encoder's, and decodes back
     bufs = cc.encode_device(codec, d_col, chunk, **kw)
     torch.cuda.synchronize()
-    blk = bufs["blk_off"].cpu().numpy().view(np.uint64)
-    size = int(blk[-1])
-    ok = ((bufs["status"].cpu().numpy() == 0).all() and np.array_equal(blk, host.meta["blk_off"])
-          and np.array_equal(bufs["col_len"].cpu().numpy().view(np.uint64), host.meta["col_len"])
-          and np.array_equal(bufs["data"][:size].cpu().numpy(), host.data))
+    if codec == "brle":
+        size = int(bufs["size"].item())
+        nc = host.n_chunks
+        ok = np.array_equal(bufs["container"][:size].cpu().numpy(), host.params["container"])
+        meta_out = 0  # ptr[] and the sizes are inside the container
+    else:
+        blk = bufs["blk_off"].cpu().numpy().view(np.uint64)
+        size = int(blk[-1])
+        nc = blk.size - 1
+        meta_out = 8 * (nc + 1) + 8 * 32 * nc
+        ok = ((bufs["status"].cpu().numpy() == 0).all() and np.array_equal(blk, host.meta["blk_off"])
+              and np.array_equal(bufs["col_len"].cpu().numpy().view(np.uint64), host.meta["col_len"])
+              and np.array_equal(bufs["data"][:size].cpu().numpy(), host.data))
     if not ok:
         raise RuntimeError(f"{codec} device encoder differs from the host encoder")
     job = cc.DeviceJob(host, dev)
@@ -761,27 +774,39 @@ def run_encode(args, rank, world, local_rank):
         torch.cuda.synchronize()
     ms = max_over_ranks([statistics.mean(a.elapsed_time(b) for a, b in evs)], world, dev)[0]
     value = job_rate(raw.size, world, ms)
-    nc = blk.size - 1
-    alg = raw.size + size + 8 * (nc + 1) + 8 * 32 * nc  # column in; container, blk_off, col_len out
+    alg = raw.size + size + meta_out  # column in; container (and blk_off, col_len) out
     peak, peak_kind = peaks()
     gbs = alg / (ms / 1e3) / 1e9
 
     e2e = None
     if not args.no_e2e:
         h_col = torch.from_numpy(raw.copy()).pin_memory()
-        h_data = torch.empty(bufs["data"].numel(), dtype=torch.uint8).pin_memory()
-        h_meta = torch.empty(nc + 1 + 32 * nc, dtype=torch.int64).pin_memory()
         d_in = torch.empty_like(d_col)
+        if codec == "brle":
+            h_data = torch.empty(bufs["container"].numel(), dtype=torch.uint8).pin_memory()
+            h_size = torch.empty(1, dtype=torch.int64).pin_memory()
 
-        def host_call():
-            d_in.copy_(h_col, non_blocking=True)
-            cc.encode_device(codec, d_in, chunk, bufs=bufs, **kw)
-            h_meta[:nc + 1].copy_(bufs["blk_off"], non_blocking=True)
-            h_meta[nc + 1:].copy_(bufs["col_len"], non_blocking=True)
-            torch.cuda.synchronize()
-            n = int(h_meta[nc])
-            h_data[:n].copy_(bufs["data"][:n])
-            return n
+            def host_call():
+                d_in.copy_(h_col, non_blocking=True)
+                cc.encode_device(codec, d_in, chunk, bufs=bufs)
+                h_size.copy_(bufs["size"], non_blocking=True)
+                torch.cuda.synchronize()
+                n = int(h_size[0])
+                h_data[:n].copy_(bufs["container"][:n])
+                return n
+        else:
+            h_data = torch.empty(bufs["data"].numel(), dtype=torch.uint8).pin_memory()
+            h_meta = torch.empty(nc + 1 + 32 * nc, dtype=torch.int64).pin_memory()
+
+            def host_call():
+                d_in.copy_(h_col, non_blocking=True)
+                cc.encode_device(codec, d_in, chunk, bufs=bufs, **kw)
+                h_meta[:nc + 1].copy_(bufs["blk_off"], non_blocking=True)
+                h_meta[nc + 1:].copy_(bufs["col_len"], non_blocking=True)
+                torch.cuda.synchronize()
+                n = int(h_meta[nc])
+                h_data[:n].copy_(bufs["data"][:n])
+                return n
 
         for _ in range(2):
             host_call()
@@ -792,17 +817,18 @@ def run_encode(args, rank, world, local_rank):
             ts.append(time.perf_counter() - t0)
         e2e_s = max_over_ranks([statistics.median(ts)], world, dev)[0]
         e2e = {"value": round(job_rate(raw.size, world, e2e_s * 1e3), 3), "unit": "GB/s",
-               "h2d_bytes_per_step": int(raw.size), "d2h_bytes_per_step": int(size + 8 * (nc + 1 + 32 * nc)),
+               "h2d_bytes_per_step": int(raw.size), "d2h_bytes_per_step": int(size + meta_out),
                "path": "pinned column H2D, gd_*_encode_device, container D2H"}
 
     line = {
         "metric": f"encoded GB/s ({codec} device encoder, column bytes in)", "value": round(value, 2),
         "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": round(ms, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u32" if codec == "rlev1" else "int64", "data": "synthetic (seeded generators)",
+        "dtype": {"brle": "u8", "rlev1": "u32"}.get(codec, "int64"), "data": "synthetic (seeded generators)",
         "config": {"workload": label, "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"replicas x{world}", "ratio": round(size / raw.size, 4)},
-        "roofline": {"bound": "hbm", "kernel": f"{codec} encode (lane encode + offsets + interleave)",
+        "roofline": {"bound": "hbm", "kernel": f"{codec} encode (" + ("regions + header + placement" if codec == "brle"
+                                                                   else "lane encode + offsets + interleave") + ")",
                      "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s", "frac": round(gbs / peak, 4),
                      "peak_source": peak_kind, "traffic": None, "alg_bytes": alg},
         "gpu_launches": 3 * K, "step": "one column encoded", "clocks": clk.summary(), "e2e": e2e,
@@ -851,7 +877,7 @@ def run_reference(args):
             vals.append(gbs)
     v = statistics.median(vals)
     metric = ("decompressed GB/s (byte-RLE + RLE v2 columns)" if args.workload == "brle_rlev2"
-              else f"encoded GB/s ({args.workload[:5]} device encoder, column bytes in)"
+              else f"encoded GB/s ({args.workload.split('_')[0]} device encoder, column bytes in)"
               if args.workload.endswith("_encode") else f"decompressed GB/s ({args.workload})")
     return {"impl": "reference", "metric": metric,
             "value": round(v, 3), "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -868,7 +894,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="brle_rlev2", choices=["brle_rlev2", "rlev1", "lzss", "deflate", "mixed",
-                                                                 "rlev1_encode", "rlev2_encode"])
+                                                                 "brle_encode", "rlev1_encode", "rlev2_encode"])
     ap.add_argument("--scale", type=float, default=1.0, help="workload size factor (1.0 = full size)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

@@ -234,7 +234,7 @@ def deflate_encode(raw, out_off: np.ndarray, level: int = 6, mode: np.ndarray | 
 
 
 # --------------------------------------------------------------------------
-# device encoders (RLE v1 / RLE v2 containers written on the GPU)
+# device encoders (byte-RLE / RLE v1 / RLE v2 containers written on the GPU)
 # --------------------------------------------------------------------------
 
 def encode_device(codec: str, d_col, chunk_size: int, *, comp_col_len: int = 128, elem_bytes: int = 4,
@@ -243,10 +243,14 @@ def encode_device(codec: str, d_col, chunk_size: int, *, comp_col_len: int = 128
     CUDA uint8 tensor holding the column.  Returns the device tensors
     {"data", "blk_off", "col_len", "status", "scratch"}; "data" is sized to
     the bound and the container's length is blk_off[-1].  `bufs` (a previous
-    return value) reuses its buffers."""
+    return value) reuses its buffers.  For "brle" (gd_brle_encode_device) the
+    tensors are {"container", "size", "scratch"}: the whole container and its
+    length."""
     import torch
     n = int(d_col.numel())
     L = lib()
+    if codec == "brle":
+        return _brle_encode_device(d_col, chunk_size, stream, bufs)
     if codec == "rlev1":
         bound = L.gd_rlev1_encode_bound(n, chunk_size, elem_bytes)
     elif codec == "rlev2":
@@ -276,16 +280,44 @@ def encode_device(codec: str, d_col, chunk_size: int, *, comp_col_len: int = 128
     return bufs
 
 
+def _brle_encode_device(d_col, chunk_size: int, stream=None, bufs: dict | None = None) -> dict:
+    """gd_brle_encode_device: {"container", "size" (device int64[1]), "scratch"}."""
+    import torch
+    n = int(d_col.numel())
+    L = lib()
+    cap = L.gd_brle_max_encoded_bytes(n, chunk_size)
+    sb = L.gd_brle_encode_scratch_bytes(n, chunk_size)
+    if sb == 0:
+        raise ValueError("bad encoder arguments")
+    dev = d_col.device
+    if bufs is None or bufs["container"].numel() < cap or bufs["scratch"].numel() < sb:
+        bufs = {"scratch": torch.empty(sb, dtype=torch.uint8, device=dev),
+                "container": torch.empty(cap, dtype=torch.uint8, device=dev),
+                "size": torch.zeros(1, dtype=torch.int64, device=dev)}
+    s = (stream or torch.cuda.current_stream()).cuda_stream
+    p = lambda t: C.c_void_p(t.data_ptr())
+    check(L.gd_brle_encode_device(p(d_col), n, chunk_size, p(bufs["scratch"]), p(bufs["container"]),
+                                  p(bufs["size"]), C.c_void_p(s)), "gd_brle_encode_device")
+    return bufs
+
+
 def encode_gpu(codec: str, raw, chunk_size: int, *, comp_col_len: int = 128, elem_bytes: int = 4,
                read_unit: int = 32) -> Encoded:
-    """The device encoder from host memory: the same Encoded as rlev1_encode /
-    rlev2_encode (rle_v1::compress_gpu, include/rle_v1/rlev1.h:25-97;
+    """The device encoder from host memory: the same Encoded as brle_encode /
+    rlev1_encode / rlev2_encode (brle::compress_gpu, include/brle/brle.h:242-303;
+    rle_v1::compress_gpu, include/rle_v1/rlev1.h:25-97;
     rlev2::compress_gpu_transpose, include/rlev2/encoder_trans.h:428-537)."""
     import torch
     b = _as_u8(raw)
     d = torch.from_numpy(b.copy()).cuda()
     r = encode_device(codec, d, chunk_size, comp_col_len=comp_col_len, elem_bytes=elem_bytes, read_unit=read_unit)
     torch.cuda.synchronize()
+    if codec == "brle":
+        cont = r["container"][:int(r["size"].item())].cpu().numpy()
+        n_ptr = int(cont[:4].view(np.uint32)[0])
+        ptr = cont[4:4 + 8 * n_ptr].copy().view(np.uint64)
+        hdr = 4 + 8 * n_ptr + 8
+        return Encoded("brle", cont[hdr:].copy(), b.size, n_ptr - 1, chunk_size, {"ptr": ptr}, {"container": cont})
     st = r["status"].cpu().numpy()
     if (st != 0).any():
         raise DecodeError(int(st[st != 0][0]), f"gd_{codec}_encode_device")

@@ -389,9 +389,9 @@ uint64_t gd_rlev2_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uin
 uint64_t gd_rlev2_encode_stream(const int64_t* vals, uint64_t n, uint8_t* out, uint64_t cap);
 
 /* ------------------------------------------------------------------------
- * Device encoders (sm_100a) for the RLE v1 and RLE v2 containers: the same
- * bytes as gd_rlev1_encode / gd_rlev2_encode, written from a column already
- * in device memory.  Asynchronous on `stream`.
+ * Device encoders (sm_100a) for the byte-RLE, RLE v1 and RLE v2 containers:
+ * the same bytes as gd_brle_encode / gd_rlev1_encode / gd_rlev2_encode,
+ * written from a column already in device memory.  Asynchronous on `stream`.
  *
  * d_scratch and d_data each hold gd_*_encode_bound(n_bytes, ...) bytes (4-byte
  * aligned); d_blk_off holds n_chunks + 1 and d_col_len 32 * n_chunks values;
@@ -400,6 +400,15 @@ uint64_t gd_rlev2_encode_stream(const int64_t* vals, uint64_t n, uint8_t* out, u
  * d_blk_off[n_chunks].  n_bytes must be a multiple of the value size and
  * d_in aligned to it; the last chunk is zero-padded as the host encoders do.
  * ------------------------------------------------------------------------ */
+/* brle::compress_gpu (include/brle/brle.h:242-303): the whole container
+ * [u32 n_ptr][u64 ptr][u64 total][data] written to d_out (4-byte aligned,
+ * gd_brle_max_encoded_bytes(n_bytes, chunk_size) bytes); its length goes to
+ * the device word *d_out_bytes.  d_scratch: gd_brle_encode_scratch_bytes
+ * bytes, 16-byte aligned. */
+uint64_t gd_brle_encode_scratch_bytes(uint64_t n_bytes, uint64_t chunk_size);
+gd_status_t gd_brle_encode_device(const uint8_t* d_in, uint64_t n_bytes, uint64_t chunk_size,
+                                  uint8_t* d_scratch, uint8_t* d_out, uint64_t* d_out_bytes,
+                                  gd_stream_t stream);
 /* rle_v1::compress_gpu (include/rle_v1/rlev1.h:25-97); elem_bytes 4 or 8. */
 uint64_t gd_rlev1_encode_bound(uint64_t n_bytes, uint64_t chunk_size, uint32_t elem_bytes);
 gd_status_t gd_rlev1_encode_device(const uint8_t* d_in, uint64_t n_bytes, uint64_t chunk_size,

@@ -40,6 +40,10 @@ def test_device_api_rejects_bad_arguments_without_gpu():
     assert L.gd_rlev2_encode_device(8, 996, 8192, 1, 4, 4, 8, 8, None, None) == 1
     assert L.gd_rlev2_encode_device(8, 1000, 8192, 3, 4, 4, 8, 8, None, None) == 1
     assert L.gd_rlev1_encode_device(None, 0, 4096, 128, 4, None, None, None, None, None, None) == 0  # empty
+    assert L.gd_brle_encode_device(None, 100, 4096, 16, 4, 8, None) == 1          # no input
+    assert L.gd_brle_encode_device(1, 100, 4096, 8, 4, 8, None) == 1             # scratch not 16-aligned
+    assert L.gd_brle_encode_device(1, 0, 4096, 16, 4, 8, None) == 1              # empty column
+    assert L.gd_brle_encode_scratch_bytes(0, 4096) == 0
     # bounds: 32 lane slots per chunk, each holding the longest lane stream
     assert L.gd_rlev1_encode_bound(128 * 1024, 128 * 1024, 4) == 32 * ((1024 * 5 + 1024 // 64 + 16 + 3) & ~3)
     assert L.gd_rlev2_encode_bound(2 * 256 * 1024, 256 * 1024) == 2 * 32 * ((1024 * 11 + 64 + 3) & ~3)

@@ -1,5 +1,5 @@
-"""GPU parity of the RLE v1 / RLE v2 device encoders: the container written on
-the device (data, blk_off, col_len) is byte-identical to the host encoder's,
+"""GPU parity of the byte-RLE, RLE v1 and RLE v2 device encoders: the
+container written on the device is byte-identical to the host encoder's,
 whose streams are pinned against the reference's own encoders in
 test_golden.py, and decodes back to the column through the device decoder
 and the oracle."""
@@ -88,10 +88,46 @@ def test_rlev2_device_encoder(cuda, ru, chunk):
         _roundtrip(dev, raw, cuda, exact=i not in (3, 7))
 
 
+def _brle_inputs():
+    rng = np.random.default_rng(7)
+    yield cc.gen_brle_bytes(1, 700000)
+    yield np.zeros(300000, np.uint8)                                   # one long run
+    yield rng.integers(0, 256, 200000).astype(np.uint8)                # incompressible: one region
+    yield rng.integers(0, 2, 300000).astype(np.uint8)                  # short runs
+    yield np.arange(100000, dtype=np.uint8)
+    for L in (5, 129, 130, 131, 133, 134, 135, 260, 261, 264, 265):   # run lengths around 130 multiples
+        pieces = []
+        for _ in range(400):
+            pieces.append(np.full(L if rng.random() < 0.5 else int(rng.integers(1, 7)), int(rng.integers(0, 4)),
+                                  np.uint8))
+            pieces.append(rng.integers(0, 256, int(rng.integers(0, 140))).astype(np.uint8))
+        yield np.concatenate(pieces)
+    pieces = []                                                         # runs right after 126..129 literals
+    for _ in range(500):
+        pieces.append((np.arange(int(rng.integers(120, 135))) * 3 % 251).astype(np.uint8))
+        pieces.append(np.full(int(rng.integers(3, 300)), 255, np.uint8))
+    yield np.concatenate(pieces)
+    for n in (1, 2, 3, 100, 255, 257, 4097):
+        yield cc.gen_brle_bytes(n, n)
+
+
+@pytest.mark.parametrize("chunk", [256 * 1024, 65536, 4096, 1000])
+def test_brle_device_encoder(cuda, chunk):
+    for raw in _brle_inputs():
+        host = cc.brle_encode(raw, chunk)
+        dev = cc.encode_gpu("brle", raw, chunk)
+        assert np.array_equal(dev.params["container"], host.params["container"])
+        _roundtrip(dev, raw, cuda)
+
+
 def test_device_encoders_at_bench_sizes(cuda):
-    """Full-size columns (64 MiB int32 RLE v1, 256 MiB int64 RLE v2): the
-    device container equals the host encoder's, and the device decoder
-    returns what the oracle decodes."""
+    """Full-size columns (256 MiB byte-RLE, 64 MiB int32 RLE v1, 256 MiB
+    int64 RLE v2): the device container equals the host encoder's, and the
+    device decoder returns what the oracle decodes."""
+    raw = cc.gen_brle_bytes(0xB0, 256 << 20)
+    dev = cc.encode_gpu("brle", raw, 256 * 1024)
+    assert np.array_equal(dev.params["container"], cc.brle_encode(raw, 256 * 1024).params["container"])
+    _roundtrip(dev, raw, cuda)
     v1 = cc.gen_rlev1_ints(0xA0, (64 << 20) // 4)
     v2 = cc.gen_rlev2_ints(0xB0, (256 << 20) // 8)
     for codec, v, kw, host in (
@@ -115,3 +151,5 @@ def test_device_encoder_argument_errors(cuda):
         cc.encode_device("rlev2", d[:996], 8192, read_unit=1)                     # not whole int64 values
     with pytest.raises(cc.DecodeError):
         cc.encode_device("rlev2", d, 8192, read_unit=3)                           # chunk % (256 * ru)
+    with pytest.raises(cc.DecodeError):
+        cc.encode_device("brle", d, 1 << 31)                                      # chunk above 1 GiB
