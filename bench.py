@@ -10,7 +10,8 @@ A step decodes both columns from HBM to HBM.  Synthetic seeded data stands in
 for the reference's datasets, which are not available.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload brle_rlev2|rlev1|lzss|deflate|mixed|brle_encode|rlev1_encode|rlev2_encode]
+                    [--workload brle_rlev2|rlev1|lzss|deflate|mixed|brle_encode|lzss_encode|rlev1_encode|
+                               rlev2_encode]
                     [--scale F]
 
 Multi-GPU (torchrun, one process per GPU): every rank decodes its own copy of
@@ -692,6 +693,9 @@ def encode_column(workload: str, scale: float):
     if workload == "brle_encode":
         a = cc.gen_brle_bytes(0xB0, int(256 * MiB * scale))
         return ("brle", a, {}, 256 * 1024, f"byte-RLE encode of {256 * scale:g} MiB uint8, 256 KiB chunks")
+    if workload == "lzss_encode":
+        a = cc.gen_markov_copy(0xC0, int(GiB * scale), 4096)
+        return ("lzss", a, {}, 64 * 1024, f"LZSS encode of {1024 * scale:g} MiB Markov+copy bytes, 64 KiB chunks")
     if workload == "rlev1_encode":
         v = cc.gen_rlev1_ints(0xA0, int(64 * MiB * scale) // 4)
         return ("rlev1", v.view(np.uint8), dict(comp_col_len=128, elem_bytes=4), 128 * 1024,
@@ -705,6 +709,8 @@ def host_encode(codec, raw, chunk, kw):
     import compression_b200.codecs as cc
     if codec == "brle":
         return cc.brle_encode(raw, chunk)
+    if codec == "lzss":
+        return cc.lzss_encode(raw, chunk)
     if codec == "rlev1":
         return cc.rlev1_encode(raw, chunk, kw["comp_col_len"], kw["elem_bytes"])
     return cc.rlev2_encode(raw, chunk, kw["read_unit"])
@@ -748,6 +754,9 @@ def run_encode(args, rank, world, local_rank):
         ok = ((bufs["status"].cpu().numpy() == 0).all() and np.array_equal(blk, host.meta["blk_off"])
               and np.array_equal(bufs["col_len"].cpu().numpy().view(np.uint64), host.meta["col_len"])
               and np.array_equal(bufs["data"][:size].cpu().numpy(), host.data))
+        if codec == "lzss":
+            meta_out += 32 * nc
+            ok = ok and np.array_equal(bufs["col_map"].cpu().numpy(), host.meta["col_map"])
     if not ok:
         raise RuntimeError(f"{codec} device encoder differs from the host encoder")
     job = cc.DeviceJob(host, dev)
@@ -797,12 +806,15 @@ def run_encode(args, rank, world, local_rank):
         else:
             h_data = torch.empty(bufs["data"].numel(), dtype=torch.uint8).pin_memory()
             h_meta = torch.empty(nc + 1 + 32 * nc, dtype=torch.int64).pin_memory()
+            h_map = torch.empty(32 * nc, dtype=torch.uint8).pin_memory()
 
             def host_call():
                 d_in.copy_(h_col, non_blocking=True)
                 cc.encode_device(codec, d_in, chunk, bufs=bufs, **kw)
                 h_meta[:nc + 1].copy_(bufs["blk_off"], non_blocking=True)
                 h_meta[nc + 1:].copy_(bufs["col_len"], non_blocking=True)
+                if codec == "lzss":
+                    h_map.copy_(bufs["col_map"], non_blocking=True)
                 torch.cuda.synchronize()
                 n = int(h_meta[nc])
                 h_data[:n].copy_(bufs["data"][:n])
@@ -824,14 +836,15 @@ def run_encode(args, rank, world, local_rank):
         "metric": f"encoded GB/s ({codec} device encoder, column bytes in)", "value": round(value, 2),
         "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": round(ms, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": {"brle": "u8", "rlev1": "u32"}.get(codec, "int64"), "data": "synthetic (seeded generators)",
+        "dtype": {"brle": "u8", "lzss": "u8", "rlev1": "u32"}.get(codec, "int64"), "data": "synthetic (seeded generators)",
         "config": {"workload": label, "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"replicas x{world}", "ratio": round(size / raw.size, 4)},
-        "roofline": {"bound": "hbm", "kernel": f"{codec} encode (" + ("regions + header + placement" if codec == "brle"
+        "roofline": {"bound": "hbm", "kernel": f"{codec} encode (" + ("regions + header + placement" if codec == "brle" else
+                                                                   "columns + ranks + offsets + interleave" if codec == "lzss"
                                                                    else "lane encode + offsets + interleave") + ")",
                      "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s", "frac": round(gbs / peak, 4),
                      "peak_source": peak_kind, "traffic": None, "alg_bytes": alg},
-        "gpu_launches": 3 * K, "step": "one column encoded", "clocks": clk.summary(), "e2e": e2e,
+        "gpu_launches": (4 if codec == "lzss" else 3) * K, "step": "one column encoded", "clocks": clk.summary(), "e2e": e2e,
     }
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -894,7 +907,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="brle_rlev2", choices=["brle_rlev2", "rlev1", "lzss", "deflate", "mixed",
-                                                                 "brle_encode", "rlev1_encode", "rlev2_encode"])
+                                                                 "brle_encode", "lzss_encode", "rlev1_encode",
+                                                                 "rlev2_encode"])
     ap.add_argument("--scale", type=float, default=1.0, help="workload size factor (1.0 = full size)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

@@ -234,14 +234,15 @@ def deflate_encode(raw, out_off: np.ndarray, level: int = 6, mode: np.ndarray | 
 
 
 # --------------------------------------------------------------------------
-# device encoders (byte-RLE / RLE v1 / RLE v2 containers written on the GPU)
+# device encoders (byte-RLE / LZSS / RLE v1 / RLE v2 containers written on the GPU)
 # --------------------------------------------------------------------------
 
 def encode_device(codec: str, d_col, chunk_size: int, *, comp_col_len: int = 128, elem_bytes: int = 4,
                   read_unit: int = 32, stream=None, bufs: dict | None = None) -> dict:
-    """Enqueue gd_rlev1_encode_device / gd_rlev2_encode_device on `d_col`, a
-    CUDA uint8 tensor holding the column.  Returns the device tensors
-    {"data", "blk_off", "col_len", "status", "scratch"}; "data" is sized to
+    """Enqueue gd_rlev1_encode_device / gd_rlev2_encode_device /
+    gd_lzss_encode_device on `d_col`, a CUDA uint8 tensor holding the column.
+    Returns the device tensors {"data", "blk_off", "col_len", "col_map"
+    (LZSS), "status", "scratch"}; "data" is sized to
     the bound and the container's length is blk_off[-1].  `bufs` (a previous
     return value) reuses its buffers.  For "brle" (gd_brle_encode_device) the
     tensors are {"container", "size", "scratch"}: the whole container and its
@@ -253,6 +254,8 @@ def encode_device(codec: str, d_col, chunk_size: int, *, comp_col_len: int = 128
         return _brle_encode_device(d_col, chunk_size, stream, bufs)
     if codec == "rlev1":
         bound = L.gd_rlev1_encode_bound(n, chunk_size, elem_bytes)
+    elif codec == "lzss":
+        bound = L.gd_lzss_encode_bound(n, chunk_size)
     elif codec == "rlev2":
         bound = L.gd_rlev2_encode_bound(n, chunk_size)
     else:
@@ -266,13 +269,17 @@ def encode_device(codec: str, d_col, chunk_size: int, *, comp_col_len: int = 128
                 "data": torch.empty(bound, dtype=torch.uint8, device=dev),
                 "blk_off": torch.empty(nc + 1, dtype=torch.int64, device=dev),
                 "col_len": torch.empty(32 * nc, dtype=torch.int64, device=dev),
-                "status": torch.empty(nc, dtype=torch.int32, device=dev)}
+                "status": torch.empty(nc, dtype=torch.int32, device=dev),
+                "col_map": torch.empty(32 * nc, dtype=torch.uint8, device=dev)}
     s = (stream or torch.cuda.current_stream()).cuda_stream
     p = lambda t: C.c_void_p(t.data_ptr())
     if codec == "rlev1":
         rc = L.gd_rlev1_encode_device(p(d_col), n, chunk_size, comp_col_len, elem_bytes, p(bufs["scratch"]),
                                       p(bufs["data"]), p(bufs["blk_off"]), p(bufs["col_len"]), p(bufs["status"]),
                                       C.c_void_p(s))
+    elif codec == "lzss":
+        rc = L.gd_lzss_encode_device(p(d_col), n, chunk_size, p(bufs["scratch"]), p(bufs["data"]), p(bufs["blk_off"]),
+                                     p(bufs["col_len"]), p(bufs["col_map"]), p(bufs["status"]), C.c_void_p(s))
     else:
         rc = L.gd_rlev2_encode_device(p(d_col), n, chunk_size, read_unit, p(bufs["scratch"]), p(bufs["data"]),
                                       p(bufs["blk_off"]), p(bufs["col_len"]), p(bufs["status"]), C.c_void_p(s))
@@ -304,7 +311,8 @@ def _brle_encode_device(d_col, chunk_size: int, stream=None, bufs: dict | None =
 def encode_gpu(codec: str, raw, chunk_size: int, *, comp_col_len: int = 128, elem_bytes: int = 4,
                read_unit: int = 32) -> Encoded:
     """The device encoder from host memory: the same Encoded as brle_encode /
-    rlev1_encode / rlev2_encode (brle::compress_gpu, include/brle/brle.h:242-303;
+    lzss_encode / rlev1_encode / rlev2_encode (brle::compress_gpu,
+    include/brle/brle.h:242-303; lzss::compress_gpu, include/lzss/lzss_gpu2.h:1915-2127;
     rle_v1::compress_gpu, include/rle_v1/rlev1.h:25-97;
     rlev2::compress_gpu_transpose, include/rlev2/encoder_trans.h:428-537)."""
     import torch
@@ -325,9 +333,12 @@ def encode_gpu(codec: str, raw, chunk_size: int, *, comp_col_len: int = 128, ele
     col = r["col_len"].cpu().numpy().view(np.uint64)
     data = r["data"][:int(blk[-1])].cpu().numpy()
     nc = blk.size - 1
+    meta = {"blk_off": blk, "col_len": col}
+    if codec == "lzss":
+        meta["col_map"] = r["col_map"].cpu().numpy()
     params = ({"comp_col_len": comp_col_len, "elem_bytes": elem_bytes} if codec == "rlev1"
-              else {"read_unit": read_unit})
-    return Encoded(codec, data, b.size, nc, chunk_size, {"blk_off": blk, "col_len": col}, params)
+              else {"read_unit": read_unit} if codec == "rlev2" else {})
+    return Encoded(codec, data, b.size, nc, chunk_size, meta, params)
 
 
 # --------------------------------------------------------------------------

@@ -389,8 +389,8 @@ uint64_t gd_rlev2_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uin
 uint64_t gd_rlev2_encode_stream(const int64_t* vals, uint64_t n, uint8_t* out, uint64_t cap);
 
 /* ------------------------------------------------------------------------
- * Device encoders (sm_100a) for the byte-RLE, RLE v1 and RLE v2 containers:
- * the same bytes as gd_brle_encode / gd_rlev1_encode / gd_rlev2_encode,
+ * Device encoders (sm_100a) for the byte-RLE, LZSS, RLE v1 and RLE v2
+ * containers: the same bytes as the host encoders gd_*_encode,
  * written from a column already in device memory.  Asynchronous on `stream`.
  *
  * d_scratch and d_data each hold gd_*_encode_bound(n_bytes, ...) bytes (4-byte
@@ -408,6 +408,17 @@ uint64_t gd_rlev2_encode_stream(const int64_t* vals, uint64_t n, uint8_t* out, u
 uint64_t gd_brle_encode_scratch_bytes(uint64_t n_bytes, uint64_t chunk_size);
 gd_status_t gd_brle_encode_device(const uint8_t* d_in, uint64_t n_bytes, uint64_t chunk_size,
                                   uint8_t* d_scratch, uint8_t* d_out, uint64_t* d_out_bytes,
+                                  gd_stream_t stream);
+/* lzss::compress_gpu (include/lzss/lzss_gpu2.h:1915-2127): the interleaved
+ * container with its .meta arrays -- d_blk_off (n_chunks + 1), d_col_len and
+ * d_col_map (32 * n_chunks, slots by descending column length).  chunk_size
+ * a multiple of 128, at most 128 KiB; d_in, d_scratch and d_data 4-byte
+ * aligned, the latter two gd_lzss_encode_bound bytes each.  The last chunk
+ * is zero-padded to a whole chunk. */
+uint64_t gd_lzss_encode_bound(uint64_t n_bytes, uint64_t chunk_size);
+gd_status_t gd_lzss_encode_device(const uint8_t* d_in, uint64_t n_bytes, uint64_t chunk_size,
+                                  uint8_t* d_scratch, uint8_t* d_data, uint64_t* d_blk_off,
+                                  uint64_t* d_col_len, uint8_t* d_col_map, uint32_t* d_status,
                                   gd_stream_t stream);
 /* rle_v1::compress_gpu (include/rle_v1/rlev1.h:25-97); elem_bytes 4 or 8. */
 uint64_t gd_rlev1_encode_bound(uint64_t n_bytes, uint64_t chunk_size, uint32_t elem_bytes);

@@ -44,6 +44,9 @@ def test_device_api_rejects_bad_arguments_without_gpu():
     assert L.gd_brle_encode_device(1, 100, 4096, 8, 4, 8, None) == 1             # scratch not 16-aligned
     assert L.gd_brle_encode_device(1, 0, 4096, 16, 4, 8, None) == 1              # empty column
     assert L.gd_brle_encode_scratch_bytes(0, 4096) == 0
+    assert L.gd_lzss_encode_device(4, 1000, 1000, 4, 4, 8, 8, 1, None, None) == 1     # chunk % 128
+    assert L.gd_lzss_encode_device(4, 1000, 256 * 1024, 4, 4, 8, 8, 1, None, None) == 1  # column > 4 KiB
+    assert L.gd_lzss_encode_device(2, 1000, 4096, 4, 4, 8, 8, 1, None, None) == 1     # unaligned input
     # bounds: 32 lane slots per chunk, each holding the longest lane stream
     assert L.gd_rlev1_encode_bound(128 * 1024, 128 * 1024, 4) == 32 * ((1024 * 5 + 1024 // 64 + 16 + 3) & ~3)
     assert L.gd_rlev2_encode_bound(2 * 256 * 1024, 256 * 1024) == 2 * 32 * ((1024 * 11 + 64 + 3) & ~3)

@@ -1,4 +1,4 @@
-"""GPU parity of the byte-RLE, RLE v1 and RLE v2 device encoders: the
+"""GPU parity of the byte-RLE, LZSS, RLE v1 and RLE v2 device encoders: the
 container written on the device is byte-identical to the host encoder's,
 whose streams are pinned against the reference's own encoders in
 test_golden.py, and decodes back to the column through the device decoder
@@ -17,6 +17,8 @@ def _same(a: cc.Encoded, b: cc.Encoded):
     assert np.array_equal(a.meta["blk_off"], b.meta["blk_off"])
     assert np.array_equal(a.meta["col_len"], b.meta["col_len"])
     assert np.array_equal(a.data, b.data)
+    if "col_map" in b.meta:
+        assert np.array_equal(a.meta["col_map"], b.meta["col_map"])
 
 
 def _roundtrip(enc: cc.Encoded, raw_bytes: np.ndarray, dev, exact: bool = True):
@@ -120,13 +122,38 @@ def test_brle_device_encoder(cuda, chunk):
         _roundtrip(dev, raw, cuda)
 
 
+def _lzss_inputs():
+    rng = np.random.default_rng(11)
+    yield cc.gen_markov_copy(3, 1 << 20, 4096)
+    yield np.zeros(300000, np.uint8)                                    # 34-byte matches everywhere
+    yield rng.integers(0, 256, 200000).astype(np.uint8)                 # literals only
+    yield np.tile(np.arange(7, dtype=np.uint8), 40000)
+    yield rng.integers(0, 4, 300000).astype(np.uint8)                   # long candidate lists, short matches
+    yield (np.arange(300000) // 64 % 5).astype(np.uint8)
+    yield cc.gen_markov_copy(4, 100003, 4096)                           # a short last chunk
+
+
+@pytest.mark.parametrize("chunk", [64 * 1024, 128 * 1024, 4096, 128])
+def test_lzss_device_encoder(cuda, chunk):
+    for raw in _lzss_inputs():
+        host = cc.lzss_encode(raw, chunk)
+        dev = cc.encode_gpu("lzss", raw, chunk)
+        _same(dev, host)
+        _roundtrip(dev, raw, cuda)
+
+
 def test_device_encoders_at_bench_sizes(cuda):
     """Full-size columns (256 MiB byte-RLE, 64 MiB int32 RLE v1, 256 MiB
-    int64 RLE v2): the device container equals the host encoder's, and the
-    device decoder returns what the oracle decodes."""
+    int64 RLE v2; 256 MiB of the LZSS column): the device container equals
+    the host encoder's, and the device decoder returns what the oracle
+    decodes."""
     raw = cc.gen_brle_bytes(0xB0, 256 << 20)
     dev = cc.encode_gpu("brle", raw, 256 * 1024)
     assert np.array_equal(dev.params["container"], cc.brle_encode(raw, 256 * 1024).params["container"])
+    _roundtrip(dev, raw, cuda)
+    raw = cc.gen_markov_copy(0xC0, 256 << 20, 4096)                     # LZSS: a quarter of the 1 GiB column
+    dev = cc.encode_gpu("lzss", raw, 64 * 1024)
+    _same(dev, cc.lzss_encode(raw, 64 * 1024))
     _roundtrip(dev, raw, cuda)
     v1 = cc.gen_rlev1_ints(0xA0, (64 << 20) // 4)
     v2 = cc.gen_rlev2_ints(0xB0, (256 << 20) // 8)
@@ -153,3 +180,7 @@ def test_device_encoder_argument_errors(cuda):
         cc.encode_device("rlev2", d, 8192, read_unit=3)                           # chunk % (256 * ru)
     with pytest.raises(cc.DecodeError):
         cc.encode_device("brle", d, 1 << 31)                                      # chunk above 1 GiB
+    with pytest.raises(cc.DecodeError):
+        cc.encode_device("lzss", d, 1000)                                         # chunk not 128-byte rows
+    with pytest.raises(cc.DecodeError):
+        cc.encode_device("lzss", d, 256 * 1024)                                   # column above 4 KiB
