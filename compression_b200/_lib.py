@@ -35,6 +35,7 @@ SIGNATURES = {
     "gd_gpuinflate": (i32, [vp, vp, i32, i32, vp]),
     "gd_lzss_contig_decode": (i32, [vp, vp, u32, u64, vp, u64, vp, vp]),
     "gd_brle_trans_decode": (i32, [vp, vp, vp, vp, u32, u64, vp, u64, vp, vp]),
+    "gd_brle_trans4_decode": (i32, [vp, vp, vp, vp, u32, u64, vp, u64, vp, vp]),
     "gd_copy_uncompressed_blocks": (i32, [vp, i32, vp]),
     "gd_batch_decode": (i32, [vp, u32, vp, i32, u32, u32, vp, vp, vp, vp]),
     "gd_batch_warps": (u32, [u32, u32]),
@@ -54,6 +55,7 @@ SIGNATURES = {
     "gd_lzss_contig_decompress": (i32, [vp, u64, vp, vp]),
     "gd_inflate_decompress": (i32, [vp, u64, vp, vp, vp, u32, i32, vp, vp]),
     "gd_brle_trans_decompress": (i32, [vp, u64, vp, u64, vp, u64, vp, u64, u64, vp, vp]),
+    "gd_brle_trans4_decompress": (i32, [vp, u64, vp, u64, vp, u64, vp, u64, u64, vp, vp]),
     "gd_brle_max_encoded_bytes": (u64, [u64, u64]),
     "gd_brle_encode": (u64, [vp, u64, u64, vp]),
     "gd_rlev1_max_encoded_bytes": (u64, [u64, u64]),
@@ -77,6 +79,8 @@ SIGNATURES = {
     "gd_lzss_contig_encode": (u64, [vp, u64, u64, vp]),
     "gd_brle_trans_max_encoded_bytes": (u64, [u64, u64]),
     "gd_brle_trans_encode": (u64, [vp, u64, u64, vp, vp, vp, vp]),
+    "gd_brle_trans4_max_encoded_bytes": (u64, [u64, u64]),
+    "gd_brle_trans4_encode": (u64, [vp, u64, u64, vp, vp, vp, vp]),
     "gd_deflate_max_encoded_bytes": (u64, [vp, u32]),
     "gd_deflate_encode": (u64, [vp, vp, u32, i32, vp, i32, vp, vp, vp]),
     "gd_gen_rlev1_ints": (None, [u64, u64, vp]),

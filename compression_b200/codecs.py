@@ -210,6 +210,25 @@ def brle_trans_encode(raw, chunk_size: int = 4096) -> Encoded:
                    {"blk_off": blk, "col_len": col, "col_map": cmap}, {})
 
 
+def brle_trans4_encode(raw, chunk_size: int = 8192) -> Encoded:
+    """brle::compress_gpu of include/brle/brle_gpu_4B.h:640-715: the flag-byte
+    columns over 4-byte symbols, same ranked 32-column layout (8 KiB chunks
+    in the reference)."""
+    b = _as_u8(raw)
+    L = lib()
+    nc = (b.size + chunk_size - 1) // chunk_size
+    cap = L.gd_brle_trans4_max_encoded_bytes(b.size, chunk_size)
+    data = np.empty(cap, dtype=np.uint8)
+    blk = np.empty(nc + 1, dtype=np.uint64)
+    col = np.empty(32 * nc, dtype=np.uint64)
+    cmap = np.empty(32 * nc, dtype=np.uint8)
+    n = L.gd_brle_trans4_encode(_p(b), b.size, chunk_size, _p(data), _p(blk), _p(col), _p(cmap))
+    if n == 0:
+        raise ValueError("brle_trans4 encode failed")
+    return Encoded("brle_trans4", data[:n].copy(), b.size, nc, chunk_size,
+                   {"blk_off": blk, "col_len": col, "col_map": cmap}, {})
+
+
 def deflate_encode(raw, out_off: np.ndarray, level: int = 6, mode: np.ndarray | None = None,
                    zlib_header: int = 1) -> Encoded:
     """Per-chunk zlib streams padded to 8 bytes (orig_compressor.py:44-126).
@@ -401,9 +420,10 @@ class DeviceJob:
         elif e.codec == "lzss_contig":
             rc = L.gd_lzss_contig_decode(ptr(self.d_data), ptr(m["ends"]), e.n_chunks, e.chunk_size, ptr(self.d_out),
                                          e.n_out, ptr(self.d_status), s)
-        elif e.codec == "brle_trans":
-            rc = L.gd_brle_trans_decode(ptr(self.d_data), ptr(m["blk_off"]), ptr(m["col_len"]), ptr(m["col_map"]),
-                                        e.n_chunks, e.chunk_size, ptr(self.d_out), e.n_out, ptr(self.d_status), s)
+        elif e.codec in ("brle_trans", "brle_trans4"):
+            fn = L.gd_brle_trans_decode if e.codec == "brle_trans" else L.gd_brle_trans4_decode
+            rc = fn(ptr(self.d_data), ptr(m["blk_off"]), ptr(m["col_len"]), ptr(m["col_map"]),
+                    e.n_chunks, e.chunk_size, ptr(self.d_out), e.n_out, ptr(self.d_status), s)
         elif e.codec == "deflate" and self.d_order is not None:
             rc = L.gd_inflate_ordered(ptr(self.d_data), ptr(m["comp_off"]), ptr(m["comp_len"]), ptr(m["out_off"]),
                                       e.n_chunks, e.params["zlib_header"], ptr(self.d_out), ptr(self.d_status),
@@ -484,10 +504,10 @@ def decode_host(enc: Encoded, keep: bool = True) -> np.ndarray:
     elif enc.codec == "lzss_contig":
         cont = enc.params["container"]
         rc = L.gd_lzss_contig_decompress(_p(cont), cont.size, C.byref(out), C.byref(n))
-    elif enc.codec == "brle_trans":
-        rc = L.gd_brle_trans_decompress(_p(enc.data), enc.data.size, _p(m["col_len"]), m["col_len"].nbytes,
-                                        _p(m["col_map"]), m["col_map"].nbytes, _p(m["blk_off"]), m["blk_off"].nbytes,
-                                        enc.chunk_size, C.byref(out), C.byref(n))
+    elif enc.codec in ("brle_trans", "brle_trans4"):
+        fn = L.gd_brle_trans_decompress if enc.codec == "brle_trans" else L.gd_brle_trans4_decompress
+        rc = fn(_p(enc.data), enc.data.size, _p(m["col_len"]), m["col_len"].nbytes, _p(m["col_map"]),
+                m["col_map"].nbytes, _p(m["blk_off"]), m["blk_off"].nbytes, enc.chunk_size, C.byref(out), C.byref(n))
     elif enc.codec == "deflate":
         oo = m["out_off"]
         cs = int(oo[1] - oo[0]) if enc.n_chunks > 0 else 1

@@ -1,4 +1,5 @@
-// brle_trans.cu -- byte-RLE flag-byte interleaved container decoder for sm_100a.
+// brle_trans.cu -- byte-RLE flag-byte interleaved container decoder for sm_100a
+// (1-byte symbols, and the 4-byte-symbol variant of brle_gpu_4B.h).
 //
 // Container (brle_trans::compress_gpu / decompress_gpu, include/brle/
 // brle_trans.h:563-791): a chunk (4 KiB in the reference) is 32 columns,
@@ -31,6 +32,10 @@ __host__ __device__ constexpr uint32_t warp_smem(uint32_t chunk) {
     return ((in_cap(chunk / 32u) + 15u) & ~15u) + chunk;
 }
 
+// SYM = 1: brle_trans; SYM = 4: the 4-byte-symbol variant (brle::
+// decompress_func, include/brle/brle_gpu_4B.h:75-223): literals are 4-byte
+// symbols and a run item is a count byte followed by the symbol.
+template <int SYM>
 __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restrict__ data,
                                                          const uint64_t* __restrict__ blk_off,
                                                          const uint64_t* __restrict__ col_len,
@@ -84,6 +89,7 @@ __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restr
             uint32_t row_base = 0, row = 0;  // byte offset of the current row
             uint32_t o = 0, block = 0, head = 0, cnt = 0;
             bool pend = false;  // a count byte waits for its value byte
+            uint32_t nb = 0, symv = 0;  // SYM 4: symbol bytes still to come, the symbol so far
             for (uint32_t j = 0; j < len; ++j) {
                 if (j && (j & 3u) == 0) {  // next row
                     row_base += 4u * act;
@@ -91,6 +97,38 @@ __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restr
                     while (act > 0 && slen[act - 1] <= 4u * row) --act;
                 }
                 const uint32_t v = sin[row_base + 4u * lane + (j & 3u)];
+                if constexpr (SYM == 4) {
+                    if (nb) {  // a symbol byte
+                        symv |= v << (8u * (4u - nb));
+                        if (--nb == 0) {
+                            if (o + 4u * cnt > L) {
+                                err = ST_OVERRUN;
+                                break;
+                            }
+                            for (uint32_t k = 0; k < cnt; ++k, o += 4)
+                                *reinterpret_cast<uint32_t*>(tile + (o >> 2) * 128u + col * 4u) = symv;
+                        }
+                        continue;
+                    }
+                    if (block == 0) {
+                        head = v;
+                        block = 1;
+                        continue;
+                    }
+                    const uint32_t lit = head & 1u;
+                    head >>= 1;
+                    if (++block == 9) block = 0;
+                    if (lit) {  // v is the symbol's first byte
+                        cnt = 1;
+                        symv = v;
+                        nb = 3;
+                    } else {  // v is the count
+                        cnt = v;
+                        symv = 0;
+                        nb = 4;
+                    }
+                    continue;
+                }
                 if (pend) {
                     pend = false;
                     if (o + cnt > L) {
@@ -120,7 +158,7 @@ __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restr
                     pend = true;
                 }
             }
-            if (err == ST_OK && (pend || o != L)) err = ST_CORRUPT;
+            if (err == ST_OK && (pend || nb || o != L)) err = ST_CORRUPT;
         }
         const uint32_t e = __reduce_max_sync(GD_FULL_MASK, err);
         __syncwarp();
@@ -144,10 +182,10 @@ __global__ void __launch_bounds__(WPB * 32) decode_kernel(const uint8_t* __restr
 }  // namespace brlet
 }  // namespace gd
 
-extern "C" gd_status_t gd_brle_trans_decode(const uint8_t* d_data, const uint64_t* d_blk_off, const uint64_t* d_col_len,
-                                            const uint8_t* d_col_map, uint32_t n_chunks, uint64_t chunk_size,
-                                            uint8_t* d_out, uint64_t out_n_bytes, uint32_t* d_status,
-                                            gd_stream_t stream) {
+template <int SYM>
+static gd_status_t flag_decode(const uint8_t* d_data, const uint64_t* d_blk_off, const uint64_t* d_col_len,
+                               const uint8_t* d_col_map, uint32_t n_chunks, uint64_t chunk_size, uint8_t* d_out,
+                               uint64_t out_n_bytes, uint32_t* d_status, gd_stream_t stream) {
     using namespace gd::brlet;
     if (n_chunks == 0) return GD_OK;
     if (!d_data || !d_blk_off || !d_col_len || !d_col_map || !d_out) return GD_ERR_INVALID_ARG;
@@ -155,7 +193,7 @@ extern "C" gd_status_t gd_brle_trans_decode(const uint8_t* d_data, const uint64_
     if (out_n_bytes > chunk_size * (uint64_t)n_chunks || out_n_bytes <= chunk_size * (uint64_t)(n_chunks - 1))
         return GD_ERR_INVALID_ARG;
     const uint32_t smem = WPB * warp_smem((uint32_t)chunk_size);
-    if (cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(decode_kernel<SYM>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
         return GD_ERR_CUDA;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -163,7 +201,24 @@ extern "C" gd_status_t gd_brle_trans_decode(const uint8_t* d_data, const uint64_
     uint32_t grid = (n_chunks + WPB - 1) / WPB;
     const uint32_t cap = (uint32_t)sms * 16;
     if (grid > cap) grid = cap;
-    decode_kernel<<<grid, WPB * 32, smem, (cudaStream_t)stream>>>(d_data, d_blk_off, d_col_len, d_col_map, n_chunks,
-                                                                 (uint32_t)chunk_size, d_out, out_n_bytes, d_status);
+    decode_kernel<SYM><<<grid, WPB * 32, smem, (cudaStream_t)stream>>>(d_data, d_blk_off, d_col_len, d_col_map,
+                                                                      n_chunks, (uint32_t)chunk_size, d_out,
+                                                                      out_n_bytes, d_status);
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+}
+
+extern "C" gd_status_t gd_brle_trans_decode(const uint8_t* d_data, const uint64_t* d_blk_off, const uint64_t* d_col_len,
+                                            const uint8_t* d_col_map, uint32_t n_chunks, uint64_t chunk_size,
+                                            uint8_t* d_out, uint64_t out_n_bytes, uint32_t* d_status,
+                                            gd_stream_t stream) {
+    return flag_decode<1>(d_data, d_blk_off, d_col_len, d_col_map, n_chunks, chunk_size, d_out, out_n_bytes,
+                          d_status, stream);
+}
+
+extern "C" gd_status_t gd_brle_trans4_decode(const uint8_t* d_data, const uint64_t* d_blk_off,
+                                             const uint64_t* d_col_len, const uint8_t* d_col_map, uint32_t n_chunks,
+                                             uint64_t chunk_size, uint8_t* d_out, uint64_t out_n_bytes,
+                                             uint32_t* d_status, gd_stream_t stream) {
+    return flag_decode<4>(d_data, d_blk_off, d_col_len, d_col_map, n_chunks, chunk_size, d_out, out_n_bytes,
+                          d_status, stream);
 }

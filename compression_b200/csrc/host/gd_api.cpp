@@ -520,10 +520,13 @@ gd_status_t gd_lzss_contig_decompress(const uint8_t* in, uint64_t in_n_bytes, ui
 // col_len / col_map / blk_offset from ./input_data side files): the output is
 // n_chunks * chunk_size bytes, n_chunks = blk_n_bytes/8 - 1.
 // ---------------------------------------------------------------------------
-gd_status_t gd_brle_trans_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* col_len,
-                                     uint64_t col_n_bytes, const uint8_t* col_map, uint64_t map_n_bytes,
-                                     const uint64_t* blk_off, uint64_t blk_n_bytes, uint64_t chunk_size,
-                                     uint8_t** out, uint64_t* out_n_bytes) {
+using FlagDecode = gd_status_t (*)(const uint8_t*, const uint64_t*, const uint64_t*, const uint8_t*, uint32_t,
+                                   uint64_t, uint8_t*, uint64_t, uint32_t*, gd_stream_t);
+
+static gd_status_t flag_decompress(FlagDecode decode, const uint8_t* in, uint64_t in_n_bytes,
+                                   const uint64_t* col_len, uint64_t col_n_bytes, const uint8_t* col_map,
+                                   uint64_t map_n_bytes, const uint64_t* blk_off, uint64_t blk_n_bytes,
+                                   uint64_t chunk_size, uint8_t** out, uint64_t* out_n_bytes) {
     if (!in || !col_len || !col_map || !blk_off || !out || !out_n_bytes || blk_n_bytes < 16) return GD_ERR_INVALID_ARG;
     const uint64_t n = blk_n_bytes / 8 - 1;
     if (col_n_bytes < 8 * 32 * n || map_n_bytes < 32 * n) return GD_ERR_INVALID_ARG;
@@ -551,8 +554,8 @@ gd_status_t gd_brle_trans_decompress(const uint8_t* in, uint64_t in_n_bytes, con
             return ok ? GD_OK : GD_ERR_CUDA;
         },
         [&](uint64_t a, uint64_t b, cudaStream_t st) {
-            return gd_brle_trans_decode(d_data, d_bo + a, d_cl + 32 * a, d_map + 32 * a, (uint32_t)(b - a),
-                                        chunk_size, d_out + a * chunk_size, (b - a) * chunk_size, d_st + a, st);
+            return decode(d_data, d_bo + a, d_cl + 32 * a, d_map + 32 * a, (uint32_t)(b - a), chunk_size,
+                          d_out + a * chunk_size, (b - a) * chunk_size, d_st + a, st);
         });
     if (r != GD_OK) {
         gd_free(h);
@@ -561,6 +564,24 @@ gd_status_t gd_brle_trans_decompress(const uint8_t* in, uint64_t in_n_bytes, con
     *out = h;
     *out_n_bytes = total;
     return GD_OK;
+}
+
+gd_status_t gd_brle_trans_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* col_len,
+                                     uint64_t col_n_bytes, const uint8_t* col_map, uint64_t map_n_bytes,
+                                     const uint64_t* blk_off, uint64_t blk_n_bytes, uint64_t chunk_size,
+                                     uint8_t** out, uint64_t* out_n_bytes) {
+    return flag_decompress(gd_brle_trans_decode, in, in_n_bytes, col_len, col_n_bytes, col_map, map_n_bytes, blk_off,
+                           blk_n_bytes, chunk_size, out, out_n_bytes);
+}
+
+// brle::decompress_gpu of include/brle/brle_gpu_4B.h:717-897 (4-byte
+// symbols, 8 KiB chunks there), with its side files' arrays passed in.
+gd_status_t gd_brle_trans4_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* col_len,
+                                      uint64_t col_n_bytes, const uint8_t* col_map, uint64_t map_n_bytes,
+                                      const uint64_t* blk_off, uint64_t blk_n_bytes, uint64_t chunk_size,
+                                      uint8_t** out, uint64_t* out_n_bytes) {
+    return flag_decompress(gd_brle_trans4_decode, in, in_n_bytes, col_len, col_n_bytes, col_map, map_n_bytes,
+                           blk_off, blk_n_bytes, chunk_size, out, out_n_bytes);
 }
 
 

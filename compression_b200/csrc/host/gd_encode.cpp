@@ -279,6 +279,53 @@ void brle_trans_encode_column(const uint8_t* d, uint32_t L, std::vector<uint8_t>
     }
 }
 
+// The 4-byte-symbol variant of the flag-byte column (restated from
+// brle::compress_func, include/brle/brle_gpu_4B.h:321-638): the column's
+// 4-byte words are its symbols; a maximal run of 3 or more equal symbols is
+// a run item (count byte, symbol; flag bit 0), a shorter one that many
+// literal items (the symbol; flag bit 1).  A flag byte precedes every 8
+// items and after the 8th item of a group the next one is reserved -- except
+// after the column's last item when that is a run, which the reference
+// writes without counting it (brle_gpu_4B.h:604-616).  A reserved flag byte
+// that no item follows is 0 here; the reference leaves it unwritten.
+void brle_trans4_encode_column(const uint8_t* d, uint32_t L, std::vector<uint8_t>& out) {
+    out.assign(1, 0);
+    size_t hpos = 0;
+    uint32_t items = 0;
+    uint8_t flags = 0;
+    auto put_sym = [&](uint32_t k) { out.insert(out.end(), d + 4 * k, d + 4 * k + 4); };
+    auto item_done = [&]() {
+        if (++items == 8) {
+            out[hpos] = flags;
+            flags = 0;
+            items = 0;
+            hpos = out.size();
+            out.push_back(0);
+        }
+        if (items != 0) out[hpos] = flags;
+    };
+    const uint32_t ns = L / 4;
+    uint32_t i = 0;
+    while (i < ns) {
+        uint32_t j = i + 1;
+        while (j < ns && memcmp(d + 4 * j, d + 4 * i, 4) == 0) ++j;
+        const uint32_t run = j - i;
+        const bool last = j == ns;
+        if (run >= 3) {
+            out.push_back((uint8_t)run);
+            put_sym(i);
+            if (!last) item_done();
+        } else {
+            for (uint32_t k = 0; k < run; ++k) {
+                flags |= (uint8_t)(1u << items);
+                put_sym(i);
+                item_done();
+            }
+        }
+        i = j;
+    }
+}
+
 // Columns of a chunk (column q = bytes 4q + 128k .. +3), encoded by `enc`,
 // ranked by descending length (ties by descending column), interleaved over
 // the active ranks in 4-byte words; blocks 128-byte aligned.  Shared by the
@@ -594,6 +641,22 @@ uint64_t gd_brle_trans_max_encoded_bytes(uint64_t n, uint64_t chunk_size) {
 uint64_t gd_brle_trans_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* data, uint64_t* blk_off,
                               uint64_t* col_len, uint8_t* col_map) {
     return ranked_container(in, n, chunk_size, data, blk_off, col_len, col_map, brle_trans_encode_column);
+}
+
+// The 4-byte-symbol flag container (brle::compress_gpu,
+// include/brle/brle_gpu_4B.h:640-715): brle_trans4_encode_column in the same
+// ranked 32-column layout.  The reference fixes the chunk at 8 KiB and drops
+// a partial last chunk; here any multiple of 128 up to 8 KiB is accepted and
+// the last chunk is zero padded.
+uint64_t gd_brle_trans4_max_encoded_bytes(uint64_t n, uint64_t chunk_size) {
+    uint64_t nc = n ? (n - 1) / chunk_size + 1 : 0;
+    return nc * (chunk_size + chunk_size / 16 + 32 * 8 + 256);
+}
+
+uint64_t gd_brle_trans4_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* data, uint64_t* blk_off,
+                               uint64_t* col_len, uint8_t* col_map) {
+    if (chunk_size > 8192) return 0;
+    return ranked_container(in, n, chunk_size, data, blk_off, col_len, col_map, brle_trans4_encode_column);
 }
 
 // ---------------------------------------------------------------------------

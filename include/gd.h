@@ -151,6 +151,13 @@ gd_status_t gd_brle_trans_decode(const uint8_t* d_data, const uint64_t* d_blk_of
                                  const uint8_t* d_col_map, uint32_t n_chunks, uint64_t chunk_size,
                                  uint8_t* d_out, uint64_t out_n_bytes, uint32_t* d_status,
                                  gd_stream_t stream);
+/* The 4-byte-symbol variant (brle::decompress_func, include/brle/
+ * brle_gpu_4B.h:75-223; 8 KiB chunks there): the same container, literals
+ * are 4-byte symbols and a run item is a count byte and a symbol.
+ * chunk_size a multiple of 128, at most 8192. */
+gd_status_t gd_brle_trans4_decode(const uint8_t* d_data, const uint64_t* d_blk_off, const uint64_t* d_col_len,
+                                  const uint8_t* d_col_map, uint32_t n_chunks, uint64_t chunk_size,
+                                  uint8_t* d_out, uint64_t out_n_bytes, uint32_t* d_status, gd_stream_t stream);
 
 /*
  * cuDF-compatible inflate interface (layouts of gpu_inflate_input_s and
@@ -365,6 +372,12 @@ gd_status_t gd_brle_trans_decompress(const uint8_t* in, uint64_t in_n_bytes, con
                                      uint64_t col_n_bytes, const uint8_t* col_map, uint64_t map_n_bytes,
                                      const uint64_t* blk_off, uint64_t blk_n_bytes, uint64_t chunk_size,
                                      uint8_t** out, uint64_t* out_n_bytes);
+/* brle::decompress_gpu of include/brle/brle_gpu_4B.h:717-897 (4-byte symbols),
+ * with the arrays of its side files passed in. */
+gd_status_t gd_brle_trans4_decompress(const uint8_t* in, uint64_t in_n_bytes, const uint64_t* col_len,
+                                      uint64_t col_n_bytes, const uint8_t* col_map, uint64_t map_n_bytes,
+                                      const uint64_t* blk_off, uint64_t blk_n_bytes, uint64_t chunk_size,
+                                      uint8_t** out, uint64_t* out_n_bytes);
 
 /* ------------------------------------------------------------------------
  * Encoders and generators (host; produce the containers above)
@@ -448,6 +461,11 @@ uint64_t gd_brle_trans_max_encoded_bytes(uint64_t n, uint64_t chunk_size);
 /* brle_trans::compress_gpu (include/brle/brle_trans.h:563-660). */
 uint64_t gd_brle_trans_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* data,
                               uint64_t* blk_off, uint64_t* col_len, uint8_t* col_map);
+
+uint64_t gd_brle_trans4_max_encoded_bytes(uint64_t n, uint64_t chunk_size);
+/* brle::compress_gpu of include/brle/brle_gpu_4B.h:640-715 (4-byte symbols). */
+uint64_t gd_brle_trans4_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* data,
+                               uint64_t* blk_off, uint64_t* col_len, uint8_t* col_map);
 
 uint64_t gd_deflate_max_encoded_bytes(const uint64_t* out_off, uint32_t n);
 /* zlib_chunk_compress (orig_compressor.py:44-126) with per-chunk sizes. */

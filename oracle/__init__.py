@@ -33,8 +33,9 @@ def lib():
         L.gdo_inflate.argtypes = [vp, vp, vp, vp, u32, i32, vp]
         L.gdo_lzss_contig_decode.argtypes = [vp, u64, vp, u64]
         L.gdo_brle_trans_decode.argtypes = [vp, u64, vp, vp, vp, u32, u64, vp, u64]
+        L.gdo_brle_trans4_decode.argtypes = [vp, u64, vp, vp, vp, u32, u64, vp, u64]
         for f in ("gdo_brle_decode", "gdo_rlev1_decode", "gdo_rlev2_decode", "gdo_lzss_decode", "gdo_inflate",
-                  "gdo_lzss_contig_decode", "gdo_brle_trans_decode"):
+                  "gdo_lzss_contig_decode", "gdo_brle_trans_decode", "gdo_brle_trans4_decode"):
             getattr(L, f).restype = i32
         L.gdo_rlev2_decode_stream.argtypes = [vp, u64, vp, u64]
         L.gdo_lzss_decode_stream.argtypes = [vp, u64, vp, u64]
@@ -76,6 +77,9 @@ def decode(enc) -> tuple[int, np.ndarray]:
     elif enc.codec == "brle_trans":
         rc = L.gdo_brle_trans_decode(_p(d), d.size, _p(m["blk_off"]), _p(m["col_len"]), _p(m["col_map"]),
                                      enc.n_chunks, enc.chunk_size, _p(out), enc.n_out)
+    elif enc.codec == "brle_trans4":
+        rc = L.gdo_brle_trans4_decode(_p(d), d.size, _p(m["blk_off"]), _p(m["col_len"]), _p(m["col_map"]),
+                                      enc.n_chunks, enc.chunk_size, _p(out), enc.n_out)
     elif enc.codec == "deflate":
         rc = L.gdo_inflate(_p(d), _p(m["comp_off"]), _p(m["comp_len"]), _p(m["out_off"]), enc.n_chunks,
                            enc.params["zlib_header"], _p(out))

@@ -682,6 +682,88 @@ int gdo_brle_trans_decode(const uint8_t* data, uint64_t data_len, const uint64_t
     return rc;
 }
 
+/*
+ * One column stream of the 4-byte-symbol variant (restates
+ * brle::decompress_func of include/brle/brle_gpu_4B.h:75-223): the same
+ * flag-byte grammar over 4-byte symbols -- bit 1 = one literal symbol (4
+ * bytes), bit 0 = a count byte then a symbol written count times.
+ */
+static int brle_trans4_decode_column(const uint8_t* s, uint64_t s_len, uint8_t* col, uint64_t col_bytes) {
+    uint64_t p = 0, o = 0;
+    uint32_t block = 0, head = 0;
+    while (p < s_len) {
+        uint8_t v = s[p];
+        if (block == 0) {
+            head = v;
+            block = 1;
+            ++p;
+            continue;
+        }
+        const uint32_t lit = head & 1;
+        head >>= 1;
+        if (++block == 9) block = 0;
+        uint32_t cnt = 1;
+        if (!lit) {
+            cnt = v;
+            ++p;
+        }
+        if (p + 4 > s_len) return GDO_CORRUPT;  /* an item cut short */
+        if (o + 4ull * cnt > col_bytes) return GDO_OVERRUN;
+        for (uint32_t k = 0; k < cnt; ++k, o += 4) memcpy(col + o, s + p, 4);
+        p += 4;
+    }
+    return o == col_bytes ? GDO_OK : GDO_CORRUPT;
+}
+
+/*
+ * Whole-container decode of brle_trans (sym 1) or its 4-byte-symbol variant
+ * (sym 4, brle::decompress_gpu in brle_gpu_4B.h:717-897, 8 KiB chunks in the
+ * reference): the same ranked 32-column container.
+ */
+static int brle_flag_container_decode(const uint8_t* data, uint64_t data_len, const uint64_t* blk_off,
+                                      const uint64_t* col_len, const uint8_t* col_map, uint32_t n_chunks,
+                                      uint64_t chunk_size, uint8_t* out, uint64_t out_total, int sym) {
+    if (chunk_size == 0 || chunk_size % 128) return GDO_INVALID;
+    uint64_t col_bytes = chunk_size / 32;
+    uint8_t* col = (uint8_t*)malloc(col_bytes);
+    uint8_t* tmp = (uint8_t*)malloc(chunk_size);
+    uint8_t* ranks[32];
+    uint64_t cap = 0;
+    for (uint64_t i = 0; i < 32ull * n_chunks; ++i)
+        if (col_len[i] + 8 > cap) cap = col_len[i] + 8;
+    for (int t = 0; t < 32; ++t) ranks[t] = (uint8_t*)calloc(cap, 1);
+    int rc = GDO_OK;
+    for (uint32_t c = 0; c < n_chunks && rc == GDO_OK; ++c) {
+        if (blk_off[c] > data_len) { rc = GDO_CORRUPT; break; }
+        rc = deinterleave(data + blk_off[c], data_len - blk_off[c], col_len + 32ull * c, ranks);
+        for (int r = 0; r < 32 && rc == GDO_OK; ++r) {
+            uint32_t q = col_map[32ull * c + r];
+            if (q >= 32) { rc = GDO_CORRUPT; break; }
+            rc = sym == 4 ? brle_trans4_decode_column(ranks[r], col_len[32ull * c + r], col, col_bytes)
+                          : brle_trans_decode_column(ranks[r], col_len[32ull * c + r], col, col_bytes);
+            for (uint64_t k = 0; k < col_bytes / 4 && rc == GDO_OK; ++k)
+                memcpy(tmp + 128 * k + 4 * q, col + 4 * k, 4);
+        }
+        if (rc) break;
+        uint64_t base = (uint64_t)c * chunk_size;
+        if (base < out_total) {
+            uint64_t n = out_total - base < chunk_size ? out_total - base : chunk_size;
+            memcpy(out + base, tmp, n);
+        }
+    }
+    for (int t = 0; t < 32; ++t) free(ranks[t]);
+    free(col);
+    free(tmp);
+    return rc;
+}
+
+int gdo_brle_trans4_decode(const uint8_t* data, uint64_t data_len, const uint64_t* blk_off,
+                           const uint64_t* col_len, const uint8_t* col_map, uint32_t n_chunks,
+                           uint64_t chunk_size, uint8_t* out, uint64_t out_total) {
+    return brle_flag_container_decode(data, data_len, blk_off, col_len, col_map, n_chunks, chunk_size, out,
+                                      out_total, 4);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Deflate / zlib                                                           */
 /* ------------------------------------------------------------------------ */

@@ -232,6 +232,34 @@ def test_brle_trans_patterns(cuda):
         _parity(cc.brle_trans_encode(raw, 4096), raw, cuda)
 
 
+def _word_runs(seed, n):
+    rng = np.random.default_rng(seed)
+    words = np.repeat(rng.integers(0, 6, n // 40 + 1), rng.integers(1, 20, n // 40 + 1)).astype(np.uint32)
+    return np.resize(words, (n + 3) // 4).view(np.uint8)[:n].copy()
+
+
+@pytest.mark.parametrize("n,chunk", [(8192 * 300, 8192), (8192 * 5 + 100, 8192), (4096 * 33, 4096), (128 * 50, 128)])
+def test_brle_trans4(cuda, n, chunk):
+    _parity(cc.brle_trans4_encode(_word_runs(n, n), chunk), _word_runs(n, n), cuda)
+    rng = np.random.default_rng(n)
+    for raw in [np.zeros(n, np.uint8), rng.integers(0, 256, n).astype(np.uint8)]:
+        _parity(cc.brle_trans4_encode(raw, chunk), raw, cuda)
+
+
+def test_brle_trans4_host_api_and_corruption(cuda):
+    raw = _word_runs(3, 8192 * 40 + 17)
+    out = cc.decode_host(cc.brle_trans4_encode(raw, 8192))
+    # like the reference's decompress_gpu, the host call returns whole chunks
+    # (the last one zero-padded)
+    assert out.size == 8192 * 41 and np.array_equal(out[:raw.size], raw) and not out[raw.size:].any()
+    e = cc.brle_trans4_encode(raw, 8192)
+    e.meta["col_len"][0] -= 1  # truncated rank-0 stream: an item cut short
+    _expect_error(e, cuda)
+    e = cc.brle_trans4_encode(raw, 8192)
+    e.meta["col_map"][1] = e.meta["col_map"][0]  # not a permutation
+    _expect_error(e, cuda)
+
+
 def test_new_containers_host_api(cuda):
     raw = cc.gen_markov_copy(8, 5 * 65536 + 333, 4096)
     assert np.array_equal(cc.decode_host(cc.lzss_contig_encode(raw, 65536)), raw)

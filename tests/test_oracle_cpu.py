@@ -164,6 +164,129 @@ def test_brle_trans_column_grammar():
     assert rc == 0 and np.array_equal(out, raw)
 
 
+def _sym_column_chunk(col: np.ndarray) -> np.ndarray:
+    """An 8 KiB chunk whose column 0 holds `col` (256 bytes); the other
+    columns are zero."""
+    raw = np.zeros(8192, np.uint8)
+    for k in range(64):
+        raw[128 * k:128 * k + 4] = col[4 * k:4 * k + 4]
+    return raw
+
+
+@pytest.mark.parametrize("n,chunk", [(8192 * 20, 8192), (8192 * 3 + 1000, 8192), (4096 * 9, 4096), (128 * 5, 128)])
+def test_brle_trans4_roundtrip(n, chunk):
+    rng = np.random.default_rng(n)
+    # 4-byte symbols: runs of equal words, as a column of int32 values sees them
+    words = np.repeat(rng.integers(0, 6, n // 40 + 1), rng.integers(1, 20, n // 40 + 1)).astype(np.uint32)
+    raw = np.resize(words, (n + 3) // 4).view(np.uint8)[:n].copy()
+    _roundtrip(cc.brle_trans4_encode(raw, chunk), raw)
+    raw = rng.integers(0, 256, n).astype(np.uint8)
+    _roundtrip(cc.brle_trans4_encode(raw, chunk), raw)
+
+
+def test_brle_trans4_column_grammar():
+    # column 0 (64 symbols): 5 x A, 2 x B, 56 x C, 1 x D, as the reference's
+    # compress_func writes it (brle_gpu_4B.h:321-638): flag byte, run item
+    # (count, symbol), literal items (symbol), flag bits LSB first
+    A, B, C, D = (np.frombuffer(x, np.uint8) for x in (b"AAAA", b"BBBB", b"CCCC", b"DDDD"))
+    col = np.concatenate([A] * 5 + [B] * 2 + [C] * 56 + [D])
+    e = cc.brle_trans4_encode(_sym_column_chunk(col), 8192)
+    r = int(np.nonzero(e.meta["col_map"][:32] == 0)[0][0])
+    n = int(e.meta["col_len"][r])
+    lanes, off = oracle.export_lanes(cc.Encoded("lzss", e.data, e.n_out, e.n_chunks, e.chunk_size, e.meta, {}))
+    stream = lanes[off[r]:off[r + 1]]
+    want = np.concatenate([[0b10110], [5], A, B, B, [56], C, D]).astype(np.uint8)
+    assert n == want.size and np.array_equal(stream, want)
+    rc, out = oracle.decode(e)
+    assert rc == 0 and np.array_equal(out, _sym_column_chunk(col))
+
+
+def test_brle_trans4_group_ends():
+    A = np.frombuffer(b"\x01\x02\x03\x04", np.uint8)
+    B = np.frombuffer(b"\x05\x06\x07\x08", np.uint8)
+    # 8 literal items end a group: a reserved flag byte follows the last one
+    lit = np.concatenate([np.full(4, i, np.uint8) for i in range(1, 9)])
+    col = np.concatenate([lit, np.tile(np.concatenate([A, B]), 28)])
+    e = cc.brle_trans4_encode(_sym_column_chunk(col), 8192)
+    rc, out = oracle.decode(e)
+    assert rc == 0 and np.array_equal(out, _sym_column_chunk(col))
+    # 7 literal items then a final run: the run closes the group with no
+    # reserved flag byte after it (the reference writes the last run uncounted)
+    col = np.concatenate([np.concatenate([np.full(4, i, np.uint8) for i in range(1, 8)]), np.tile(A, 57)])
+    e = cc.brle_trans4_encode(_sym_column_chunk(col), 8192)
+    r = int(np.nonzero(e.meta["col_map"][:32] == 0)[0][0])
+    assert int(e.meta["col_len"][r]) == 1 + 7 * 4 + 5
+    rc, out = oracle.decode(e)
+    assert rc == 0 and np.array_equal(out, _sym_column_chunk(col))
+
+
+def _ref_compress_func_4B(col: np.ndarray) -> bytes:
+    """brle::compress_func of include/brle/brle_gpu_4B.h:321-638 for one
+    column, restated loop for loop over an output zeroed beforehand (the
+    reference's output buffer is not cleared: a reserved flag byte that no
+    item follows keeps whatever was there)."""
+    syms = [bytes(col[4 * k:4 * k + 4]) for k in range(col.size // 4)]
+    out = bytearray(col.size * 2 + 16)
+    pos = 1                    # byte_offset: header byte 0 reserved
+    hdr, header, blocks = 0, 0, 0
+    counter, prev = 0, None
+
+    def item_done():
+        nonlocal blocks, header, hdr, pos
+        blocks += 1
+        if blocks == 8:
+            out[hdr] = header
+            header = 0
+            hdr = pos
+            pos += 1
+            blocks = 0
+        if blocks != 0:
+            out[hdr] = header
+
+    def put(bs):
+        nonlocal pos
+        out[pos:pos + len(bs)] = bs
+        pos += len(bs)
+
+    for v in syms:
+        if counter == 0:
+            prev = v
+        if prev == v:
+            counter += 1
+            continue
+        if counter >= 3:
+            put(bytes([counter]) + prev)
+            item_done()
+        else:
+            for _ in range(counter):
+                header |= 1 << blocks
+                put(prev)
+                item_done()
+        counter, prev = 1, v
+    if counter >= 3:           # the last run: written, not counted
+        put(bytes([counter]) + prev)
+    else:
+        for _ in range(counter):
+            header |= 1 << blocks
+            put(prev)
+            item_done()
+    return bytes(out[:pos])
+
+
+def test_brle_trans4_encoder_matches_reference_writer():
+    rng = np.random.default_rng(44)
+    L = cc.lib()
+    for trial in range(300):
+        k = int(rng.integers(1, 5))
+        words = np.repeat(rng.integers(0, k, 64), rng.integers(1, 12, 64))[:64]
+        words = np.resize(words, 64).astype(np.uint32) * 0x01010101
+        col = words.view(np.uint8)
+        e = cc.brle_trans4_encode(_sym_column_chunk(col), 8192)
+        r = int(np.nonzero(e.meta["col_map"][:32] == 0)[0][0])
+        lanes, off = oracle.export_lanes(cc.Encoded("lzss", e.data, e.n_out, e.n_chunks, e.chunk_size, e.meta, {}))
+        assert bytes(lanes[off[r]:off[r + 1]]) == _ref_compress_func_4B(col), trial
+
+
 def test_new_containers_reject_corruption():
     raw = cc.gen_markov_copy(5, 20000, 4096)
     e = cc.lzss_contig_encode(raw, 8192)
