@@ -5,10 +5,11 @@
 // up to RCAP runs per stream:
 //   * parse: lane 0 of warp w walks stream w's run boundaries (the only
 //     serial part of the format: a run's byte length follows from its first
-//     header bytes), recording each run's header offset and first value
-//     index; then the warp's lanes decode the recorded headers -- kind,
-//     widths, bit offset of the packed data, base, delta -- into the warp's
-//     shared-memory run table.  After the copy into shared memory the warps
+//     header bytes), recording each run's header offset; then the warp's
+//     lanes decode the recorded headers -- kind, length, widths, bit offset
+//     of the packed data, base, delta -- into the warp's shared-memory run
+//     table, and a warp prefix sum of the lengths gives each run's first
+//     value.  After the copy into shared memory the warps
 //     of a block never wait on each other, so one warp's walk overlaps the
 //     others' expansion;
 //   * expand: warp w produces the values of stream w, 32 consecutive values
@@ -45,7 +46,7 @@ struct RunTab {
     uint64_t base[LANES_PER_BLOCK][RCAP];
     uint64_t aux[LANES_PER_BLOCK][RCAP];
     uint8_t prun[LANES_PER_BLOCK][RCAP];  // PATCHED_BASE runs with patch entries
-    uint32_t nr[LANES_PER_BLOCK], npr[LANES_PER_BLOCK], err[LANES_PER_BLOCK];
+    uint32_t nr[LANES_PER_BLOCK], npr[LANES_PER_BLOCK];
 };
 
 __device__ __forceinline__ uint64_t shfl_up64(uint64_t v, uint32_t o) {
@@ -244,33 +245,23 @@ __global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
     // parser state: lane 0 of warp w walks stream w, so the walks of a
     // block's streams run on different warps (no divergence between streams,
     // no block barrier: after the copy above each warp runs on its own)
-    uint32_t p_pos = 0, p_g = 0, p_err = ST_OK;
+    uint32_t p_pos = 0, p_err = ST_OK;
     const uint32_t plen = s_len[t];
     uint32_t vbeg = 0;  // first value of this warp's current batch
     uint32_t werr = ST_OK;
 
     for (;;) {
-        // ---- parse 1: run boundaries (lane 0) ----
+        // ---- parse 1: run header positions (lane 0) ----
+        // Only the positions: a SHORT_REPEAT run's size is in its first byte,
+        // the others' in their first 4 (DELTA: the ends of two varints).
+        // Run lengths, value starts and all validation come in parse 2.
         if (lane == 0) {
             uint32_t nr = 0;
-            while (p_err == ST_OK && p_g < nv && nr < (uint32_t)RCAP) {
-                // SHORT_REPEAT (most runs): length and size from the first byte
-                const uint32_t h0 = p_pos < plen ? sbuf[p_pos] : 0xffu;
+            while (p_pos < plen && nr < (uint32_t)RCAP) {
+                const uint32_t h0 = sbuf[p_pos];
                 if (h0 < 64u) {
-                    const uint32_t next = p_pos + 2u + ((h0 >> 3) & 7u), rl = (h0 & 7u) + 3u;
-                    if (next > plen) {
-                        p_err = ST_CORRUPT;
-                        break;
-                    }
-                    if (p_g + rl > nv) {
-                        p_err = ST_OVERRUN;
-                        break;
-                    }
-                    R.vs[wid][nr] = p_g;
-                    R.pos[wid][nr] = p_pos;
-                    ++nr;
-                    p_pos = next;
-                    p_g += rl;
+                    R.pos[wid][nr++] = p_pos;
+                    p_pos += 2u + ((h0 >> 3) & 7u);
                     continue;
                 }
                 const Skip k = skip_run(sbuf, p_pos, plen);
@@ -278,41 +269,49 @@ __global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
                     p_err = k.err;
                     break;
                 }
-                if (p_g + k.len > nv) {
-                    p_err = ST_OVERRUN;
-                    break;
-                }
-                R.vs[wid][nr] = p_g;
-                R.pos[wid][nr] = p_pos;
-                ++nr;
+                R.pos[wid][nr++] = p_pos;
                 p_pos = k.next;
-                p_g += k.len;
             }
-            // the stream must end exactly with its last run
-            if (p_err == ST_OK && p_g == nv && p_pos != plen) p_err = ST_CORRUPT;
-            R.vs[wid][nr] = p_g;
             R.nr[wid] = nr;
             R.npr[wid] = 0;
-            R.err[wid] = p_err;
         }
         __syncwarp();
-        // ---- parse 2: decode the recorded headers, one run per lane ----
-        {
-            const uint32_t nrp = R.nr[wid];
-            for (uint32_t ri = lane; ri < nrp; ri += 32) {
+        // ---- parse 2: decode the recorded headers, one run per lane; run
+        // starts are a warp prefix sum of the lengths ----
+        const uint32_t nr = R.nr[wid];
+        uint32_t perr = ST_OK, carry = vbeg;
+        for (uint32_t b0 = 0; b0 < nr; b0 += 32) {
+            const uint32_t ri = b0 + lane;
+            uint32_t rl = 0;
+            if (ri < nr) {
                 const Run r = parse_fast(sbuf, R.pos[wid][ri], plen);
+                if (r.err != ST_OK) perr = r.err;
+                rl = r.len;
                 R.meta[wid][ri] = r.kind | (r.fbw << 2) | (r.flags << 9) | (r.pll << 11) | (r.pw << 16) | (r.cfb << 23);
                 R.vbit[wid][ri] = r.vbit;
                 R.base[wid][ri] = r.base;
                 R.aux[wid][ri] = r.kind == 2 ? (uint64_t)r.pbit : r.delta;
                 if (r.kind == 2 && r.pll) R.prun[wid][atomicAdd(&R.npr[wid], 1u)] = (uint8_t)ri;
             }
+            const uint32_t inc = warp_incl_scan(rl);
+            if (ri < nr) R.vs[wid][ri] = carry + inc - rl;
+            carry += __shfl_sync(GD_FULL_MASK, inc, 31);
         }
+        // the batch's status: a header that runs past the stream, values
+        // past the stream's nv, or a stream that ends short of nv values
+        const uint32_t pos_now = __shfl_sync(GD_FULL_MASK, p_pos, 0);
+        uint32_t berr = max(__reduce_max_sync(GD_FULL_MASK, perr), __shfl_sync(GD_FULL_MASK, p_err, 0));
+        if (berr == ST_OK && carry > nv) berr = ST_OVERRUN;
+        if (berr == ST_OK && pos_now >= plen && (pos_now != plen || carry != nv)) berr = ST_CORRUPT;
+        if (lane == 0) R.vs[wid][nr] = carry;
         __syncwarp();
+        if (berr != ST_OK) {
+            werr = berr;
+            break;
+        }
 
         // ---- expand: values [vbeg, vend) of stream t, 32 per round ----
-        const uint32_t nr = R.nr[wid];
-        const uint32_t vend = R.vs[wid][nr];
+        const uint32_t vend = carry;
         int rcur = -1;              // run holding the value before this round
         int cr_run = -2;            // run whose delta sum is carried in cr_acc
         uint64_t cr_acc = 0;
@@ -409,11 +408,9 @@ __global__ void __launch_bounds__(LANES_PER_BLOCK * 32) decode_kernel(
         }
         vbeg = vend;
         __syncwarp();  // the next batch rewrites this warp's run tables
-        const bool more = lane == 0 && p_err == ST_OK && p_g < nv;
-        if (!__any_sync(GD_FULL_MASK, more)) break;
+        if (pos_now >= plen) break;  // the stream is consumed (and held exactly nv values)
     }
-    const uint32_t err = max(werr, R.err[wid]);
-    if (lane == 0 && err != ST_OK && status) atomicMax(status + chunk, err);
+    if (lane == 0 && werr != ST_OK && status) atomicMax(status + chunk, werr);
 }
 
 }  // namespace rlev2
