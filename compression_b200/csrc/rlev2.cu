@@ -30,7 +30,7 @@
 namespace gd {
 namespace rlev2 {
 
-constexpr int RCAP = 64;  // runs per stream per batch
+constexpr int RCAP = 32;  // runs per stream per batch (small run tables: 8 blocks per SM fit)
 
 // Run tables of one batch (structure of arrays, one row per stream);
 // LANES_PER_BLOCK = warps per block = lane streams per block (4 default, 8
