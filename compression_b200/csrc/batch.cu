@@ -31,7 +31,7 @@ __host__ __device__ constexpr uint32_t warp_smem_bytes(uint32_t max_lane) {
     // union of the per-codec warp workspaces
     uint32_t a = (uint32_t)sizeof(BatchInflSmem);
     uint32_t b = lzss::WARP_SMEM;
-    uint32_t c = (uint32_t)sizeof(SegTable) + ((max_lane + 15u) & ~15u) + 160u;
+    uint32_t c = (uint32_t)sizeof(SegTable) + ((max_lane + 15u) & ~15u) + 160u + (uint32_t)sizeof(rlev2::WarpRuns);
     uint32_t d = brlew::WARP_SMEM;
     uint32_t m = a > b ? a : b;
     m = m > c ? m : c;
@@ -88,7 +88,10 @@ __device__ uint32_t rle_task(const gd_task& t, uint32_t max_lane, uint8_t* ws) {
         const uint32_t ru = t.param;
         if (ru == 0 || t.chunk_size % (256ull * ru) || (reinterpret_cast<uintptr_t>(t.dst) & 7u)) return ST_INVALID;
         const uint32_t nv = (uint32_t)(t.chunk_size / 256u);
-        return rlev2::lane_warp(sbuf, my_len, nv, slot, ru, reinterpret_cast<uint64_t*>(t.dst), t.dst_len / 8);
+        // the run table sits past the stream's slot and its 160-byte tail
+        auto* runs = reinterpret_cast<rlev2::WarpRuns*>(sbuf + ((max_lane + 15u) & ~15u) + 160u);
+        return rlev2::decode_stream(sbuf, my_len, nv, slot, ru, reinterpret_cast<uint64_t*>(t.dst), t.dst_len / 8,
+                                    *runs);
     }
     const uint32_t eb = t.param >> 16, wil = t.param & 0xffffu;
     if (!(eb == 4 || eb == 8) || wil == 0 || t.chunk_size % (32ull * wil * eb) ||
