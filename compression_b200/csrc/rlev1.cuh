@@ -15,8 +15,10 @@
 //   * runs are closed form: lane i writes base + i*delta;
 //   * a literal group is decoded 32 values at a time: the lanes load a
 //     128-byte window, ballot the varint terminators (bytes < 0x80), and lane
-//     j finds the j-th terminator with a select over the 128-bit mask, so
-//     every lane knows where its varint starts and ends and decodes it alone.
+//     j finds the j-th terminator (the mask quarter by comparison with the
+//     quarters' prefix counts, then one select), so every lane knows where
+//     its varint starts and ends and decodes it alone (32-bit values: one
+//     funnel-shifted word and a fifth byte, compacted with masks).
 #pragma once
 #include "interleave.cuh"
 
@@ -32,19 +34,6 @@ __host__ __device__ constexpr uint32_t stream_cap(uint32_t nv, uint32_t eb) {
 
 // Shared-memory bytes reserved for a lane stream of at most `n` bytes.
 __host__ __device__ constexpr uint32_t lane_cap(uint32_t n) { return ((n + 15u) & ~15u) + 144u; }
-
-// index (0-based) of the n-th set bit of the 128-bit mask m[0..3] (n < popc)
-__device__ __forceinline__ uint32_t select128(const uint32_t m[4], uint32_t n) {
-    uint32_t base = 0;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const uint32_t c = __popc(m[q]);
-        if (n < c) return base + __fns(m[q], 0, (int)n + 1);
-        n -= c;
-        base += 32;
-    }
-    return 0xffffffffu;
-}
 
 // Decode one lane stream (sbuf[0..len), readable 144 bytes past len) of nv
 // elements of type T with the calling warp.  Lane stream t with wil = values
@@ -123,20 +112,41 @@ static __device__ __noinline__ uint32_t lane_warp(const uint8_t* __restrict__ sb
                 const bool term = (bpos < len) && !(sbuf[bpos] & 0x80u);
                 m[q] = __ballot_sync(GD_FULL_MASK, term);
             }
-            const uint32_t nterm = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
+            const uint32_t c0 = __popc(m[0]), c01 = c0 + __popc(m[1]), c012 = c01 + __popc(m[2]);
+            const uint32_t nterm = c012 + __popc(m[3]);
             if (nterm == 0) {  // no varint ends within 128 bytes (or the stream ran out)
                 err = ST_CORRUPT;
                 break;
             }
             const uint32_t take = min(min(rem, nterm), 32u);
-            const uint32_t end = lane < take ? select128(m, lane) : 0u;
+            // lane j's varint ends at the j-th terminator: its 32-bit quarter
+            // of the mask by comparison, then one select within it
+            uint32_t end = 0;
+            if (lane < take) {
+                const uint32_t q = (lane >= c0) + (lane >= c01) + (lane >= c012);
+                const uint32_t mq = q == 0 ? m[0] : (q == 1 ? m[1] : (q == 2 ? m[2] : m[3]));
+                const uint32_t nq = lane - (q == 0 ? 0u : (q == 1 ? c0 : (q == 2 ? c01 : c012)));
+                end = 32u * q + __fns(mq, 0, (int)nq + 1);
+            }
             const uint32_t prev = __shfl_up_sync(GD_FULL_MASK, end, 1);  // the previous varint's last byte
             if (lane < take) {
                 const uint32_t beg = lane ? prev + 1 : 0;
                 uint64_t v = 0;
-                uint32_t sh = 0;
-                for (uint32_t k = beg; k <= end; ++k, sh += 7)
-                    if (sh < 64) v |= (uint64_t)(sbuf[p + k] & 0x7fu) << sh;
+                if constexpr (sizeof(T) == 4) {
+                    // a 32-bit value takes the varint's first 5 bytes: the
+                    // first 4 by one funnel-shifted word, 7 bits apiece
+                    const uint32_t a = p + beg, n = end - beg + 1;
+                    const uint32_t* wp = reinterpret_cast<const uint32_t*>(sbuf + (a & ~3u));
+                    uint32_t lo = __funnelshift_r(wp[0], wp[1], 8u * (a & 3u));
+                    if (n < 4) lo &= (1u << (8u * n)) - 1u;
+                    const uint32_t hi = n >= 5 ? (uint32_t)sbuf[a + 4] : 0u;
+                    v = (lo & 0x7fu) | ((lo >> 1) & 0x3f80u) | ((lo >> 2) & 0x1fc000u) | ((lo >> 3) & 0xfe00000u) |
+                        (hi << 28);
+                } else {
+                    uint32_t sh = 0;
+                    for (uint32_t k = beg; k <= end; ++k, sh += 7)
+                        if (sh < 64) v |= (uint64_t)(sbuf[p + k] & 0x7fu) << sh;
+                }
                 put(g + lane, v);
             }
             p += __shfl_sync(GD_FULL_MASK, end, take - 1) + 1;
