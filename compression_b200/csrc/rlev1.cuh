@@ -47,10 +47,13 @@ static __device__ __noinline__ uint32_t lane_warp(const uint8_t* __restrict__ sb
     // reference's configurations): shifts instead of a division per value
     const bool pow2 = (wil & (wil - 1u)) == 0u;
     const uint32_t wsh = __ffs(wil) - 1u;
-    auto put = [&](uint32_t e, uint64_t v) {
-        const uint64_t oe = pow2 ? ((uint64_t)(e >> wsh) << (wsh + 5u)) + ((uint64_t)t << wsh) + (e & (wil - 1u))
-                                 : (uint64_t)(e / wil) * 32u * wil + (uint64_t)t * wil + (e % wil);
-        if (oe < want) outv[oe] = (T)v;
+    // a chunk holds at most 2^31 bytes, so element indices fit in 32 bits
+    const uint32_t want32 = want < 0xffffffffull ? (uint32_t)want : 0xffffffffu;
+    const uint32_t tw = t << wsh;
+    auto put = [&](uint32_t e, T v) {
+        const uint32_t oe = pow2 ? ((e >> wsh) << (wsh + 5u)) + tw + (e & (wil - 1u))
+                                 : (e / wil) * 32u * wil + t * wil + (e % wil);
+        if (oe < want32) outv[oe] = v;
     };
     uint32_t err = ST_OK, pos = 0, g = 0;
     while (g < nv) {
@@ -96,8 +99,8 @@ static __device__ __noinline__ uint32_t lane_warp(const uint8_t* __restrict__ sb
             err = ST_OVERRUN;
             break;
         }
-        if (kind == 0) {  // run: closed form
-            for (uint32_t i = lane; i < cnt; i += 32) put(g + i, base + (uint64_t)i * delta);
+        if (kind == 0) {  // run: closed form (in T's width: the low bits of base + i*delta)
+            for (uint32_t i = lane; i < cnt; i += 32) put(g + i, (T)base + (T)i * (T)delta);
             g += cnt;
             pos = next;
             continue;
@@ -147,7 +150,7 @@ static __device__ __noinline__ uint32_t lane_warp(const uint8_t* __restrict__ sb
                     for (uint32_t k = beg; k <= end; ++k, sh += 7)
                         if (sh < 64) v |= (uint64_t)(sbuf[p + k] & 0x7fu) << sh;
                 }
-                put(g + lane, v);
+                put(g + lane, (T)v);
             }
             p += __shfl_sync(GD_FULL_MASK, end, take - 1) + 1;
             g += take;
