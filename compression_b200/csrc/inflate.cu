@@ -185,6 +185,7 @@ gd_status_t launch_inflate(const Chunks& ch, uint32_t n, int zlib_hdr, const uin
         case 11: return launch_pair<Chunks, 8192, 1, 1024, 8, 512, 64>(ch, n, zlib_hdr, order, s);
         case 12: return launch_pair<Chunks, 4096, 1, 1024, 8, 512, 64>(ch, n, zlib_hdr, order, s);
         case 13: return launch_pair<Chunks, 4096, 2, 1024, 8, 512, 64>(ch, n, zlib_hdr, order, s);
+        case 14: return launch_pair<Chunks, 2048, 1, 1024, 8, 512, 64>(ch, n, zlib_hdr, order, s);
         default: return launch_pair<Chunks, 32768, 1>(ch, n, zlib_hdr, order, s);
     }
 }

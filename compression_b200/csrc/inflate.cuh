@@ -457,7 +457,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
     static_assert(RB >= 1024 && (RB & (RB - 1)) == 0, "input ring: a power of two >= 1 KiB");
     // a window below the Deflate window's 32 KiB serves the nearer copies;
     // the executor reads farther ones from the output
-    static_assert(WIN == 0 || (WIN >= 4096 && (WIN & (WIN - 1)) == 0), "window: 0 or a power of two >= 4 KiB");
+    static_assert(WIN == 0 || (WIN >= 2048 && (WIN & (WIN - 1)) == 0), "window: 0 or a power of two >= 2 KiB");
     const uint32_t lane = lane_id();
     uint32_t err = ST_OK;
     // input ring: compressed byte i (chunk-relative) at ring[(i + sh) % RB];

@@ -273,7 +273,7 @@ typedef enum gd_tune_key {
                                     9 / 10: 8 / 4 KiB window; 11 / 12: 8 / 4 KiB window with a
                                     1 KiB ring and batches of 512 literals / 64 commands;
                                     13: as 12, 2 pairs per block (copies beyond the window
-                                    read the output);
+                                    read the output); 14: as 12 with a 2 KiB window;
                                     0 (default): 12 for >= 4 streams per SM, else 6 */
     GD_TUNE_BRLE_BLOCKS_PER_SM = 1,   /* byte-RLE grid = value x SMs blocks (default 8) */
     GD_TUNE_RLEV1_LANES_PER_BLOCK = 2, /* 0/8: 8 lane streams per block; 4: 4 */

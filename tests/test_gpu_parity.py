@@ -349,7 +349,7 @@ def test_lzss_token_shapes(cuda, knob, chunk):
     assert np.array_equal(out, ref)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14])
 def test_inflate_variants(cuda, variant):
     """Every inflate kernel shape on streams of mixed size with dynamic,
     fixed-Huffman and stored blocks, against zlib."""
