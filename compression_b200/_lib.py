@@ -72,6 +72,10 @@ SIGNATURES = {
     "gd_rlev1_encode_device": (i32, [vp, u64, u64, u32, u32, vp, vp, vp, vp, vp, vp]),
     "gd_rlev2_encode_bound": (u64, [u64, u64]),
     "gd_rlev2_encode_device": (i32, [vp, u64, u64, u32, vp, vp, vp, vp, vp, vp]),
+    "gd_brle_compress": (i32, [vp, u64, vp, vp]),
+    "gd_rlev1_compress": (i32, [vp, u64, u32, u32, u64, vp, vp, vp, vp, vp]),
+    "gd_rlev2_compress": (i32, [vp, u64, u32, u64, vp, vp, vp, vp, vp]),
+    "gd_lzss_compress": (i32, [vp, u64, vp, vp, vp, vp, vp]),
     "gd_lzss_max_encoded_bytes": (u64, [u64, u64]),
     "gd_lzss_encode": (u64, [vp, u64, u64, vp, vp, vp, vp]),
     "gd_lzss_encode_stream": (u64, [vp, u32, vp, u64]),

@@ -360,6 +360,68 @@ def encode_gpu(codec: str, raw, chunk_size: int, *, comp_col_len: int = 128, ele
     return Encoded(codec, data, b.size, nc, chunk_size, meta, params)
 
 
+def _take(ptr: C.c_void_p, n: int, dtype=np.uint8) -> np.ndarray:
+    """Copy a library-owned host buffer into numpy and release it (gd_free)."""
+    a = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint8)), shape=(n,)).copy() if n else np.empty(0, np.uint8)
+    lib().gd_free(ptr)
+    return a.view(dtype)
+
+
+def compress_host(codec: str, raw, chunk_size: int = 0, *, comp_col_len: int = 128, elem_bytes: int = 4,
+                  read_unit: int = 32) -> Encoded:
+    """The reference-shaped synchronous compress call (H2D, device encoder,
+    D2H) via the C ABI: gd_brle_compress (256 KiB chunks, brle::compress_gpu),
+    gd_rlev1_compress (rle_v1::compress_gpu), gd_rlev2_compress
+    (rlev2::compress_gpu_transpose; the Encoded keeps the encoded size in
+    blk_off[-1], as the host encoder's does) or gd_lzss_compress (128 KiB
+    chunks, lzss::compress_gpu).  chunk_size applies to RLE v1 / v2."""
+    b = _as_u8(raw)
+    L = lib()
+    out, n = C.c_void_p(), C.c_uint64()
+    if codec == "brle":
+        check(L.gd_brle_compress(_p(b), b.size, C.byref(out), C.byref(n)), "gd_brle_compress")
+        cont = _take(out, n.value)
+        n_ptr = int(cont[:4].view(np.uint32)[0])
+        ptr = cont[4:4 + 8 * n_ptr].copy().view(np.uint64)
+        hdr = 4 + 8 * n_ptr + 8
+        return Encoded("brle", cont[hdr:].copy(), b.size, n_ptr - 1, BRLE_CHUNK, {"ptr": ptr}, {"container": cont})
+    if codec == "lzss":
+        meta, lens, num = C.c_void_p(), C.c_void_p(), C.c_uint64()
+        check(L.gd_lzss_compress(_p(b), b.size, C.byref(out), C.byref(n), C.byref(meta), C.byref(lens),
+                                 C.byref(num)), "gd_lzss_compress")
+        data = _take(out, n.value)
+        ptrs = C.cast(meta, C.POINTER(C.c_void_p))
+        ln = np.ctypeslib.as_array(C.cast(lens, C.POINTER(C.c_uint64)), shape=(num.value,)).copy()
+        blobs = [_take(C.c_void_p(ptrs[i]), int(ln[i])) for i in range(num.value)]
+        L.gd_free(meta)
+        L.gd_free(lens)
+        cs = int(blobs[0].view(np.uint64)[0])
+        m = {"blk_off": blobs[1].view(np.uint64), "col_len": blobs[2].view(np.uint64), "col_map": blobs[3]}
+        return Encoded("lzss", data, b.size, m["blk_off"].size - 1, cs, m, {})
+    col, blk, nc = C.c_void_p(), C.c_void_p(), C.c_uint64()
+    if codec == "rlev1":
+        check(L.gd_rlev1_compress(_p(b), b.size, comp_col_len, elem_bytes, chunk_size, C.byref(out), C.byref(n),
+                                  C.byref(col), C.byref(blk), C.byref(nc)), "gd_rlev1_compress")
+        cont = _take(out, n.value)
+        params = {"comp_col_len": comp_col_len, "elem_bytes": elem_bytes, "container": cont}
+        data = cont[8:].copy()
+    elif codec == "rlev2":
+        check(L.gd_rlev2_compress(_p(b), b.size, read_unit, chunk_size, C.byref(out), C.byref(n), C.byref(blk),
+                                  C.byref(col), C.byref(nc)), "gd_rlev2_compress")
+        data = _take(out, n.value)
+        params = {"read_unit": read_unit}
+    else:
+        raise ValueError(f"no compress call for {codec}")
+    k = nc.value
+    bo = _take(blk, 8 * (k + 1), np.uint64)
+    if codec == "rlev2":
+        assert int(bo[-1]) == b.size  # the reference keeps the column's size there
+        bo = bo.copy()
+        bo[-1] = data.size
+    return Encoded(codec, data, b.size, k, chunk_size, {"blk_off": bo, "col_len": _take(col, 8 * 32 * k, np.uint64)},
+                   params)
+
+
 # --------------------------------------------------------------------------
 # device jobs
 # --------------------------------------------------------------------------

@@ -620,6 +620,226 @@ gd_status_t gd_inflate_decompress(const uint8_t* in, uint64_t in_n_bytes, const 
 
 }  // extern "C"
 
+// ---------------------------------------------------------------------------
+// Host compress calls on the device encoders: the column is copied in,
+// encoded on the device and the container and its metadata copied back.
+// Their own grow-only pool, so interleaved compress and decompress calls do
+// not resize each other's staging buffers.
+namespace {
+thread_local Pool g_epool;
+
+struct EncBufs {
+    uint8_t* in;
+    uint8_t* scratch;
+    uint8_t* data;
+    uint64_t* blk_off;
+    uint64_t* col_len;
+    uint8_t* col_map;
+    uint32_t* st;
+};
+
+// Stage the column and size the interleaved encoders' buffers for nc chunks.
+gd_status_t enc_stage(const uint8_t* in, uint64_t n, uint64_t nc, uint64_t bound, EncBufs& b, cudaStream_t s) {
+    b.in = (uint8_t*)g_epool.get(0, n);
+    b.scratch = (uint8_t*)g_epool.get(1, bound);
+    b.data = (uint8_t*)g_epool.get(2, bound);
+    b.blk_off = (uint64_t*)g_epool.get(3, 8 * (nc + 1));
+    b.col_len = (uint64_t*)g_epool.get(4, 8 * 32 * nc);
+    b.col_map = (uint8_t*)g_epool.get(5, 32 * nc);
+    b.st = (uint32_t*)g_epool.get(6, 4 * nc);
+    if (!b.in || !b.scratch || !b.data || !b.blk_off || !b.col_len || !b.col_map || !b.st) return GD_ERR_NOMEM;
+    return cudaMemcpyAsync(b.in, in, n, cudaMemcpyHostToDevice, s) == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+}
+
+// After the encoder: its status, then blk_off and col_len (and col_map) into
+// malloc'd arrays and the blk_off[nc] data bytes into a pinned buffer at
+// offset `at` (the caller fills the first `at` bytes).
+gd_status_t enc_fetch(const EncBufs& b, uint64_t nc, uint64_t at, cudaStream_t s, uint8_t** data, uint64_t* data_n,
+                      uint64_t** blk_off, uint64_t** col_len, uint8_t** col_map) {
+    gd_status_t r = collect(b.st, (uint32_t)nc, s);
+    if (r != GD_OK) return r;
+    uint64_t* bo = (uint64_t*)malloc(8 * (nc + 1));
+    uint64_t* cl = (uint64_t*)malloc(8 * 32 * nc);
+    uint8_t* cm = col_map ? (uint8_t*)malloc(32 * nc) : nullptr;
+    uint8_t* h = nullptr;
+    bool ok = bo && cl && (!col_map || cm);
+    ok = ok && cudaMemcpyAsync(bo, b.blk_off, 8 * (nc + 1), cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(cl, b.col_len, 8 * 32 * nc, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    ok = ok && (!cm || cudaMemcpyAsync(cm, b.col_map, 32 * nc, cudaMemcpyDeviceToHost, s) == cudaSuccess);
+    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+    if (ok) {
+        h = (uint8_t*)pinned().get(at + bo[nc]);
+        ok = h && cudaMemcpyAsync(h + at, b.data, bo[nc], cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+             cudaStreamSynchronize(s) == cudaSuccess;
+    }
+    if (!ok) {
+        free(bo);
+        free(cl);
+        free(cm);
+        if (h) gd_free(h);
+        return GD_ERR_CUDA;
+    }
+    *data = h;
+    *data_n = at + bo[nc];
+    *blk_off = bo;
+    *col_len = cl;
+    if (col_map) *col_map = cm;
+    return GD_OK;
+}
+}  // namespace
+
+extern "C" {
+
+gd_status_t gd_brle_compress(const uint8_t* in, uint64_t in_n_bytes, uint8_t** out, uint64_t* out_n_bytes) {
+    if (!in || !out || !out_n_bytes || in_n_bytes == 0) return GD_ERR_INVALID_ARG;
+    *out = nullptr;
+    *out_n_bytes = 0;
+    const uint64_t chunk = 256 * 1024;  // CHUNK_SIZE, include/brle/brle.h:8
+    const uint64_t cap = gd_brle_max_encoded_bytes(in_n_bytes, chunk);
+    const uint64_t sb = gd_brle_encode_scratch_bytes(in_n_bytes, chunk);
+    if (!cap || !sb) return GD_ERR_INVALID_ARG;
+    if (!g_pipe.init()) return GD_ERR_CUDA;
+    cudaStream_t s = g_pipe.st[1];
+    uint8_t* d_in = (uint8_t*)g_epool.get(0, in_n_bytes);
+    uint8_t* d_sc = (uint8_t*)g_epool.get(1, sb);
+    uint8_t* d_out = (uint8_t*)g_epool.get(2, cap);
+    uint64_t* d_len = (uint64_t*)g_epool.get(3, 8);
+    if (!d_in || !d_sc || !d_out || !d_len) return GD_ERR_NOMEM;
+    if (cudaMemcpyAsync(d_in, in, in_n_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return GD_ERR_CUDA;
+    gd_status_t r = gd_brle_encode_device(d_in, in_n_bytes, chunk, d_sc, d_out, d_len, s);
+    if (r != GD_OK) {
+        cudaStreamSynchronize(s);  // the input copy may still be reading `in`
+        return r;
+    }
+    uint64_t len = 0;
+    if (cudaMemcpyAsync(&len, d_len, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return GD_ERR_CUDA;
+    if (len > cap) return GD_ERR_OVERRUN;
+    uint8_t* h = (uint8_t*)pinned().get(len);
+    if (!h) return GD_ERR_NOMEM;
+    if (cudaMemcpyAsync(h, d_out, len, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        gd_free(h);
+        return GD_ERR_CUDA;
+    }
+    *out = h;
+    *out_n_bytes = len;
+    return GD_OK;
+}
+
+gd_status_t gd_rlev1_compress(const uint8_t* in, uint64_t in_n_bytes, uint32_t comp_col_len, uint32_t elem_bytes,
+                              uint64_t chunk_size, uint8_t** out, uint64_t* out_n_bytes, uint64_t** col_len,
+                              uint64_t** blk_off, uint64_t* n_chunks) {
+    if (!in || !out || !out_n_bytes || !col_len || !blk_off || !n_chunks || in_n_bytes == 0 || chunk_size == 0)
+        return GD_ERR_INVALID_ARG;
+    *out = nullptr;
+    *out_n_bytes = 0;
+    const uint64_t bound = gd_rlev1_encode_bound(in_n_bytes, chunk_size, elem_bytes);
+    if (!bound) return GD_ERR_INVALID_ARG;
+    if (!g_pipe.init()) return GD_ERR_CUDA;
+    cudaStream_t s = g_pipe.st[1];
+    const uint64_t nc = (in_n_bytes + chunk_size - 1) / chunk_size;
+    EncBufs b;
+    gd_status_t r = enc_stage(in, in_n_bytes, nc, bound, b, s);
+    if (r == GD_OK)
+        r = gd_rlev1_encode_device(b.in, in_n_bytes, chunk_size, comp_col_len, elem_bytes, b.scratch, b.data,
+                                   b.blk_off, b.col_len, b.st, s);
+    if (r == GD_OK) r = enc_fetch(b, nc, 8, s, out, out_n_bytes, blk_off, col_len, nullptr);
+    if (r != GD_OK) {
+        cudaStreamSynchronize(s);  // the input copy may still be reading `in`
+        return r;
+    }
+    memcpy(*out, &in_n_bytes, 8);  // [u64 in_n_bytes][data], include/rle_v1/rlev1.h:67-70
+    *n_chunks = nc;
+    return GD_OK;
+}
+
+gd_status_t gd_rlev2_compress(const uint8_t* in, uint64_t in_n_bytes, uint32_t read_unit, uint64_t chunk_size,
+                              uint8_t** out, uint64_t* out_n_bytes, uint64_t** blk_off, uint64_t** col_len,
+                              uint64_t* n_chunks) {
+    if (!in || !out || !out_n_bytes || !blk_off || !col_len || !n_chunks || in_n_bytes == 0 || chunk_size == 0)
+        return GD_ERR_INVALID_ARG;
+    *out = nullptr;
+    *out_n_bytes = 0;
+    const uint64_t bound = gd_rlev2_encode_bound(in_n_bytes, chunk_size);
+    if (!bound) return GD_ERR_INVALID_ARG;
+    if (!g_pipe.init()) return GD_ERR_CUDA;
+    cudaStream_t s = g_pipe.st[1];
+    const uint64_t nc = (in_n_bytes + chunk_size - 1) / chunk_size;
+    EncBufs b;
+    gd_status_t r = enc_stage(in, in_n_bytes, nc, bound, b, s);
+    if (r == GD_OK)
+        r = gd_rlev2_encode_device(b.in, in_n_bytes, chunk_size, read_unit, b.scratch, b.data, b.blk_off, b.col_len,
+                                   b.st, s);
+    if (r == GD_OK) r = enc_fetch(b, nc, 0, s, out, out_n_bytes, blk_off, col_len, nullptr);
+    if (r != GD_OK) {
+        cudaStreamSynchronize(s);  // the input copy may still be reading `in`
+        return r;
+    }
+    (*blk_off)[nc] = in_n_bytes;  // the column's size in the last entry, include/rlev2/encoder_trans.h:492
+    *n_chunks = nc;
+    return GD_OK;
+}
+
+int gd_lzss_compress(const uint8_t* in, uint64_t in_n_bytes, uint8_t** out, uint64_t* out_n_bytes,
+                     uint8_t*** out_meta, uint64_t** out_meta_lens, uint64_t* out_meta_num) {
+    if (!in || !out || !out_n_bytes || !out_meta || !out_meta_lens || !out_meta_num || in_n_bytes == 0)
+        return GD_ERR_INVALID_ARG;
+    *out = nullptr;
+    *out_n_bytes = 0;
+    const uint64_t chunk = 128 * 1024;  // CHUNK_SIZE_(), include/lzss/lzss_gpu2.h:25
+    const uint64_t bound = gd_lzss_encode_bound(in_n_bytes, chunk);
+    if (!bound) return GD_ERR_INVALID_ARG;
+    if (!g_pipe.init()) return GD_ERR_CUDA;
+    cudaStream_t s = g_pipe.st[1];
+    const uint64_t nc = (in_n_bytes + chunk - 1) / chunk;
+    EncBufs b;
+    uint64_t *bo = nullptr, *cl = nullptr;
+    uint8_t* cm = nullptr;
+    gd_status_t r = enc_stage(in, in_n_bytes, nc, bound, b, s);
+    if (r == GD_OK)
+        r = gd_lzss_encode_device(b.in, in_n_bytes, chunk, b.scratch, b.data, b.blk_off, b.col_len, b.col_map, b.st,
+                                  s);
+    if (r == GD_OK) r = enc_fetch(b, nc, 0, s, out, out_n_bytes, &bo, &cl, &cm);
+    if (r != GD_OK) {
+        cudaStreamSynchronize(s);  // the input copy may still be reading `in`
+        return r;
+    }
+    // Four blobs as include/lzss/lzss_gpu2.h:2090-2108 hands them out:
+    // chunk size, blk_offset, col_len, col_map.
+    uint8_t** meta = (uint8_t**)malloc(4 * sizeof(uint8_t*));
+    uint64_t* lens = (uint64_t*)malloc(4 * sizeof(uint64_t));
+    uint64_t* cs = (uint64_t*)malloc(8);
+    if (!meta || !lens || !cs) {
+        free(meta);
+        free(lens);
+        free(cs);
+        free(bo);
+        free(cl);
+        free(cm);
+        gd_free(*out);
+        *out = nullptr;
+        *out_n_bytes = 0;
+        return GD_ERR_NOMEM;
+    }
+    *cs = chunk;
+    meta[0] = (uint8_t*)cs;
+    meta[1] = (uint8_t*)bo;
+    meta[2] = (uint8_t*)cl;
+    meta[3] = cm;
+    lens[0] = 8;
+    lens[1] = 8 * (nc + 1);
+    lens[2] = 8 * 32 * nc;
+    lens[3] = 32 * nc;
+    *out_meta = meta;
+    *out_meta_lens = lens;
+    *out_meta_num = 4;
+    return GD_OK;
+}
+
+}  // extern "C"
+
 namespace {
 gd_status_t inflate_piped(const uint8_t* in, uint64_t in_n, const uint64_t* comp_off, const uint64_t* comp_len,
                           const uint64_t* out_off, uint64_t n, int zlib_header, uint8_t* d_data, uint64_t* d_meta,

@@ -446,6 +446,39 @@ gd_status_t gd_rlev2_encode_device(const uint8_t* d_in, uint64_t n_bytes, uint64
                                    uint64_t* d_blk_off, uint64_t* d_col_len, uint32_t* d_status,
                                    gd_stream_t stream);
 
+/* ------------------------------------------------------------------------
+ * Host compress calls on the device encoders (synchronous): the column is
+ * copied from host memory, encoded on the current device and the container
+ * and its metadata returned in buffers released with gd_free, each one
+ * separately.  The same bytes as the host encoders gd_*_encode.
+ * in_n_bytes == 0 is GD_ERR_INVALID_ARG.
+ * ------------------------------------------------------------------------ */
+/* brle::compress_gpu (include/brle/brle.h:242-303): the container
+ * [u32 n_ptr][u64 ptr][u64 total][data] in 256 KiB chunks, the input of
+ * gd_brle_decompress. */
+gd_status_t gd_brle_compress(const uint8_t* in, uint64_t in_n_bytes, uint8_t** out, uint64_t* out_n_bytes);
+/* rle_v1::compress_gpu (include/rle_v1/rlev1.h:25-97): *out is
+ * [u64 in_n_bytes][data]; *col_len (32 * n_chunks values) and *blk_off
+ * (n_chunks + 1) are the arrays the reference writes to its side files
+ * ./input_data/rle_v1_{col_len,blk_offset}.bin.  elem_bytes 4 or 8. */
+gd_status_t gd_rlev1_compress(const uint8_t* in, uint64_t in_n_bytes, uint32_t comp_col_len, uint32_t elem_bytes,
+                              uint64_t chunk_size, uint8_t** out, uint64_t* out_n_bytes, uint64_t** col_len,
+                              uint64_t** blk_off, uint64_t* n_chunks);
+/* rlev2::compress_gpu_transpose (include/rlev2/encoder_trans.h:428-537) on
+ * int64 values: *out is the data, *blk_off (n_chunks + 1) ends with
+ * in_n_bytes (encoder_trans.h:492), *col_len holds 32 * n_chunks values. */
+gd_status_t gd_rlev2_compress(const uint8_t* in, uint64_t in_n_bytes, uint32_t read_unit, uint64_t chunk_size,
+                              uint8_t** out, uint64_t* out_n_bytes, uint64_t** blk_off, uint64_t** col_len,
+                              uint64_t* n_chunks);
+/* lzss::compress_gpu (include/lzss/lzss_gpu2.h:1915-2127), 128 KiB chunks:
+ * *out is the data; *out_meta_num = 4 blobs in *out_meta (lengths in
+ * *out_meta_lens): the u64 chunk size, blk_offset, col_len and col_map --
+ * the metadata gd_lzss_decompress takes.  The last chunk is zero-padded to
+ * a whole chunk (the reference drops a partial last chunk).  Release the
+ * four blobs, *out_meta and *out_meta_lens with gd_free. */
+int gd_lzss_compress(const uint8_t* in, uint64_t in_n_bytes, uint8_t** out, uint64_t* out_n_bytes,
+                     uint8_t*** out_meta, uint64_t** out_meta_lens, uint64_t* out_meta_num);
+
 uint64_t gd_lzss_max_encoded_bytes(uint64_t n, uint64_t chunk_size);
 /* lzss::compress_gpu (include/lzss/lzss_gpu2.h:1915-2127). */
 uint64_t gd_lzss_encode(const uint8_t* in, uint64_t n, uint64_t chunk_size, uint8_t* data,

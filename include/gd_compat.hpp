@@ -197,3 +197,96 @@ inline int gpu_copy_uncompressed_blocks(gpu_inflate_input_s* inputs, int count, 
 }
 }  // namespace io
 }  // namespace cudf
+
+// ---------------------------------------------------------------------------
+// Writers: the reference's compress calls on the device encoders.  Outputs
+// are new[] buffers (the LZSS metadata malloc'd), as the reference hands
+// them out; rle_v1 writes its side files as the reference does.
+
+namespace gd_compat_detail {
+inline bool write_file(const char* path, const void* p, uint64_t n) {
+    std::ofstream f(path, std::ios::binary);
+    return f && f.write(static_cast<const char*>(p), (std::streamsize)n);
+}
+}  // namespace gd_compat_detail
+
+// include/brle/brle.h:251-303
+namespace brle {
+inline void compress_gpu(const uint8_t* in, uint8_t** out, const uint64_t in_n_bytes, uint64_t* out_n_bytes) {
+    uint8_t* p = nullptr;
+    uint64_t n = 0;
+    const gd_status_t rc = gd_brle_compress(in, in_n_bytes, &p, &n);
+    gd_compat_detail::report(rc, "brle::compress_gpu");
+    *out = rc == GD_OK ? gd_compat_detail::adopt(p, n) : nullptr;
+    *out_n_bytes = rc == GD_OK ? n : 0;
+}
+}  // namespace brle
+
+// include/rle_v1/rlev1.h:22-97: [u64 in_n_bytes][data], with col_len and
+// blk_offset written to ./input_data/rle_v1_{col_len,blk_offset}.bin.
+namespace rle_v1 {
+template <typename READ_COL_TYPE, typename DATA_TYPE, typename OUT_COL_TYPE>
+void compress_gpu(const uint8_t* const in, uint8_t** out, const uint64_t in_n_bytes, uint64_t* out_n_bytes,
+                  int COMP_COL_LEN, uint64_t CHUNK_SIZE) {
+    uint8_t* p = nullptr;
+    uint64_t n = 0, nc = 0, *col = nullptr, *blk = nullptr;
+    const gd_status_t rc = gd_rlev1_compress(in, in_n_bytes, (uint32_t)COMP_COL_LEN, (uint32_t)sizeof(DATA_TYPE),
+                                             CHUNK_SIZE, &p, &n, &col, &blk, &nc);
+    gd_compat_detail::report(rc, "rle_v1::compress_gpu");
+    *out = nullptr;
+    *out_n_bytes = 0;
+    if (rc != GD_OK) return;
+    if (!gd_compat_detail::write_file("./input_data/rle_v1_col_len.bin", col, 8 * 32 * nc) ||
+        !gd_compat_detail::write_file("./input_data/rle_v1_blk_offset.bin", blk, 8 * (nc + 1)))
+        std::fprintf(stderr, "gd: rle_v1::compress_gpu: cannot write ./input_data side files\n");
+    gd_free(col);
+    gd_free(blk);
+    *out = gd_compat_detail::adopt(p, n);
+    *out_n_bytes = n;
+}
+}  // namespace rle_v1
+
+// include/rlev2/encoder_trans.h:428-537 (8-byte values; blk_off[n_chunks]
+// holds in_n_bytes, as decompress_gpu expects).
+namespace rlev2 {
+template <int READ_UNIT, typename COMP_TYPE, typename IN_T>
+void compress_gpu_transpose(const IN_T* const in, const uint64_t in_n_bytes, uint8_t*& out, uint64_t& out_n_bytes,
+                            uint64_t& meta_data_size, uint64_t& out_n_chunks, uint64_t*& blk_off,
+                            uint64_t*& col_len, uint64_t CHUNK_SIZE) {
+    static_assert(sizeof(IN_T) == 8, "the RLE v2 encoder takes 8-byte values");
+    uint8_t* p = nullptr;
+    uint64_t n = 0, nc = 0, *bo = nullptr, *cl = nullptr;
+    const gd_status_t rc = gd_rlev2_compress(reinterpret_cast<const uint8_t*>(in), in_n_bytes, (uint32_t)READ_UNIT,
+                                             CHUNK_SIZE, &p, &n, &bo, &cl, &nc);
+    gd_compat_detail::report(rc, "rlev2::compress_gpu_transpose");
+    out = nullptr;
+    out_n_bytes = meta_data_size = out_n_chunks = 0;
+    blk_off = col_len = nullptr;
+    if (rc != GD_OK) return;
+    blk_off = new uint64_t[nc + 1];
+    col_len = new uint64_t[32 * nc];
+    std::memcpy(blk_off, bo, 8 * (nc + 1));
+    std::memcpy(col_len, cl, 8 * 32 * nc);
+    gd_free(bo);
+    gd_free(cl);
+    out = gd_compat_detail::adopt(p, n);
+    out_n_bytes = n;
+    out_n_chunks = nc;
+    meta_data_size = 8 * 32 * nc + 8 * (nc + 1);  // encoder_trans.h:443
+}
+}  // namespace rlev2
+
+// include/lzss/lzss_gpu2.h:1952-2127 (128 KiB chunks; the four metadata
+// blobs and their arrays are malloc'd, as the reference's are)
+namespace lzss {
+inline void compress_gpu(const uint8_t* const in, const uint64_t in_n_bytes, uint8_t** out, uint64_t* out_n_bytes,
+                         uint8_t*** out_metadata, uint64_t** out_metadata_lens, uint64_t* out_metadata_num) {
+    uint8_t* p = nullptr;
+    uint64_t n = 0;
+    const int rc = gd_lzss_compress(in, in_n_bytes, &p, &n, out_metadata, out_metadata_lens, out_metadata_num);
+    gd_compat_detail::report(rc, "lzss::compress_gpu");
+    *out = rc == GD_OK ? gd_compat_detail::adopt(p, n) : nullptr;
+    *out_n_bytes = rc == GD_OK ? n : 0;
+    if (rc != GD_OK) *out_metadata_num = 0;
+}
+}  // namespace lzss

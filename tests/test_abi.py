@@ -78,6 +78,13 @@ int main(int argc, char**) {
         brle_trans::decompress_gpu(nullptr, &out, 0, &n);
         deflate::decompress_gpu<uint64_t, 8, 2, 1>(nullptr, &out, 0, &n, cl, 8, bo, 16, 65536);
         cudf::io::gpuinflate(nullptr, nullptr, 0, 1);
+        brle::compress_gpu(nullptr, &out, 0, &n);
+        rle_v1::compress_gpu<uint64_t, uint32_t, uint32_t>(nullptr, &out, 0, &n, 128, 128 * 1024);
+        uint8_t* enc = nullptr; uint64_t ms = 0, nch = 0; uint64_t* pbo = nullptr; uint64_t* pcl = nullptr;
+        const uint64_t* in64 = nullptr;
+        rlev2::compress_gpu_transpose<32, uint64_t>(in64, 0, enc, n, ms, nch, pbo, pcl, 256 * 1024);
+        uint8_t** meta = nullptr; uint64_t* ml = nullptr; uint64_t mn = 0;
+        lzss::compress_gpu(nullptr, 0, &out, &n, &meta, &ml, &mn);
     }
     return 0;
 }
@@ -99,3 +106,20 @@ def test_tuning_knobs_set_and_get():
         assert L.gd_tune_get(key) == 4
         assert L.gd_tune_set(key, old) == 4
     assert L.gd_tune_get(5) == -1 and L.gd_tune_set(5, 1) == -1 and L.gd_tune_set(0, -1) == -1
+
+
+def test_host_compress_argument_errors():
+    # rejected on the host, before any device call
+    import ctypes as C
+    L = _lib.lib()
+    out, n, a, b, k = C.c_void_p(), C.c_uint64(), C.c_void_p(), C.c_void_p(), C.c_uint64()
+    buf = (C.c_uint8 * 16)()
+    bad = [L.gd_brle_compress(None, 16, C.byref(out), C.byref(n)),
+           L.gd_brle_compress(buf, 0, C.byref(out), C.byref(n)),
+           L.gd_rlev1_compress(buf, 0, 128, 4, 4096, C.byref(out), C.byref(n), C.byref(a), C.byref(b), C.byref(k)),
+           L.gd_rlev1_compress(buf, 16, 128, 4, 0, C.byref(out), C.byref(n), C.byref(a), C.byref(b), C.byref(k)),
+           L.gd_rlev2_compress(buf, 0, 32, 8192, C.byref(out), C.byref(n), C.byref(a), C.byref(b), C.byref(k)),
+           L.gd_rlev2_compress(buf, 16, 32, 8192, None, C.byref(n), C.byref(a), C.byref(b), C.byref(k)),
+           L.gd_lzss_compress(buf, 0, C.byref(out), C.byref(n), C.byref(a), C.byref(b), C.byref(k)),
+           L.gd_lzss_compress(buf, 16, C.byref(out), C.byref(n), None, C.byref(b), C.byref(k))]
+    assert all(L.gd_status_string(rc) == b"invalid argument" for rc in bad), bad

@@ -184,3 +184,35 @@ def test_device_encoder_argument_errors(cuda):
         cc.encode_device("lzss", d, 1000)                                         # chunk not 128-byte rows
     with pytest.raises(cc.DecodeError):
         cc.encode_device("lzss", d, 256 * 1024)                                   # column above 4 KiB
+
+
+def test_host_compress_calls(cuda):
+    """gd_brle_compress / gd_rlev1_compress / gd_rlev2_compress /
+    gd_lzss_compress (the reference's compress_gpu calls, host buffers in
+    and out): the same container and metadata as the host encoders, and the
+    host decompress call returns the column."""
+    raw = cc.gen_brle_bytes(5, 3_000_001)
+    dev = cc.compress_host("brle", raw)
+    assert np.array_equal(dev.params["container"], cc.brle_encode(raw).params["container"])
+    assert np.array_equal(cc.decode_host(dev), raw)
+    raw = cc.gen_markov_copy(6, 1_000_003, 4096)
+    dev = cc.compress_host("lzss", raw)
+    _same(dev, cc.lzss_encode(raw, 128 * 1024))
+    assert dev.chunk_size == 128 * 1024
+    assert np.array_equal(cc.decode_host(dev)[:raw.size], raw)
+    for eb, ccl, chunk in ((4, 128, 128 * 1024), (8, 64, 64 * 1024)):
+        v = cc.gen_rlev1_ints(eb, 700_001).astype(np.uint32 if eb == 4 else np.uint64)
+        raw = v.view(np.uint8)
+        dev = cc.compress_host("rlev1", raw, chunk, comp_col_len=ccl, elem_bytes=eb)
+        _same(dev, cc.rlev1_encode(raw, chunk, ccl, eb))
+        assert int(dev.params["container"][:8].view(np.uint64)[0]) == raw.size
+        assert np.array_equal(cc.decode_host(dev), raw)
+    for ru, chunk in ((32, 256 * 1024), (4, 4 * 4096)):
+        raw = cc.gen_rlev2_ints(7, 500_001).view(np.uint8)
+        dev = cc.compress_host("rlev2", raw, chunk, read_unit=ru)
+        _same(dev, cc.rlev2_encode(raw, chunk, ru))
+        assert np.array_equal(cc.decode_host(dev), raw)
+    # twice in a row on the same thread: the staging pool is reused
+    raw = cc.gen_brle_bytes(8, 100_000)
+    a, b = cc.compress_host("brle", raw), cc.compress_host("brle", raw)
+    assert np.array_equal(a.params["container"], b.params["container"])
