@@ -67,7 +67,9 @@ SIGNATURES = {
     "gd_brle_encode_scratch_bytes": (u64, [u64, u64]),
     "gd_brle_encode_device": (i32, [vp, u64, u64, vp, vp, vp, vp]),
     "gd_lzss_encode_bound": (u64, [u64, u64]),
+    "gd_brle_trans_encode_bound": (u64, [u64, u64]),
     "gd_lzss_encode_device": (i32, [vp, u64, u64, vp, vp, vp, vp, vp, vp, vp]),
+    "gd_brle_trans_encode_device": (i32, [vp, u64, u64, vp, vp, vp, vp, vp, vp, vp]),
     "gd_rlev1_encode_bound": (u64, [u64, u64, u32]),
     "gd_rlev1_encode_device": (i32, [vp, u64, u64, u32, u32, vp, vp, vp, vp, vp, vp]),
     "gd_rlev2_encode_bound": (u64, [u64, u64]),

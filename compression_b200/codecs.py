@@ -275,6 +275,8 @@ def encode_device(codec: str, d_col, chunk_size: int, *, comp_col_len: int = 128
         bound = L.gd_rlev1_encode_bound(n, chunk_size, elem_bytes)
     elif codec == "lzss":
         bound = L.gd_lzss_encode_bound(n, chunk_size)
+    elif codec == "brle_trans":
+        bound = L.gd_brle_trans_encode_bound(n, chunk_size)
     elif codec == "rlev2":
         bound = L.gd_rlev2_encode_bound(n, chunk_size)
     else:
@@ -296,9 +298,10 @@ def encode_device(codec: str, d_col, chunk_size: int, *, comp_col_len: int = 128
         rc = L.gd_rlev1_encode_device(p(d_col), n, chunk_size, comp_col_len, elem_bytes, p(bufs["scratch"]),
                                       p(bufs["data"]), p(bufs["blk_off"]), p(bufs["col_len"]), p(bufs["status"]),
                                       C.c_void_p(s))
-    elif codec == "lzss":
-        rc = L.gd_lzss_encode_device(p(d_col), n, chunk_size, p(bufs["scratch"]), p(bufs["data"]), p(bufs["blk_off"]),
-                                     p(bufs["col_len"]), p(bufs["col_map"]), p(bufs["status"]), C.c_void_p(s))
+    elif codec in ("lzss", "brle_trans"):
+        fn = L.gd_lzss_encode_device if codec == "lzss" else L.gd_brle_trans_encode_device
+        rc = fn(p(d_col), n, chunk_size, p(bufs["scratch"]), p(bufs["data"]), p(bufs["blk_off"]),
+                p(bufs["col_len"]), p(bufs["col_map"]), p(bufs["status"]), C.c_void_p(s))
     else:
         rc = L.gd_rlev2_encode_device(p(d_col), n, chunk_size, read_unit, p(bufs["scratch"]), p(bufs["data"]),
                                       p(bufs["blk_off"]), p(bufs["col_len"]), p(bufs["status"]), C.c_void_p(s))
@@ -353,7 +356,7 @@ def encode_gpu(codec: str, raw, chunk_size: int, *, comp_col_len: int = 128, ele
     data = r["data"][:int(blk[-1])].cpu().numpy()
     nc = blk.size - 1
     meta = {"blk_off": blk, "col_len": col}
-    if codec == "lzss":
+    if codec in ("lzss", "brle_trans"):
         meta["col_map"] = r["col_map"].cpu().numpy()
     params = ({"comp_col_len": comp_col_len, "elem_bytes": elem_bytes} if codec == "rlev1"
               else {"read_unit": read_unit} if codec == "rlev2" else {})

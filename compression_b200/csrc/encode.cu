@@ -513,3 +513,130 @@ extern "C" gd_status_t gd_lzss_encode_device(const uint8_t* d_in, uint64_t n_byt
                                                   d_col_map);
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
 }
+
+// ---------------------------------------------------------------------------
+// Byte-RLE flag container (brle_trans::compress_gpu, include/brle/brle_trans.h:
+// 563-660; column streams by compress_func :437-562)
+// ---------------------------------------------------------------------------
+//
+// Same column split, ranking and interleave as the LZSS container; only the
+// column stream differs: maximal runs of equal bytes, a run of 3 or more as a
+// run item (count byte, value byte; flag bit 0), a shorter one as that many
+// literal items (flag bit 1), a flag byte before every 8 items (LSB first)
+// and, after the 8th item of a group, the next flag byte reserved (0 if no
+// item follows).  A thread per column: the warp's 32 lanes are one chunk's
+// 32 columns, so each step reads 128 contiguous input bytes.  Output bytes
+// gather in a word register; a group's flag byte goes into that register when
+// its word is still open, else it is stored over the 0 already written.
+// Run counts fit the count byte because a column holds at most 252 bytes.
+
+__global__ void __launch_bounds__(NT) brle_trans_column_kernel(const uint8_t* __restrict__ in, uint64_t n_bytes,
+                                                               uint64_t chunk_size, uint32_t n_cols,
+                                                               uint8_t* __restrict__ scratch, uint32_t cap,
+                                                               uint32_t* __restrict__ raw_len) {
+    const uint32_t col = blockIdx.x * NT + threadIdx.x;
+    if (col >= n_cols) return;
+    const uint64_t c = col >> 5;
+    const uint32_t q = col & 31u;
+    const uint32_t L = (uint32_t)(chunk_size / 32u);
+    const uint64_t base = c * chunk_size + 4u * q;
+    uint8_t* slot = scratch + (uint64_t)col * cap;
+    uint32_t* wslot = reinterpret_cast<uint32_t*>(slot);
+    uint32_t pos = 1, hpos = 0, items = 0, flags = 0, wbuf = 0;  // byte 0: the first flag byte
+    auto put = [&](uint32_t b) {
+        wbuf |= b << (8u * (pos & 3u));
+        if ((++pos & 3u) == 0) {
+            wslot[(pos >> 2) - 1u] = wbuf;
+            wbuf = 0;
+        }
+    };
+    auto set_flag = [&]() {
+        if (hpos >= (pos & ~3u))
+            wbuf |= flags << (8u * (hpos & 3u));
+        else
+            slot[hpos] = (uint8_t)flags;
+    };
+    auto item_done = [&]() {
+        if (++items == 8u) {
+            set_flag();
+            flags = 0;
+            items = 0;
+            hpos = pos;
+            put(0u);
+        }
+    };
+    auto emit = [&](uint32_t v, uint32_t run) {
+        if (run >= 3u) {
+            put(run);
+            put(v);
+            item_done();
+        } else {
+            for (uint32_t k = 0; k < run; ++k) {
+                flags |= 1u << items;
+                put(v);
+                item_done();
+            }
+        }
+    };
+    uint32_t cur = 0, run = 0;
+    for (uint32_t k = 0; k < L / 4u; ++k) {
+        const uint64_t at = base + 128ull * k;
+        uint32_t w = 0;
+        if (at + 4u <= n_bytes) {
+            w = *reinterpret_cast<const uint32_t*>(in + at);
+        } else {
+            for (uint32_t b = 0; b < 4u; ++b)
+                if (at + b < n_bytes) w |= (uint32_t)in[at + b] << (8u * b);
+        }
+#pragma unroll
+        for (uint32_t b = 0; b < 4u; ++b) {
+            const uint32_t x = (w >> (8u * b)) & 0xffu;
+            if (run && x == cur) {
+                ++run;
+            } else {
+                if (run) emit(cur, run);
+                cur = x;
+                run = 1;
+            }
+        }
+    }
+    if (run) emit(cur, run);
+    if (items) set_flag();
+    if (pos & 3u) wslot[pos >> 2] = wbuf;
+    raw_len[col] = pos;
+}
+
+extern "C" uint64_t gd_brle_trans_encode_bound(uint64_t n_bytes, uint64_t chunk_size) {
+    if (n_bytes == 0 || chunk_size == 0) return 0;
+    return (n_bytes + chunk_size - 1) / chunk_size * 32u * (lzss_col_cap(chunk_size) + 4u) + 16u;
+}
+
+extern "C" gd_status_t gd_brle_trans_encode_device(const uint8_t* d_in, uint64_t n_bytes, uint64_t chunk_size,
+                                                   uint8_t* d_scratch, uint8_t* d_data, uint64_t* d_blk_off,
+                                                   uint64_t* d_col_len, uint8_t* d_col_map, uint32_t* d_status,
+                                                   gd_stream_t stream) {
+    if (n_bytes == 0) return GD_OK;
+    if (!d_in || !d_scratch || !d_data || !d_blk_off || !d_col_len || !d_col_map) return GD_ERR_INVALID_ARG;
+    if (chunk_size == 0 || chunk_size % 128u || chunk_size / 32u > 252u) return GD_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(d_in) & 3u) || (reinterpret_cast<uintptr_t>(d_scratch) & 3u) ||
+        (reinterpret_cast<uintptr_t>(d_data) & 3u))
+        return GD_ERR_INVALID_ARG;
+    const uint64_t nc = (n_bytes + chunk_size - 1) / chunk_size;
+    if (nc * 32u > 0xffffffffull) return GD_ERR_UNSUPPORTED;
+    const uint64_t cap = lzss_col_cap(chunk_size);
+    uint32_t* raw_len = reinterpret_cast<uint32_t*>(d_scratch + nc * 32u * cap);
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t ncol = (uint32_t)(nc * 32u);
+    brle_trans_column_kernel<<<(ncol + NT - 1) / NT, NT, 0, s>>>(d_in, n_bytes, chunk_size, ncol, d_scratch,
+                                                                 (uint32_t)cap, raw_len);
+    lzss_rank_kernel<<<(uint32_t)((nc + NT / 32 - 1) / (NT / 32)), NT, 0, s>>>(raw_len, (uint32_t)nc, d_col_len,
+                                                                              d_col_map, d_blk_off + 1, d_status);
+    offsets_kernel<<<1, 1024, 0, s>>>(d_blk_off, (uint32_t)nc);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t g3 = nc < (uint64_t)sms * 16u ? nc : (uint64_t)sms * 16u;
+    interleave_kernel<<<(uint32_t)g3, NT, 0, s>>>(d_scratch, (uint32_t)cap, d_col_len, d_blk_off, (uint32_t)nc, d_data,
+                                                  d_col_map);
+    return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+}

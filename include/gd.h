@@ -433,6 +433,17 @@ gd_status_t gd_lzss_encode_device(const uint8_t* d_in, uint64_t n_bytes, uint64_
                                   uint8_t* d_scratch, uint8_t* d_data, uint64_t* d_blk_off,
                                   uint64_t* d_col_len, uint8_t* d_col_map, uint32_t* d_status,
                                   gd_stream_t stream);
+/* brle_trans::compress_gpu (include/brle/brle_trans.h:563-660): the
+ * byte-RLE flag container with the arrays of its side files -- d_blk_off
+ * (n_chunks + 1), d_col_len and d_col_map (32 * n_chunks, slots by
+ * descending column length).  chunk_size a multiple of 128, at most 8064
+ * (the reference's is 4096); buffers as for gd_lzss_encode_device, sized by
+ * gd_brle_trans_encode_bound.  The last chunk is zero-padded. */
+uint64_t gd_brle_trans_encode_bound(uint64_t n_bytes, uint64_t chunk_size);
+gd_status_t gd_brle_trans_encode_device(const uint8_t* d_in, uint64_t n_bytes, uint64_t chunk_size,
+                                        uint8_t* d_scratch, uint8_t* d_data, uint64_t* d_blk_off,
+                                        uint64_t* d_col_len, uint8_t* d_col_map, uint32_t* d_status,
+                                        gd_stream_t stream);
 /* rle_v1::compress_gpu (include/rle_v1/rlev1.h:25-97); elem_bytes 4 or 8. */
 uint64_t gd_rlev1_encode_bound(uint64_t n_bytes, uint64_t chunk_size, uint32_t elem_bytes);
 gd_status_t gd_rlev1_encode_device(const uint8_t* d_in, uint64_t n_bytes, uint64_t chunk_size,

@@ -47,6 +47,11 @@ def test_device_api_rejects_bad_arguments_without_gpu():
     assert L.gd_lzss_encode_device(4, 1000, 1000, 4, 4, 8, 8, 1, None, None) == 1     # chunk % 128
     assert L.gd_lzss_encode_device(4, 1000, 256 * 1024, 4, 4, 8, 8, 1, None, None) == 1  # column > 4 KiB
     assert L.gd_lzss_encode_device(2, 1000, 4096, 4, 4, 8, 8, 1, None, None) == 1     # unaligned input
+    assert L.gd_brle_trans_encode_device(4, 1000, 1000, 4, 4, 8, 8, 1, None, None) == 1   # chunk % 128
+    assert L.gd_brle_trans_encode_device(4, 1000, 8192, 4, 4, 8, 8, 1, None, None) == 1   # column > 252 bytes
+    assert L.gd_brle_trans_encode_device(2, 1000, 4096, 4, 4, 8, 8, 1, None, None) == 1   # unaligned input
+    assert L.gd_brle_trans_encode_device(4, 1000, 4096, 4, None, 8, 8, 1, None, None) == 1  # no data buffer
+    assert L.gd_brle_trans_encode_bound(2 * 4096, 4096) == 2 * 32 * (((128 + 16 + 8 + 3) & ~3) + 4) + 16
     # bounds: 32 lane slots per chunk, each holding the longest lane stream
     assert L.gd_rlev1_encode_bound(128 * 1024, 128 * 1024, 4) == 32 * ((1024 * 5 + 1024 // 64 + 16 + 3) & ~3)
     assert L.gd_rlev2_encode_bound(2 * 256 * 1024, 256 * 1024) == 2 * 32 * ((1024 * 11 + 64 + 3) & ~3)

@@ -1,6 +1,6 @@
-"""GPU parity of the byte-RLE, LZSS, RLE v1 and RLE v2 device encoders: the
-container written on the device is byte-identical to the host encoder's,
-whose streams are pinned against the reference's own encoders in
+"""GPU parity of the byte-RLE, byte-RLE flag, LZSS, RLE v1 and RLE v2 device
+encoders: the container written on the device is byte-identical to the host
+encoder's, whose streams are pinned against the reference's own encoders in
 test_golden.py, and decodes back to the column through the device decoder
 and the oracle."""
 import numpy as np
@@ -122,6 +122,15 @@ def test_brle_device_encoder(cuda, chunk):
         _roundtrip(dev, raw, cuda)
 
 
+@pytest.mark.parametrize("chunk", [4096, 128, 1024, 8064])
+def test_brle_trans_device_encoder(cuda, chunk):
+    for raw in _brle_inputs():
+        host = cc.brle_trans_encode(raw, chunk)
+        dev = cc.encode_gpu("brle_trans", raw, chunk)
+        _same(dev, host)
+        _roundtrip(dev, raw, cuda)
+
+
 def _lzss_inputs():
     rng = np.random.default_rng(11)
     yield cc.gen_markov_copy(3, 1 << 20, 4096)
@@ -184,6 +193,8 @@ def test_device_encoder_argument_errors(cuda):
         cc.encode_device("lzss", d, 1000)                                         # chunk not 128-byte rows
     with pytest.raises(cc.DecodeError):
         cc.encode_device("lzss", d, 256 * 1024)                                   # column above 4 KiB
+    with pytest.raises(cc.DecodeError):
+        cc.encode_device("brle_trans", d, 8192)                                   # column above 252 bytes
 
 
 def test_host_compress_calls(cuda):
