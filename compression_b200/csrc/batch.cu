@@ -208,21 +208,25 @@ extern "C" uint32_t gd_batch_warps(uint32_t max_lane_bytes, uint32_t blocks_per_
 // ---------------------------------------------------------------------------
 // Batch decode with longest-first placement and no allocation at all.
 //
-// For callers that may not allocate device memory at decode time: code that
-// runs while a stream is being captured into a CUDA graph (an allocation
-// there is an error or turns into a graph node the caller did not plan for),
-// and hosts that hand the decoder a fixed memory budget up front (a query
-// engine's pre-reserved pool) and treat any further allocation as a failure.
-// gd_batch_decode needs a work-queue counter and an order array from its
-// caller; here both live in the file-scope array below, together with the
-// buckets of the sort that makes the order, so the only memory touched is the
-// caller's tasks, costs, outputs and statuses plus this fixed array.
+// For callers that may not allocate device memory at decode time: hosts that
+// hand the decoder a fixed memory budget up front (a query engine's
+// pre-reserved pool, an embedded service with a hard memory cap) and treat
+// any further allocation as a failure, and decode paths that must not pay
+// cudaMalloc / cudaFree's implicit device-wide synchronisation while other
+// streams of the process are busy.  gd_batch_decode needs a work-queue
+// counter and an order array from its caller; here both live in the
+// file-scope array below, together with the buckets of the sort that makes
+// the order, so the only memory touched is the caller's tasks, costs,
+// outputs and statuses plus this fixed array.
 //
 // Limits: at most NOALLOC_MAX_TASKS tasks per call (larger batches are
 // rejected with GD_ERR_INVALID_ARG).  Nothing has to start at zero: the sort
 // kernel clears the buckets and the counter at the start of every call.
 // Calls that overlap in time on one device (two streams, or two host
-// threads) share the array and race; the caller serialises them.
+// threads) share the array and race; the caller serialises them.  The
+// array's device address is looked up once per device and kept for the life
+// of the process; a cudaDeviceReset() of that device invalidates it, so the
+// entry point is not for use after such a reset.
 // ---------------------------------------------------------------------------
 #include <mutex>
 
@@ -235,11 +239,16 @@ constexpr uint32_t SORT_NT = 1024;  // threads of the single sort block
 // [0, MAX): order; [MAX, MAX + NBUCKET): bucket cursors; [MAX + NBUCKET]: counter
 static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_MAX_TASKS + NBUCKET + 64];
 
-// Bucket of cost c in [mn, mx]: the highest cost goes to bucket 0, so the
-// bucket order is longest first; NaN and equal costs go last / to bucket 0.
+// Bucket of cost c, with mn / mx the smallest and largest FINITE costs and
+// scale = (NBUCKET - 1) / (mx - mn) (0 when all finite costs are equal).
+// The highest cost goes to bucket 0, so the bucket order is longest first;
+// costs equal to mn (all of them when scale is 0) go to the last bucket.
+// Non-finite costs are placed explicitly: +inf first (bucket 0), -inf and
+// NaN last (bucket NBUCKET - 1).
 __device__ __forceinline__ uint32_t cost_bucket(float c, float mn, float scale) {
-    if (!(c >= mn)) return NBUCKET - 1;  // NaN or below the minimum
-    const float q = (c - mn) * scale;
+    if (c == INFINITY) return 0;
+    if (!(c > -INFINITY && c < INFINITY)) return NBUCKET - 1;  // NaN or -inf
+    const float q = (c - mn) * scale;                          // finite, >= 0
     const uint32_t b = q >= (float)(NBUCKET - 1) ? NBUCKET - 1 : (uint32_t)q;
     return NBUCKET - 1 - b;
 }
@@ -257,7 +266,7 @@ __global__ void __launch_bounds__(SORT_NT) lpt_sort_kernel(const float* __restri
     float mn = INFINITY, mx = -INFINITY;
     for (uint32_t i = tid; i < n; i += SORT_NT) {
         const float c = cost[i];
-        if (c == c) {
+        if (c > -INFINITY && c < INFINITY) {  // finite costs set the bucket range
             mn = fminf(mn, c);
             mx = fmaxf(mx, c);
         }
@@ -279,6 +288,9 @@ __global__ void __launch_bounds__(SORT_NT) lpt_sort_kernel(const float* __restri
         mn = fminf(mn, red_mn[w]);
         mx = fmaxf(mx, red_mx[w]);
     }
+    // no finite cost at all: mn = +inf, mx = -inf, span < 0, scale 0 (every
+    // cost is non-finite and placed by cost_bucket without the range); a
+    // span that overflows float gives scale 0 too
     const float span = mx - mn;
     const float scale = (span > 0.f && span < INFINITY) ? (float)(NBUCKET - 1) / span : 0.f;
     for (uint32_t i = tid; i < n; i += SORT_NT) atomicAdd(&hist[cost_bucket(cost[i], mn, scale)], 1u);

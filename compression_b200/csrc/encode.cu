@@ -524,7 +524,8 @@ extern "C" gd_status_t gd_lzss_encode_device(const uint8_t* d_in, uint64_t n_byt
 // run item (count byte, value byte; flag bit 0), a shorter one as that many
 // literal items (flag bit 1), a flag byte before every 8 items (LSB first)
 // and, after the 8th item of a group, the next flag byte reserved (0 if no
-// item follows).  A thread per column: the warp's 32 lanes are one chunk's
+// item follows) -- except after the column's last item when that is a run,
+// which the reference writes without counting it (brle_trans.h:529-536).  A thread per column: the warp's 32 lanes are one chunk's
 // 32 columns, so each step reads 128 contiguous input bytes.  Output bytes
 // gather in a word register; a group's flag byte goes into that register when
 // its word is still open, else it is stored over the 0 already written.
@@ -565,11 +566,11 @@ __global__ void __launch_bounds__(NT) brle_trans_column_kernel(const uint8_t* __
             put(0u);
         }
     };
-    auto emit = [&](uint32_t v, uint32_t run) {
+    auto emit = [&](uint32_t v, uint32_t run, bool last) {
         if (run >= 3u) {
             put(run);
             put(v);
-            item_done();
+            if (!last) item_done();  // the column's last run is written uncounted
         } else {
             for (uint32_t k = 0; k < run; ++k) {
                 flags |= 1u << items;
@@ -594,13 +595,13 @@ __global__ void __launch_bounds__(NT) brle_trans_column_kernel(const uint8_t* __
             if (run && x == cur) {
                 ++run;
             } else {
-                if (run) emit(cur, run);
+                if (run) emit(cur, run, false);
                 cur = x;
                 run = 1;
             }
         }
     }
-    if (run) emit(cur, run);
+    if (run) emit(cur, run, true);
     if (items) set_flag();
     if (pos & 3u) wslot[pos >> 2] = wbuf;
     raw_len[col] = pos;

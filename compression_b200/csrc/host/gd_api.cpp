@@ -662,23 +662,24 @@ gd_status_t enc_fetch(const EncBufs& b, uint64_t nc, uint64_t at, cudaStream_t s
     uint64_t* cl = (uint64_t*)malloc(8 * 32 * nc);
     uint8_t* cm = col_map ? (uint8_t*)malloc(32 * nc) : nullptr;
     uint8_t* h = nullptr;
-    bool ok = bo && cl && (!col_map || cm);
-    ok = ok && cudaMemcpyAsync(bo, b.blk_off, 8 * (nc + 1), cudaMemcpyDeviceToHost, s) == cudaSuccess;
-    ok = ok && cudaMemcpyAsync(cl, b.col_len, 8 * 32 * nc, cudaMemcpyDeviceToHost, s) == cudaSuccess;
-    ok = ok && (!cm || cudaMemcpyAsync(cm, b.col_map, 32 * nc, cudaMemcpyDeviceToHost, s) == cudaSuccess);
-    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
-    if (ok) {
-        h = (uint8_t*)pinned().get(at + bo[nc]);
-        ok = h && cudaMemcpyAsync(h + at, b.data, bo[nc], cudaMemcpyDeviceToHost, s) == cudaSuccess &&
-             cudaStreamSynchronize(s) == cudaSuccess;
-    }
-    if (!ok) {
+    auto fail = [&](gd_status_t why) {
         free(bo);
         free(cl);
         free(cm);
         if (h) gd_free(h);
-        return GD_ERR_CUDA;
-    }
+        return why;
+    };
+    if (!bo || !cl || (col_map && !cm)) return fail(GD_ERR_NOMEM);
+    bool ok = cudaMemcpyAsync(bo, b.blk_off, 8 * (nc + 1), cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(cl, b.col_len, 8 * 32 * nc, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    ok = ok && (!cm || cudaMemcpyAsync(cm, b.col_map, 32 * nc, cudaMemcpyDeviceToHost, s) == cudaSuccess);
+    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+    if (!ok) return fail(GD_ERR_CUDA);
+    h = (uint8_t*)pinned().get(at + bo[nc]);
+    if (!h) return fail(GD_ERR_NOMEM);  // no pinned host buffer for the container
+    ok = cudaMemcpyAsync(h + at, b.data, bo[nc], cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+         cudaStreamSynchronize(s) == cudaSuccess;
+    if (!ok) return fail(GD_ERR_CUDA);
     *data = h;
     *data_n = at + bo[nc];
     *blk_off = bo;

@@ -244,7 +244,11 @@ void lzss_encode_column(const uint8_t* d, uint32_t L, std::vector<uint8_t>& out)
 // 3 or more becomes a run item (count byte, value byte; flag bit 0), a
 // shorter run becomes that many literal items (one byte each; flag bit 1).
 // A flag byte precedes every 8 items, bits LSB first; after the 8th item of a
-// group the next flag byte is reserved even if no item follows (it stays 0).
+// group the next flag byte is reserved even if no item follows (it stays 0) --
+// except after the column's last item when that is a run: the reference
+// writes that run without counting it (compress_func, brle_trans.h:529-536;
+// compress_init_func sizes it the same way, :354-357), so no flag byte is
+// reserved after it even when it fills slot 8.
 void brle_trans_encode_column(const uint8_t* d, uint32_t L, std::vector<uint8_t>& out) {
     out.assign(1, 0);
     size_t hpos = 0;
@@ -267,7 +271,7 @@ void brle_trans_encode_column(const uint8_t* d, uint32_t L, std::vector<uint8_t>
         if (run >= 3) {
             out.push_back((uint8_t)run);
             out.push_back(d[i]);
-            item_done();
+            if (j < L) item_done();  // the column's last run is not counted
         } else {
             for (uint32_t k = 0; k < run; ++k) {
                 flags |= (uint8_t)(1u << items);

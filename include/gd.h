@@ -247,7 +247,10 @@ uint32_t gd_batch_warps(uint32_t max_lane_bytes, uint32_t blocks_per_sm);
  * any order) and fed through the dynamic work queue.  The order array, sort
  * buckets and queue counter live in a fixed device array inside the library
  * (GD_BATCH_NOALLOC_MAX_TASKS tasks at most; more is GD_ERR_INVALID_ARG).
- * Nothing needs zeroing beforehand.  The first call on a device looks up that
+ * +inf costs run first, NaN and -inf costs last.  It serves callers that may
+ * not allocate at decode time: hosts with a fixed, pre-reserved memory budget,
+ * and decode paths that must not pay cudaMalloc / cudaFree's implicit
+ * device-wide synchronisation.  Nothing needs zeroing beforehand.  The first call on a device looks up that
  * array's address (a runtime query, with the device current) and should come
  * before any stream capture.  Calls overlapping in time on one device share
  * the array and race: serialise them.  d_status[n] is written per task.

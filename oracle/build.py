@@ -35,11 +35,22 @@ def build_ref() -> bool:
     False when it is absent so the GPU box, which only uses prebuilt files,
     skips this step.
     """
-    mk = HERE / "ref" / "Makefile"
-    if not Path("/root/reference/include").exists():
+    ref = reference_dir()
+    if ref is None:
         return False
-    subprocess.run(["make", "-s", "-C", str(HERE / "ref")], check=True)
+    subprocess.run(["make", "-s", "-C", str(HERE / "ref"), f"REF={ref}"], check=True)
     return True
+
+
+def reference_dir() -> Path | None:
+    """The reference checkout: $GD_REFERENCE_DIR, else a directory named
+    "reference" beside the repository; None when neither holds include/."""
+    import os
+    cand = [os.environ.get("GD_REFERENCE_DIR"), str(HERE.parent.parent / "reference")]
+    for c in cand:
+        if c and (Path(c) / "include").is_dir():
+            return Path(c).resolve()
+    return None
 
 
 if __name__ == "__main__":

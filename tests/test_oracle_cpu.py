@@ -287,6 +287,102 @@ def test_brle_trans4_encoder_matches_reference_writer():
         assert bytes(lanes[off[r]:off[r + 1]]) == _ref_compress_func_4B(col), trial
 
 
+def _ref_compress_func_1B(col: np.ndarray) -> bytes:
+    """brle_trans::compress_func of include/brle/brle_trans.h:437-562 for one
+    column, restated loop for loop over an output zeroed beforehand: maximal
+    runs, a run of 3 or more as (count, byte), shorter ones as literal bytes,
+    a flag byte per 8 items, and the column's last run written without being
+    counted (:529-536)."""
+    out = bytearray(col.size * 2 + 16)
+    pos = 1                    # byte_offset: header byte 0 reserved
+    hdr, header, blocks = 0, 0, 0
+    counter, prev = 0, None
+
+    def item_done():
+        nonlocal blocks, header, hdr, pos
+        blocks += 1
+        if blocks == 8:
+            out[hdr] = header
+            header = 0
+            hdr = pos
+            pos += 1
+            blocks = 0
+        if blocks != 0:
+            out[hdr] = header
+
+    def put(bs):
+        nonlocal pos
+        out[pos:pos + len(bs)] = bs
+        pos += len(bs)
+
+    for v in col.tolist():
+        if counter == 0:
+            prev = v
+        if prev == v:
+            counter += 1
+            continue
+        if counter >= 3:
+            put(bytes([counter, prev]))
+            item_done()
+        else:
+            for _ in range(counter):
+                header |= 1 << blocks
+                put(bytes([prev]))
+                item_done()
+        counter, prev = 1, v
+    if counter >= 3:           # the last run: written, not counted
+        put(bytes([counter, prev]))
+    else:
+        for _ in range(counter):
+            header |= 1 << blocks
+            put(bytes([prev]))
+            item_done()
+    return bytes(out[:pos])
+
+
+def _byte_column_chunk(col: np.ndarray) -> np.ndarray:
+    """A 4 KiB chunk whose column 0 holds `col` (128 bytes); the other
+    columns are zero."""
+    raw = np.zeros(4096, np.uint8)
+    for k in range(32):
+        raw[128 * k:128 * k + 4] = col[4 * k:4 * k + 4]
+    return raw
+
+
+def _column0_stream(e):
+    r = int(np.nonzero(e.meta["col_map"][:32] == 0)[0][0])
+    lanes, off = oracle.export_lanes(cc.Encoded("lzss", e.data, e.n_out, e.n_chunks, e.chunk_size, e.meta, {}))
+    return bytes(lanes[off[r]:off[r + 1]]), int(e.meta["col_len"][r])
+
+
+def test_brle_trans_last_run_in_slot_8():
+    # 7 literal items, then a final run as the 8th item: written uncounted, so
+    # no flag byte is reserved after it (col_len 1 + 7 + 2)
+    col = np.array([1, 2, 3, 4, 5, 6, 7] + [9] * 121, np.uint8)
+    e = cc.brle_trans_encode(_byte_column_chunk(col), 4096)
+    stream, n = _column0_stream(e)
+    assert n == 10 and stream == _ref_compress_func_1B(col)
+    rc, out = oracle.decode(e)
+    assert rc == 0 and np.array_equal(out, _byte_column_chunk(col))
+    # 8 literal items end a group: the reserved flag byte follows them
+    col = np.array([1, 2, 3, 4, 5, 6, 7, 8] + [9] * 120, np.uint8)
+    e = cc.brle_trans_encode(_byte_column_chunk(col), 4096)
+    stream, n = _column0_stream(e)
+    assert n == 1 + 8 + 1 + 2 and stream == _ref_compress_func_1B(col)
+
+
+def test_brle_trans_encoder_matches_reference_writer():
+    rng = np.random.default_rng(45)
+    for trial in range(400):
+        k = int(rng.integers(1, 5))
+        col = np.repeat(rng.integers(0, k, 128), rng.integers(1, 12, 128))[:128]
+        col = np.resize(col, 128).astype(np.uint8)
+        e = cc.brle_trans_encode(_byte_column_chunk(col), 4096)
+        stream, n = _column0_stream(e)
+        assert stream == _ref_compress_func_1B(col), trial
+        assert n == len(stream)
+
+
 def test_new_containers_reject_corruption():
     raw = cc.gen_markov_copy(5, 20000, 4096)
     e = cc.lzss_contig_encode(raw, 8192)

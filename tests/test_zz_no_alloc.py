@@ -41,6 +41,24 @@ def test_noalloc_matches_batch_decode(cuda):
         torch.cuda.synchronize()
         assert np.array_equal(plan.d_status.cpu().numpy(), want_st)
         assert np.array_equal(plan.d_out.cpu().numpy(), want_out)
+    # non-finite costs: +inf runs first, NaN and -inf last, and the finite
+    # costs still set the bucket range; the output is the same either way
+    rng = np.random.default_rng(5)
+    c = plan.tasks["dst_len"].astype(np.float32)
+    for special in ([np.inf], [np.nan], [-np.inf], [np.inf, -np.inf, np.nan]):
+        cc = c.copy()
+        pick = rng.choice(n, size=max(1, n // 7), replace=False)
+        cc[pick] = rng.choice(np.array(special, np.float32), size=pick.size)
+        for costs in (cc, np.full(n, special[0], np.float32)):
+            cost2 = torch.from_numpy(costs).cuda()
+            plan.d_out.zero_()
+            plan.d_status.fill_(0xFF)
+            rc = lib().gd_batch_decode_lpt_noalloc(p(plan.d_tasks), n, p(cost2), plan.max_lane, 0,
+                                                   p(plan.d_status), s)
+            assert rc == 0
+            torch.cuda.synchronize()
+            assert np.array_equal(plan.d_status.cpu().numpy(), want_st), special
+            assert np.array_equal(plan.d_out.cpu().numpy(), want_out), special
     # more tasks than the fixed array holds: rejected before any launch
     rc = lib().gd_batch_decode_lpt_noalloc(p(plan.d_tasks), MAX_TASKS + 1, p(cost), plan.max_lane, 0,
                                            p(plan.d_status), s)
