@@ -1,23 +1,29 @@
 #!/usr/bin/env python
 """Decode throughput benchmark (one JSON line on rank 0).
 
-Default workload -- byte-RLE + RLE v2 plain decode: a 256 MiB uint8 column of
-runs (geometric mean-20 run length, 16 byte values with Zipf(1.2)
-frequencies) in the brle container with 256 KiB chunks, and a 256 MiB int64
-column of 512-value segments (DELTA / SHORT_REPEAT / DIRECT / PATCHED_BASE
-data) in the RLE v2 transposed container with 256 KiB chunks, READ_UNIT 32.
-A step decodes both columns from HBM to HBM.  Synthetic seeded data stands in
-for the reference's datasets, which are not available.
+Default (--workload all): every decode configuration on one GPU --
+  config 1  RLE v1, 64 MiB int32, 128 KiB chunks, COMP_COL_LEN 128;
+  config 2  byte-RLE 256 MiB uint8 (geometric mean-20 runs, 16 Zipf(1.2)
+            byte values) + RLE v2 256 MiB int64 (512-value DELTA /
+            SHORT_REPEAT / DIRECT / PATCHED_BASE segments), 256 KiB chunks,
+            READ_UNIT 32 -- the step `value` is quoted on;
+  config 3  LZSS, 1 GiB order-2 Markov + copy bytes, 64 KiB chunks;
+  config 4  Deflate/zlib, 1 GiB in 8192 log-uniform chunks, level 6;
+  config 5  the mixed-codec batch under five schedules (`mixed`).
+Each codec's kernel has its own line in `kernels` (CUDA-event time,
+algorithmic bytes, fraction of the measured HBM peak, e2e host call, CPU
+baseline).  Synthetic seeded data stands in for the reference's datasets,
+which are not available.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload brle_rlev2|rlev1|lzss|deflate|mixed|brle_encode|lzss_encode|rlev1_encode|
+                    [--workload all|brle_rlev2|rlev1|lzss|deflate|mixed|brle_encode|lzss_encode|rlev1_encode|
                                rlev2_encode]
-                    [--scale F]
+                    [--scale F] [--no-e2e] [--no-cpu] [--no-mixed]
 
 Multi-GPU (torchrun, one process per GPU): every rank decodes its own copy of
 the workload (independent chunks, no exchange step), weak scaling, time = max
 over ranks.  --impl reference times the reference's CPU decoders on the host
-cores (rank 0 only).
+cores (rank 0 only), on inputs built without this library.
 """
 from __future__ import annotations
 
@@ -53,8 +59,37 @@ def peaks():
 # workloads
 # --------------------------------------------------------------------------
 
+HEADLINE_METRIC = "decompressed GB/s per codec & % of HBM peak at 1 B200; mixed-batch makespan learned vs static"
+HEADLINE = "brle_rlev2"
+LABELS = {
+    "brle_rlev2": "byte-RLE 256 MiB uint8 + RLE v2 256 MiB int64, 256 KiB chunks, READ_UNIT 32",
+    "rlev1": "RLE v1 64 MiB int32, 128 KiB chunks, COMP_COL_LEN 128",
+    "lzss": "LZSS 1 GiB Markov+copy bytes, 64 KiB chunks",
+    "deflate": "Deflate/zlib 1 GiB in 8192 chunks log-uniform 4 KiB-1 MiB, level 6",
+}
+DECODE_WORKLOADS = ("rlev1", "brle_rlev2", "lzss", "deflate")
+L2_NOTE = "flushed between timed steps (256 MiB write)"
+
+
+def run_config(workload: str, world: int) -> dict:
+    """The `config` of a workload's line; identical in both arms."""
+    cfg = {"workload": LABELS.get(workload, workload), "l2": L2_NOTE, "parallelism": f"replicas x{world}"}
+    if workload == HEADLINE:
+        cfg["columns"] = 2
+    return cfg
+
+
+def deflate_modes(n: int) -> np.ndarray:
+    rng = np.random.default_rng(0xD2)
+    mode = np.zeros(n, np.uint8)
+    r = rng.random(n)
+    mode[r < 0.015] = 1
+    mode[(r >= 0.015) & (r < 0.03)] = 2
+    return mode
+
+
 def make_workload(name: str, scale: float = 1.0):
-    """Returns (label, [(codec_name, Encoded, raw_bytes_view)], config dict)."""
+    """Returns ([(codec_name, Encoded, raw_bytes_view)], config label)."""
     import compression_b200.codecs as cc
     if name == "brle_rlev2":
         n = int(256 * MiB * scale)
@@ -62,29 +97,22 @@ def make_workload(name: str, scale: float = 1.0):
         e1 = cc.brle_encode(a, 256 * 1024)
         v = cc.gen_rlev2_ints(0xB1, n // 8)
         e2 = cc.rlev2_encode(v, 256 * 1024, 32)
-        cfg = {"workload": "byte-RLE 256 MiB uint8 + RLE v2 256 MiB int64, 256 KiB chunks, READ_UNIT 32",
-               "columns": 2}
-        return [("brle", e1, a), ("rlev2", e2, v.view(np.uint8))], cfg
+        return [("brle", e1, a), ("rlev2", e2, v.view(np.uint8))]
     if name == "rlev1":
         v = cc.gen_rlev1_ints(0xA0, int(64 * MiB * scale) // 4)
         e = cc.rlev1_encode(v, 128 * 1024, 128, 4)
-        return [("rlev1", e, v.view(np.uint8))], {"workload": "RLE v1 64 MiB int32, 128 KiB chunks, COMP_COL_LEN 128"}
+        return [("rlev1", e, v.view(np.uint8))]
     if name == "lzss":
         a = cc.gen_markov_copy(0xC0, int(GiB * scale), 4096)
         e = cc.lzss_encode(a, 64 * 1024)
-        return [("lzss", e, a)], {"workload": "LZSS 1 GiB Markov+copy bytes, 64 KiB chunks"}
+        return [("lzss", e, a)]
     if name == "deflate":
         total = int(GiB * scale)
         a = cc.gen_markov_copy(0xD0, total, 32768)
         sizes = cc.loguniform_sizes(0xD1, 8192, 4096, MiB, total)
         oo = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
-        rng = np.random.default_rng(0xD2)
-        mode = np.zeros(8192, np.uint8)
-        r = rng.random(8192)
-        mode[r < 0.015] = 1
-        mode[(r >= 0.015) & (r < 0.03)] = 2
-        e = cc.deflate_encode(a, oo, 6, mode, 1)
-        return [("deflate", e, a)], {"workload": "Deflate/zlib 1 GiB in 8192 chunks log-uniform 4 KiB-1 MiB, level 6"}
+        e = cc.deflate_encode(a, oo, 6, deflate_modes(8192), 1)
+        return [("deflate", e, a)]
     raise ValueError(name)
 
 
@@ -157,163 +185,234 @@ def job_rate(bytes_per_rank: int, world: int, ms: float) -> float:
 
 
 # --------------------------------------------------------------------------
-# CPU baselines (oracle restatement or the reference's own code)
+# CPU baselines (the reference's own CPU decoders, or the oracle port)
 # --------------------------------------------------------------------------
-
-def cpu_decode_sample(cols, threads: int, budget_s: float = 10.0):
-    """Decode a bounded prefix of each column on the host cores with the
-    oracle (the checker), in parallel over chunks.  Returns (GB/s of
-    decompressed bytes, description)."""
-    import concurrent.futures as cf
-    import copy
-    import oracle
-    # one sub-container per chunk range; ctypes releases the GIL
-    out_bytes = 0
-    t_total = 0.0
-    descr = []
-    for name, enc, raw in cols:
-        nch = enc.n_chunks
-        # sample size: start with 8 chunks per thread, grow until ~budget/len(cols)
-        take = min(nch, max(threads, 8))
-        per = budget_s / len(cols)
-        while True:
-            parts = _split(enc, take, threads)
-            t0 = time.perf_counter()
-            with cf.ThreadPoolExecutor(threads) as ex:
-                rcs = list(ex.map(lambda e: oracle.decode(e)[0], parts))
-            dt = time.perf_counter() - t0
-            if any(rcs):
-                raise RuntimeError(f"oracle failed on {name}")
-            if dt > per / 4 or take >= nch:
-                break
-            take = min(nch, take * 4)
-        nb = sum(p.n_out for p in parts)
-        out_bytes += nb
-        t_total += dt
-        descr.append(f"{name}: {take}/{nch} chunks ({nb / MiB:.0f} MiB out)")
-    return out_bytes / t_total / 1e9, "; ".join(descr)
-
 
 REF_BIN = ROOT / "oracle" / "_ref"
 
 
-def _ref_container(name, enc, path):
-    """Write enc in the file format of the reference harness's bench mode;
-    returns the harness binary, or None when the codec has no compiled
-    reference CPU decoder."""
+class CpuCol:
+    """One column prepared for a CPU decoder: a reference harness binary and
+    its input file (brle::decode, rlev2::block_decode, lzss::decompress_func,
+    compiled from the reference sources into oracle/_ref), or an oracle
+    container decoded by the oracle (RLE v1, whose reference decoders are
+    GPU-only; Deflate, which the reference decodes on the CPU with zlib)."""
+
+    def __init__(self, name, n_out, exe=None, path=None, cont=None):
+        self.name, self.n_out, self.exe, self.path, self.cont = name, int(n_out), exe, path, cont
+
+    @property
+    def kind(self) -> str:
+        return "reference" if self.exe is not None or self.name == "deflate" else "port"
+
+
+def _write_lanes(path, lanes, off, per):
+    with open(path, "wb") as f:
+        f.write(np.array([off.size - 1, per], dtype=np.uint64).tobytes())
+        f.write(np.ascontiguousarray(off, dtype=np.uint64).tobytes())
+        f.write(lanes.tobytes())
+        f.write(bytes(64))
+
+
+def cpu_cols_from_containers(cols, tmp: Path):
+    """CpuCols over this library's containers (byte-identical to the
+    reference encoders' output for brle, RLE v2 and LZSS): the lane / column
+    streams are exported from the interleaved blocks by the oracle."""
     import oracle
-    m = enc.meta
-    if name == "brle" and (REF_BIN / "ref_brle").exists():
-        ptr = np.ascontiguousarray(m["ptr"], dtype=np.uint64)
-        with open(path, "wb") as f:
-            f.write(np.uint32(ptr.size).tobytes())
-            f.write(ptr.tobytes())
-            f.write(np.uint64(enc.n_out).tobytes())
-            f.write(enc.data.tobytes())
-        return REF_BIN / "ref_brle"
-    if name in ("rlev2", "lzss") and (REF_BIN / f"ref_{name}").exists():
-        lanes, off = oracle.export_lanes(enc)
-        per = enc.chunk_size // 256 if name == "rlev2" else enc.chunk_size // 32
-        with open(path, "wb") as f:
-            f.write(np.array([off.size - 1, per], dtype=np.uint64).tobytes())
-            f.write(off.tobytes())
-            f.write(lanes.tobytes())
-            f.write(bytes(64))
-        return REF_BIN / f"ref_{name}"
-    return None
-
-
-def ref_decode_sample(cols, threads: int, budget_s: float = 10.0, prepared=None):
-    """Decode rate of the reference's own CPU decoders on the host cores.
-
-    byte-RLE: brle::decode per 256 KiB chunk (brle.h:26-100); RLE v2:
-    rlev2::block_decode per lane stream (decoder.h:190); LZSS:
-    lzss::decompress_func per column stream (lzss_cpu.h:110) -- compiled from
-    the reference sources into oracle/_ref, run on `threads` host threads over
-    the whole column, repeated for the time budget.  Codecs without a compiled
-    reference decoder (RLE v1, whose decoders are GPU-only; Deflate, which the
-    reference decodes on the CPU with zlib) fall back to the oracle, whose
-    Deflate path is system zlib.  Returns (GB/s, description, kind,
-    prepared) where GB/s is the rate of decoding all columns one after the
-    other."""
-    prepared = prepared if prepared is not None else {}
-    t_total, b_total, descr, kinds = 0.0, 0, [], []
-    per = budget_s / len(cols)
-    for name, enc, raw in cols:
-        if name not in prepared:
-            path = Path(tempfile.mkdtemp()) / f"{name}.bin"
-            prepared[name] = (_ref_container(name, enc, path), path)
-        exe, path = prepared[name]
-        if exe is not None:
-            r = subprocess.run([str(exe), "bench", str(path), str(threads), str(per)], capture_output=True,
-                               text=True, check=True, timeout=120 + 4 * per)
-            nb, dt = r.stdout.split()
-            rate = int(nb) / float(dt)
-            kinds.append("reference")
-            descr.append(f"{name}: reference {exe.name} over the whole column ({enc.n_out / MiB:.0f} MiB), "
-                         f"repeated {int(nb) // max(enc.n_out, 1)}x")
-        else:
-            gbs, d = cpu_decode_sample([(name, enc, raw)], threads, budget_s=per)
-            rate = gbs * 1e9
-            kinds.append("reference" if name == "deflate" else "port")
-            descr.append(("zlib inflate: " if name == "deflate" else "oracle port: ") + d)
-        t_total += enc.n_out / rate
-        b_total += enc.n_out
-    kind = kinds[0] if len(set(kinds)) == 1 else "mixed"
-    return b_total / t_total / 1e9, "; ".join(descr), kind, prepared
-
-
-def _split(enc, take, threads):
-    """Sub-containers of the first `take` chunks, split into `threads` parts."""
-    import compression_b200.codecs as cc
     res = []
-    bounds = np.linspace(0, take, threads + 1).astype(int)
-    for a, b in zip(bounds[:-1], bounds[1:]):
-        if b <= a:
-            continue
-        res.append(_sub(enc, int(a), int(b)))
+    for name, enc, raw in cols:
+        path = tmp / f"{name}.bin"
+        if name == "brle" and (REF_BIN / "ref_brle").exists():
+            ptr = np.ascontiguousarray(enc.meta["ptr"], dtype=np.uint64)
+            with open(path, "wb") as f:
+                f.write(np.uint32(ptr.size).tobytes())
+                f.write(ptr.tobytes())
+                f.write(np.uint64(enc.n_out).tobytes())
+                f.write(enc.data.tobytes())
+            res.append(CpuCol(name, enc.n_out, REF_BIN / "ref_brle", path))
+        elif name in ("rlev2", "lzss") and (REF_BIN / f"ref_{name}").exists():
+            lanes, off = oracle.export_lanes(enc)
+            per = enc.chunk_size // 256 if name == "rlev2" else enc.chunk_size // 32
+            _write_lanes(path, lanes, off, per)
+            res.append(CpuCol(name, enc.n_out, REF_BIN / f"ref_{name}", path))
+        else:
+            res.append(CpuCol(name, enc.n_out, cont=_as_container(enc)))
     return res
 
 
-def _sub(enc, a, b):
-    import compression_b200.codecs as cc
-    m = enc.meta
-    cs = enc.chunk_size
-    if enc.codec == "brle":
-        p = m["ptr"]
-        data = enc.data[int(p[a]):int(p[b])]
-        ptr = (p[a:b + 1] - p[a]).astype(np.uint64)
-        n_out = min(enc.n_out, b * cs) - a * cs
-        return cc.Encoded("brle", data, n_out, b - a, cs, {"ptr": ptr})
-    if enc.codec in ("rlev1", "rlev2", "lzss"):
+def _as_container(enc):
+    import oracle
+    return oracle.Container(enc.codec, enc.data, enc.n_out, enc.n_chunks, enc.chunk_size, dict(enc.meta),
+                            {k: v for k, v in enc.params.items() if not k.startswith("_")})
+
+
+def _zlib_streams(raw: np.ndarray, oo: np.ndarray, modes: np.ndarray, threads: int):
+    """Config 4's zlib streams written by Python's zlib (the reference's own
+    producer, orig_compressor.py:87), each padded to 8 bytes."""
+    import concurrent.futures as cf
+    import zlib
+
+    def one(i):
+        b = raw[int(oo[i]):int(oo[i + 1])].tobytes()
+        if modes[i] == 1:
+            co = zlib.compressobj(6, zlib.DEFLATED, 15, 8, zlib.Z_FIXED)
+        else:
+            co = zlib.compressobj(0 if modes[i] == 2 else 6)
+        return co.compress(b) + co.flush()
+
+    with cf.ThreadPoolExecutor(threads) as ex:
+        streams = list(ex.map(one, range(oo.size - 1)))
+    clen = np.array([len(z) for z in streams], np.uint64)
+    padded = (clen + 7) // 8 * 8
+    coff = np.concatenate([[0], np.cumsum(padded)]).astype(np.uint64)
+    data = np.zeros(int(coff[-1]), np.uint8)
+    for z, o in zip(streams, coff[:-1]):
+        data[int(o):int(o) + len(z)] = np.frombuffer(z, np.uint8)
+    return data, coff, clen
+
+
+def cpu_cols_reference(workload: str, scale: float, tmp: Path, threads: int):
+    """CpuCols of a workload built without this library: the oracle's copy of
+    the seeded generators, then the reference's own encoders (brle::encode;
+    rlev2::block_encode per lane stream; lzss::compress_func per column, all
+    from oracle/_ref), Python's zlib for Deflate, and for RLE v1 -- whose
+    only reference encoder is the GPU writer -- the oracle's input builder."""
+    import oracle
+
+    def run(*a):
+        subprocess.run([str(x) for x in a], check=True, capture_output=True, timeout=900)
+
+    res = []
+    if workload == "brle_rlev2":
+        n = int(256 * MiB * scale)
+        a = oracle.gen_brle_bytes(0xB0, n)
+        rawp, cont = tmp / "brle.raw", tmp / "brle.bin"
+        a.tofile(rawp)
+        run(REF_BIN / "ref_brle", "encode", rawp, cont)
+        res.append(CpuCol("brle", n, REF_BIN / "ref_brle", cont))
+        v = oracle.gen_rlev2_ints(0xB1, n // 8)
+        cs, ru = 256 * 1024, 32
+        nc = v.size * 8 // cs
+        # lane t of chunk c holds values c*CS/8 + t*RU + k*32*RU + j, j < RU
+        lanes = v[:nc * cs // 8].reshape(nc, cs // 8 // (32 * ru), 32, ru).transpose(0, 2, 1, 3)
+        vp_ = tmp / "rlev2.raw"
+        np.ascontiguousarray(lanes).tofile(vp_)
+        run(REF_BIN / "ref_rlev2", "encode_lanes", vp_, cs // 256, threads, tmp / "rlev2.bin")
+        res.append(CpuCol("rlev2", v.size * 8, REF_BIN / "ref_rlev2", tmp / "rlev2.bin"))
+    elif workload == "rlev1":
+        v = oracle.gen_rlev1_ints(0xA0, int(64 * MiB * scale) // 4)
+        res.append(CpuCol("rlev1", v.nbytes, cont=oracle.rlev1_encode(v, 128 * 1024, 128, 4)))
+    elif workload == "lzss":
+        cs = 64 * 1024
+        a = oracle.gen_markov_copy(0xC0, int(GiB * scale), 4096)
+        nc = a.size // cs
+        # column q of a chunk = bytes 4q + 128k .. +3
+        cols = a[:nc * cs].reshape(nc, cs // 128, 32, 4).transpose(0, 2, 1, 3)
+        cp = tmp / "lzss.raw"
+        np.ascontiguousarray(cols).tofile(cp)
+        run(REF_BIN / "ref_lzss", "encode_lanes", cp, cs // 32, threads, tmp / "lzss.bin")
+        res.append(CpuCol("lzss", nc * cs, REF_BIN / "ref_lzss", tmp / "lzss.bin"))
+    elif workload == "deflate":
+        total = int(GiB * scale)
+        a = oracle.gen_markov_copy(0xD0, total, 32768)
+        sizes = oracle.loguniform_sizes(0xD1, 8192, 4096, MiB, total)
+        oo = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+        data, coff, clen = _zlib_streams(a, oo, deflate_modes(8192), threads)
+        res.append(CpuCol("deflate", total, cont=oracle.Container(
+            "deflate", data, total, 8192, 0, {"comp_off": coff, "comp_len": clen, "out_off": oo},
+            {"zlib_header": 1})))
+    else:
+        raise ValueError(workload)
+    return res
+
+
+def _sub(cont, a, b):
+    """Chunks [a, b) of an oracle container as a container of their own."""
+    import oracle
+    m, cs = cont.meta, cont.chunk_size
+    if cont.codec in ("rlev1", "rlev2", "lzss"):
         bo = m["blk_off"]
-        data = enc.data[int(bo[a]):int(bo[b])]
         meta = {"blk_off": (bo[a:b + 1] - bo[a]).astype(np.uint64), "col_len": m["col_len"][32 * a:32 * b]}
         if "col_map" in m:
             meta["col_map"] = m["col_map"][32 * a:32 * b]
-        n_out = min(enc.n_out, b * cs) - a * cs
-        return cc.Encoded(enc.codec, data, n_out, b - a, cs, meta, dict(enc.params))
-    if enc.codec == "deflate":
+        n_out = min(cont.n_out, b * cs) - a * cs
+        return oracle.Container(cont.codec, cont.data[int(bo[a]):int(bo[b])], n_out, b - a, cs, meta,
+                                dict(cont.params))
+    if cont.codec == "deflate":
         co, cl, oo = m["comp_off"], m["comp_len"], m["out_off"]
-        data = enc.data[int(co[a]):int(co[b])]
         meta = {"comp_off": (co[a:b + 1] - co[a]).astype(np.uint64), "comp_len": cl[a:b],
                 "out_off": (oo[a:b + 1] - oo[a]).astype(np.uint64)}
-        return cc.Encoded("deflate", data, int(oo[b] - oo[a]), b - a, 0, meta, dict(enc.params))
-    raise ValueError(enc.codec)
+        return oracle.Container("deflate", cont.data[int(co[a]):int(co[b])], int(oo[b] - oo[a]), b - a, 0, meta,
+                                dict(cont.params))
+    raise ValueError(cont.codec)
+
+
+def oracle_rate(cont, threads: int, budget_s: float):
+    """Decode rate of the oracle over a growing prefix of the container's
+    chunks, split over `threads` host threads (ctypes releases the GIL), until
+    one pass takes about a quarter of the budget.  Returns (bytes/s, text)."""
+    import concurrent.futures as cf
+    import oracle
+    nch = cont.n_chunks
+    take = min(nch, max(threads, 8))
+    while True:
+        bounds = np.linspace(0, take, threads + 1).astype(int)
+        parts = [_sub(cont, int(x), int(y)) for x, y in zip(bounds[:-1], bounds[1:]) if y > x]
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(threads) as ex:
+            rcs = list(ex.map(lambda e: oracle.decode(e)[0], parts))
+        dt = time.perf_counter() - t0
+        if any(rcs):
+            raise RuntimeError(f"oracle failed on {cont.codec}")
+        if dt > budget_s / 4 or take >= nch:
+            break
+        take = min(nch, take * 4)
+    nb = sum(p.n_out for p in parts)
+    return nb / dt, f"{take}/{nch} chunks ({nb / MiB:.0f} MiB out)"
+
+
+def cpu_rates(ccols, threads: int, budget_s: float):
+    """Per column: (bytes/s, description, kind) of its CPU decoder on
+    `threads` host threads, each for about budget_s / len(ccols) seconds."""
+    per = budget_s / max(len(ccols), 1)
+    res = []
+    for c in ccols:
+        if c.exe is not None:
+            r = subprocess.run([str(c.exe), "bench", str(c.path), str(threads), str(per)], capture_output=True,
+                               text=True, check=True, timeout=120 + 4 * per)
+            nb, dt = r.stdout.split()
+            rate = int(nb) / float(dt)
+            descr = (f"{c.name}: reference {c.exe.name} over the whole column ({c.n_out / MiB:.0f} MiB), "
+                     f"repeated {int(nb) // max(c.n_out, 1)}x")
+        else:
+            rate, d = oracle_rate(c.cont, threads, per)
+            descr = ("zlib inflate: " if c.name == "deflate" else "oracle port: ") + d
+        res.append((rate, descr, c.kind))
+    return res
+
+
+def combined_rate(ccols, rates):
+    """GB/s of decoding all the columns one after the other."""
+    t = sum(c.n_out / r for c, (r, _, _) in zip(ccols, rates))
+    kinds = {k for _, _, k in rates}
+    return sum(c.n_out for c in ccols) / t / 1e9, "; ".join(d for _, d, _ in rates), \
+        kinds.pop() if len(kinds) == 1 else "mixed"
 
 
 # --------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------
 
-def run_ours(args, rank, world, local_rank):
+def time_decode(workload, args, world, dev, clk_samples):
+    """One decode workload on this GPU: parity of the benchmarked data, then
+    `steps` timed steps (CUDA events per kernel on the launching stream, L2
+    flushed between steps), the concurrent-stream step for multi-column
+    workloads, the e2e host call and the CPU baseline.  Returns a dict."""
     import torch
     import compression_b200.codecs as cc
-    import compression_b200 as cb
-
-    dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
-    cols, cfg = make_workload(args.workload, args.scale)
+    t_prep = time.perf_counter()
+    cols = make_workload(workload, args.scale)
+    t_prep = time.perf_counter() - t_prep
     jobs = [cc.DeviceJob(e, dev) for _, e, _ in cols]
     stream = torch.cuda.current_stream(dev)
 
@@ -351,11 +450,12 @@ def run_ours(args, rank, world, local_rank):
     K = args.steps
     evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in jobs] for _ in range(K)]
     torch.cuda.synchronize()
-    with Clocks(local_rank) as clk:
+    with Clocks(dev.index or 0) as clk:
         for k in range(K):
             flush.zero_()     # L2 flushed between timed steps, outside the events
             step(evs[k])
         torch.cuda.synchronize()
+    clk_samples.extend(clk.samples)
     per_kernel = [[evs[k][i][0].elapsed_time(evs[k][i][1]) for k in range(K)] for i in range(len(jobs))]
     step_ms = [sum(per_kernel[i][k] for i in range(len(jobs))) for k in range(K)]
     serial_ms = statistics.mean(step_ms)
@@ -386,37 +486,31 @@ def run_ours(args, rank, world, local_rank):
             cstep()
         torch.cuda.synchronize()
         cev = [[None, torch.cuda.Event(enable_timing=True)] for _ in range(K)]
-        with Clocks(local_rank) as clk2:
+        with Clocks(dev.index or 0) as clk2:
             for k in range(K):
                 flush.zero_()
                 cstep(cev[k])
             torch.cuda.synchronize()
+        clk_samples.extend(clk2.samples)
         conc_ms = statistics.mean(c[0].elapsed_time(c[1]) for c in cev)
         launches += len(jobs) * K
-        if clk2.samples:
-            clk.samples.extend(clk2.samples)
     ms = max_over_ranks([conc_ms if conc_ms is not None else serial_ms], world, dev)[0]
     out_bytes = sum(e.n_out for _, e, _ in cols)
-    value = job_rate(out_bytes, world, ms)
 
-    # roofline of the dominant kernel: algorithmic bytes = compressed payload
-    # + metadata read + decompressed bytes written, per launch
+    # per-kernel roofline: algorithmic bytes = compressed payload + metadata
+    # read + decompressed bytes written, per launch, over the kernel's
+    # CUDA-event time
     peak, peak_kind = peaks()
     kern = []
     for i, (name, e, _) in enumerate(cols):
-        kms = statistics.mean(per_kernel[i])
+        kms = max_over_ranks([statistics.mean(per_kernel[i])], world, dev)[0]
         alg = e.comp_bytes + e.meta_bytes + e.n_out
-        kern.append({"kernel": name, "ms": round(kms, 4), "alg_bytes": alg,
-                     "gbs": round(alg / (kms / 1e3) / 1e9, 1),
-                     "decomp_gbs": round(e.n_out / (kms / 1e3) / 1e9, 1),
-                     "ratio": round(e.comp_bytes / max(e.n_out, 1), 4)})
-    dom = max(kern, key=lambda k: k["ms"])
-    traffic = None
-    tp = ROOT / "profiles" / "dram_traffic.json"
-    if tp.exists() and args.scale == 1.0:
-        t = json.loads(tp.read_text()).get(args.workload, {}).get(dom["kernel"])
-        if t:
-            traffic = int(t["read"] + t["write"])
+        gbs = alg / (kms / 1e3) / 1e9
+        kern.append({"kernel": name, "workload": LABELS[workload], "ms": round(kms, 4), "alg_bytes": alg,
+                     "gbs": round(gbs, 1), "frac": round(gbs / peak, 4), "decomp_gbs": round(e.n_out / (kms / 1e3) / 1e9, 1),
+                     "ratio": round(e.comp_bytes / max(e.n_out, 1), 4),
+                     "parity": "bit-exact against the input column (the oracle where the reference's encoder "
+                               "does not round-trip)"})
 
     # e2e: the reference-shaped host call (host buffers; H2D + decode + D2H inside)
     e2e = None
@@ -435,31 +529,109 @@ def run_ours(args, rank, world, local_rank):
         e2e = {"value": round(job_rate(out_bytes, world, e2e_s * 1e3), 3), "unit": "GB/s",
                "h2d_bytes_per_step": int(tot_h2d), "d2h_bytes_per_step": int(out_bytes),
                "path": "gd_*_decompress host C-ABI calls (pinned host buffers)"}
+    res = {"workload": workload, "ms": ms, "serial_ms": serial_ms, "conc": conc_ms is not None,
+           "value": job_rate(out_bytes, world, ms), "out_bytes": out_bytes, "kernels": kern, "e2e": e2e,
+           "launches": launches, "prep_s": t_prep, "cols": cols}
+    del jobs, flush
+    torch.cuda.empty_cache()
+    return res
 
+
+def attach_cpu(res, threads, budget_s):
+    """cpu_baseline of a workload (and of each of its kernels) from the
+    reference's own CPU decoders on this library's containers."""
+    with tempfile.TemporaryDirectory() as td:
+        ccols = cpu_cols_from_containers(res["cols"], Path(td))
+        rates = cpu_rates(ccols, threads, budget_s)
+    for k, (r, d, kind) in zip(res["kernels"], rates):
+        k["cpu_baseline"] = {"value": round(r / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind, "sample": d}
+    gbs, sample, kind = combined_rate(ccols, rates)
+    res["cpu_baseline"] = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind, "sample": sample}
+
+
+def run_ours(args, rank, world, local_rank):
+    """One decode workload (--workload rlev1 / brle_rlev2 / lzss / deflate)."""
+    import torch
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    samples = []
+    r = time_decode(args.workload, args, world, dev, samples)
+    if rank == 0 and not args.no_cpu:
+        attach_cpu(r, os.cpu_count() or 1, 10.0)
+    return decode_line(args, world, r, samples)
+
+
+def decode_line(args, world, r, samples, metric=None):
+    peak, peak_kind = peaks()
+    dom = max(r["kernels"], key=lambda k: k["ms"])
+    traffic = None
+    tp = ROOT / "profiles" / "dram_traffic.json"
+    if tp.exists() and args.scale == 1.0:
+        t = json.loads(tp.read_text()).get(r["workload"], {}).get(dom["kernel"])
+        if t:
+            traffic = int(t["read"] + t["write"])
+    clk = Clocks(0)
+    clk.samples = samples
     line = {
-        "metric": "decompressed GB/s (byte-RLE + RLE v2 columns)" if args.workload == "brle_rlev2"
-        else f"decompressed GB/s ({args.workload})",
-        "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
-        "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u8/int64" if args.workload == "brle_rlev2" else "u8", "data": "synthetic (seeded generators)",
-        "config": dict(cfg, l2="flushed between timed steps (256 MiB write)", parallelism=f"replicas x{world}"),
+        "metric": metric or f"decompressed GB/s ({r['workload']})",
+        "value": round(r["value"], 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(r["ms"], 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8/int64" if r["workload"] == HEADLINE else ("u32" if r["workload"] == "rlev1" else "u8"),
+        "data": "synthetic (seeded generators)",
+        "config": run_config(r["workload"], world),
         "roofline": {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["gbs"], "peak": peak,
-                     "unit": "GB/s", "frac": round(dom["gbs"] / peak, 4), "peak_source": peak_kind,
+                     "unit": "GB/s", "frac": dom["frac"], "peak_source": peak_kind,
                      "traffic": traffic, "alg_bytes": dom["alg_bytes"],
                      "traffic_source": "profiles/dram_traffic.json (ncu capture of this workload)" if traffic
                      else None},
-        "kernels": kern,
-        "gpu_launches": launches,
-        "step": f"columns decoded on concurrent streams (one after the other: {serial_ms:.4f} ms)"
-        if conc_ms is not None else "one column",
+        "kernels": r["kernels"],
+        "gpu_launches": r["launches"],
+        "step": f"columns decoded on concurrent streams (one after the other: {r['serial_ms']:.4f} ms)"
+        if r["conc"] else "one column",
         "clocks": clk.summary(),
-        "e2e": e2e,
+        "e2e": r["e2e"],
     }
-    if rank == 0 and not args.no_cpu:
-        threads = os.cpu_count() or 1
-        gbs, sample, kind, _ = ref_decode_sample(cols, threads)
-        line["cpu_baseline"] = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-                                "sample": sample}
+    if "cpu_baseline" in r:
+        line["cpu_baseline"] = r["cpu_baseline"]
+    return line
+
+
+def run_all(args, rank, world, local_rank):
+    """The default run: every decode configuration and the mixed batch.
+
+    `value`, `e2e`, `roofline` and `cpu_baseline` are the byte-RLE + RLE v2
+    step (the configuration the metric is quoted on); `kernels` holds every
+    codec's kernel (configs 1-4) with its own roofline fraction, e2e and CPU
+    baseline; `mixed` holds config 5's makespans (static mapping, FIFO queue,
+    size-ordered longest-first, learned longest-first)."""
+    import torch
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    threads = os.cpu_count() or 1
+    samples = []
+    res = {}
+    for w in (HEADLINE, "rlev1", "lzss", "deflate"):
+        res[w] = time_decode(w, args, world, dev, samples)
+        if rank == 0 and not args.no_cpu:
+            attach_cpu(res[w], threads, 8.0 if w == HEADLINE else 5.0)
+        res[w].pop("cols")
+    head = res[HEADLINE]
+    line = decode_line(args, world, head, samples, metric=HEADLINE_METRIC)
+    kern = []
+    for w in ("rlev1", HEADLINE, "lzss", "deflate"):
+        for k in res[w]["kernels"]:
+            if w != HEADLINE and res[w]["e2e"]:
+                k["e2e_gbs"] = res[w]["e2e"]["value"]
+            kern.append(k)
+    line["kernels"] = kern
+    line["gpu_launches"] = sum(r["launches"] for r in res.values())
+    if not args.no_mixed:
+        m = mixed_run(args, rank, world, local_rank, samples)
+        line["mixed"] = m
+        line["gpu_launches"] += m.pop("launches")
+    clk = Clocks(0)
+    clk.samples = samples
+    line["clocks"] = clk.summary()
     return line
 
 
@@ -467,20 +639,39 @@ def run_ours(args, rank, world, local_rank):
 # mixed-codec batch with the learned scheduler
 # --------------------------------------------------------------------------
 
-def run_mixed(args, rank, world, local_rank):
-    """Mixed-codec batch: 16384 items (log-uniform 4 KiB - 2 MiB, 4 GiB
-    decompressed in all; 20% RLE v1, 20% RLE v2, 10% byte-RLE, 25% LZSS, 25%
-    Deflate) decoded in one persistent launch.  The cost model is trained on
-    the decoder's own per-task timings (random task orders) during warm-up;
-    the timed step is the CUDA-graph replay of [MLP inference -> longest-first
-    order -> batch decode].  The static mapping (task i -> warp i mod W) and
-    the plain FIFO work queue are timed beside it on the same data."""
+MIXED_LABEL = ("mixed batch: {n} items log-uniform 4 KiB-2 MiB, {gib:.2f} GiB decompressed, 20/20/10/25/25% "
+               "RLE v1/RLE v2/byte-RLE/LZSS/Deflate")
+
+
+def task_bytes(plan):
+    """Bytes each task writes and reads (an RLE lane task writes 1/32 of its
+    chunk and reads its own lane stream)."""
+    import compression_b200.batch as B
+    X = B.task_features(plan)
+    return np.exp2(X[:, 6].astype(np.float64)) - 1.0, np.exp2(X[:, 5].astype(np.float64)) - 1.0
+
+
+def mixed_run(args, rank, world, local_rank, clk_samples):
+    """Config 5, the mixed-codec batch: 16384 items (log-uniform 4 KiB - 2 MiB,
+    4 GiB decompressed in all; 20% RLE v1, 20% RLE v2, 10% byte-RLE, 25% LZSS,
+    25% Deflate) decoded in one persistent launch under five schedules:
+
+    * static: task i on warp i mod W (the fallback);
+    * queue_fifo: the dynamic work queue in task order;
+    * size_lpt_out / size_lpt_in: longest-first through the queue with the
+      task's decompressed / compressed bytes as its cost (the method without
+      the network);
+    * learned_lpt: longest-first by the cost model's prediction, as one
+      CUDA-graph replay of [MLP inference -> order -> batch decode].
+
+    The cost model is trained on a separate, quarter-size batch of the same
+    mix (other seeds), on 200k+ per-task decode times that the batch decoder
+    measures itself in random task orders; it is evaluated on this batch."""
     import torch
     import compression_b200.batch as B
     import compression_b200.costmodel as CM
 
     dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
     n_items = max(64, int(16384 * args.scale))
     total = int(4 * GiB * args.scale)
     t0 = time.perf_counter()
@@ -511,48 +702,55 @@ def run_mixed(args, rank, world, local_rank):
     if not B.verify(plan, expect):
         raise RuntimeError("mixed batch: GPU output differs from the reference decoder")
     n_quirk = len(expect)
+    del out
 
-    # ---- training data: self-measured per-task times, random orders ----
-    X = B.task_features(plan)
+    # ---- cost model: trained on a separate batch's self-measured task times ----
     t0 = time.perf_counter()
-    ys, samples = [], 0
-    seed = 0
-    while samples < 200_000 or len(ys) < 2:
-        ys.append(np.log(np.maximum(CM.measure_tasks(plan, seed=seed), 1.0)))
-        samples += n_tasks
+    titems = B.make_mixed_batch(0xF0 + rank, max(64, n_items // 4), max(total // 4, 64 * MiB), 4096, 2 * MiB)
+    tplan = B.build_plan(titems, dev)
+    Xt = B.task_features(tplan)
+    ys, n_samples, seed = [], 0, 0
+    while n_samples < 200_000 or len(ys) < 2:
+        ys.append(np.log(np.maximum(CM.measure_tasks(tplan, seed=seed), 1.0)))
+        n_samples += tplan.tasks.size
         seed += 1
     model = CM.CostModel(seed=0, device=dev)
-    Xtr = np.concatenate([X] * len(ys))
-    ytr = np.concatenate(ys)
-    losses = model.train(Xtr, ytr, epochs=8, batch=256, lr=3e-3)
+    losses = model.train(np.concatenate([Xt] * len(ys)), np.concatenate(ys), epochs=8, batch=256, lr=3e-3)
     t_train = time.perf_counter() - t0
+    del tplan, titems
+    X = B.task_features(plan)
+    y_eval = np.log(np.maximum(CM.measure_tasks(plan, seed=99), 1.0))
     pred = model.predict(X)
-    corr = float(np.corrcoef(pred, ys[0])[0, 1])
+    corr = float(np.corrcoef(pred, y_eval)[0, 1])
     graph = CM.GraphSchedule(plan, model, X)
+    out_b, in_b = task_bytes(plan)
+    orders = {"size_lpt_out": CM.lpt_order(out_b), "size_lpt_in": CM.lpt_order(in_b)}
 
     flush = torch.empty(256 * MiB, dtype=torch.uint8, device=dev)
-    fifo = None
+    kinds = ("learned_lpt", "static", "queue_fifo", "size_lpt_out", "size_lpt_in")
 
     def run(kind):
         if kind == "static":
             B.launch(plan, None, dynamic=False, timing=False)
-        elif kind == "queue":
-            B.launch(plan, fifo, dynamic=True, timing=False)
-        else:
+        elif kind == "queue_fifo":
+            B.launch(plan, None, dynamic=True, timing=False)
+        elif kind == "learned_lpt":
             graph.replay()
+        else:
+            B.launch(plan, orders[kind], dynamic=True, timing=False)
 
     for _ in range(args.warmup):
-        for kind in ("static", "queue", "learned"):
+        for kind in kinds:
             flush.zero_()
             run(kind)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     K = args.steps
-    times = {"static": [], "queue": [], "learned": []}
+    times = {k: [] for k in kinds}
     with Clocks(local_rank) as clk:
         for _ in range(K):
-            for kind in ("learned", "static", "queue"):
+            for kind in kinds:
                 flush.zero_()
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record()
@@ -560,17 +758,17 @@ def run_mixed(args, rank, world, local_rank):
                 b.record()
                 torch.cuda.synchronize()
                 times[kind].append(a.elapsed_time(b))
-    med = {k: statistics.median(v) for k, v in times.items()}
-    ms, med["static"], med["queue"] = max_over_ranks([med["learned"], med["static"], med["queue"]], world, dev)
-    plan.d_out.zero_()
-    graph.replay()
-    torch.cuda.synchronize()
-    if not B.verify(plan, expect):
-        raise RuntimeError("mixed batch: learned schedule output differs")
-    value = job_rate(out_bytes, world, ms)
+    clk_samples.extend(clk.samples)
+    med = dict(zip(kinds, max_over_ranks([statistics.median(times[k]) for k in kinds], world, dev)))
+    for kind in kinds:  # every schedule decodes the batch bit-exact
+        plan.d_out.zero_()
+        run(kind)
+        torch.cuda.synchronize()
+        if not B.verify(plan, expect):
+            raise RuntimeError(f"mixed batch: {kind} schedule output differs")
+    ms = med["learned_lpt"]
     peak, peak_kind = peaks()
-    alg = comp_bytes + out_bytes
-    ach = alg / (ms / 1e3) / 1e9
+    ach = (comp_bytes + out_bytes) / (ms / 1e3) / 1e9
 
     e2e = None
     if not args.no_e2e:
@@ -627,37 +825,50 @@ def run_mixed(args, rank, world, local_rank):
                "path": "batch API: pinned arenas H2D, graph replay, output arena D2H; two batches in flight "
                        "(copy-out of step k overlaps copy-in and decode of step k+1)",
                "steps": K2}
-        del plan2, graph2
+        del plan2, graph2, h_in, h_meta, h_out
 
-    line = {
-        "metric": "mixed-batch decompressed GB/s (learned longest-first schedule)",
-        "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
-        "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u8/int32/int64", "data": "synthetic (seeded generators)",
-        "config": {"workload": f"mixed batch: {n_items} items log-uniform 4 KiB-2 MiB, "
-                               f"{out_bytes / GiB:.2f} GiB decompressed, 20/20/10/25/25% "
-                               "RLE v1/RLE v2/byte-RLE/LZSS/Deflate", "tasks": int(n_tasks),
-                   "warps": B.n_warps(plan), "l2": "flushed between timed launches (256 MiB write)",
-                   "parallelism": f"replicas x{world}"},
-        "makespan_ms": {"static": round(med["static"], 3), "queue_fifo": round(med["queue"], 3),
-                        "learned_lpt": round(ms, 3)},
+    res = {
+        "workload": MIXED_LABEL.format(n=n_items, gib=out_bytes / GiB), "tasks": int(n_tasks),
+        "warps": B.n_warps(plan), "value": round(job_rate(out_bytes, world, ms), 2), "unit": "GB/s",
+        "makespan_ms": {k: round(v, 3) for k, v in med.items()},
         "learned_gain_vs_static": round(1.0 - ms / med["static"], 4),
-        "cost_model": {"samples": int(len(ytr)), "epochs": 8, "final_loss": round(float(losses[-1]), 4),
-                       "corr_pred_measured": round(corr, 4), "train_s": round(t_train, 1)},
+        "learned_gain_vs_size_lpt_out": round(1.0 - ms / med["size_lpt_out"], 4),
+        "learned_gain_vs_size_lpt_in": round(1.0 - ms / med["size_lpt_in"], 4),
+        "cost_model": {"train_batch": "separate quarter-size batch of the same mix (other seeds)",
+                       "samples": int(sum(y.size for y in ys)), "epochs": 8, "final_loss": round(float(losses[-1]), 4),
+                       "corr_pred_measured_eval_batch": round(corr, 4), "train_s": round(t_train, 1)},
         "roofline": {"bound": "hbm", "kernel": "batch", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(ach / peak, 4), "peak_source": peak_kind, "traffic": None},
-        "gpu_launches": 2 * K,
-        "clocks": clk.summary(),
-        "e2e": e2e,
-        "build_s": round(t_build, 1),
+                     "frac": round(ach / peak, 4), "peak_source": peak_kind, "alg_bytes": int(comp_bytes + out_bytes)},
+        "e2e": e2e, "build_s": round(t_build, 1),
         "parity": {"items": len(items), "checked_against": "input column; reference decoder (oracle) for "
-                   f"{n_quirk} RLE v2 items its own encoder does not round-trip"},
+                   f"{n_quirk} RLE v2 items its own encoder does not round-trip", "schedules": "all bit-exact"},
+        "launches": len(kinds) * K,
     }
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        gbs, sample = mixed_cpu_sample(items, threads, 10.0)
-        line["cpu_baseline"] = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
-                                "sample": sample}
+        gbs, sample = mixed_cpu_sample(items, threads, 6.0)
+        res["cpu_baseline"] = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                               "sample": sample}
+    del graph, plan, orders, flush
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_mixed(args, rank, world, local_rank):
+    """--workload mixed: config 5 alone, as its own line."""
+    import torch
+    torch.cuda.set_device(torch.device("cuda", local_rank))
+    samples = []
+    m = mixed_run(args, rank, world, local_rank, samples)
+    clk = Clocks(0)
+    clk.samples = samples
+    line = {"metric": "mixed-batch decompressed GB/s (learned longest-first schedule)", "value": m["value"],
+            "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": m["makespan_ms"]["learned_lpt"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8/int32/int64", "data": "synthetic (seeded generators)",
+            "config": {"workload": m["workload"], "l2": L2_NOTE, "parallelism": f"replicas x{world}"},
+            "gpu_launches": m.pop("launches"), "clocks": clk.summary()}
+    line.update({k: v for k, v in m.items() if k not in ("workload", "value", "unit")})
     return line
 
 
@@ -854,50 +1065,85 @@ def run_encode(args, rank, world, local_rank):
     return line
 
 
-def run_reference(args):
-    """The reference's own CPU decoders (oracle/_ref, compiled from the
-    reference sources) on all host cores; the oracle port for codecs whose
-    reference decoders are GPU-only."""
+def run_reference(args, world):
+    """The reference's own CPU decoders on all host cores, on inputs built
+    without this library (cpu_cols_reference).  `value` is the byte-RLE +
+    RLE v2 step (the configuration the metric is quoted on), each step a
+    bounded sample: both columns decoded in full, repeated for about 3 s;
+    with the default workload, `kernels` adds every other codec's rate."""
     threads = os.cpu_count() or 1
-    vals, prep = [], None
-    if args.workload == "mixed":
-        import compression_b200.batch as B
-        n_items = max(64, int(16384 * args.scale))
-        items = B.make_mixed_batch(0xE0, n_items, int(4 * GiB * args.scale), 4096, 2 * MiB)
-        cfg = {"workload": f"mixed-codec batch, {n_items} items, {4 * args.scale:g} GiB decompressed"}
-        for _ in range(args.warmup):
-            mixed_cpu_sample(items, threads, 1.0)
-        for _ in range(args.steps):
-            gbs, sample = mixed_cpu_sample(items, threads, 4.0)
-            vals.append(gbs)
-        kind = "port"
-    elif args.workload.endswith("_encode"):
-        codec, raw, kw, chunk, label = encode_column(args.workload, args.scale)
-        cfg = {"workload": label}
+    w = args.workload
+    if w == "mixed":
+        return {"impl": "reference", "unavailable": "the mixed batch has no single reference CPU entry point; "
+                "the default run reports each codec's reference CPU rate"}
+    if w.endswith("_encode"):
+        codec, raw, kw, chunk, label = encode_column(w, args.scale)
         for _ in range(args.warmup):
             host_encode_rate(codec, raw, chunk, kw, 0.5)
+        vals = []
         for _ in range(args.steps):
             gbs, reps = host_encode_rate(codec, raw, chunk, kw, 4.0)
             vals.append(gbs)
-            sample = f"host encoder on the whole column, {reps} passes"
-        kind = "port"
-    else:
-        cols, cfg = make_workload(args.workload, args.scale)
+        v = statistics.median(vals)
+        return {"impl": "reference", "metric": f"encoded GB/s ({codec} device encoder, column bytes in)",
+                "value": round(v, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": None, "higher_is_better": True,
+                "config": {"workload": label, "l2": L2_NOTE, "parallelism": f"replicas x{world}",
+                           "ratio": None},
+                "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                                 "sample": f"host encoder on the whole column, {reps} passes"},
+                "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    head = HEADLINE if w == "all" else w
+    kern = []
+    with tempfile.TemporaryDirectory() as td:
+        tmp = Path(td)
+        t0 = time.perf_counter()
+        hc = cpu_cols_reference(head, args.scale, tmp, threads)
+        prep = time.perf_counter() - t0
         for _ in range(args.warmup):
-            _, _, _, prep = ref_decode_sample(cols, threads, budget_s=1.0, prepared=prep)
+            cpu_rates(hc, threads, 1.0)
+        vals, per_col = [], [[] for _ in hc]
         for _ in range(args.steps):
-            gbs, sample, kind, prep = ref_decode_sample(cols, threads, budget_s=4.0, prepared=prep)
+            rates = cpu_rates(hc, threads, 3.0)
+            gbs, sample, kind = combined_rate(hc, rates)
             vals.append(gbs)
+            for i, r in enumerate(rates):
+                per_col[i].append(r[0])
+        for c, rs, r in zip(hc, per_col, rates):
+            kern.append({"kernel": c.name, "workload": LABELS[head], "value": round(statistics.median(rs) / 1e9, 3),
+                         "unit": "GB/s", "kind": c.kind, "sample": r[1]})
+        for f in tmp.iterdir():
+            f.unlink()
+        if w == "all":
+            for ow in ("rlev1", "lzss", "deflate"):
+                oc = cpu_cols_reference(ow, args.scale, tmp, threads)
+                for c, (r, d, kind) in zip(oc, cpu_rates(oc, threads, 5.0)):
+                    kern.append({"kernel": c.name, "workload": LABELS[ow], "value": round(r / 1e9, 3), "unit": "GB/s",
+                                 "kind": kind, "sample": d})
+                del oc
+                for f in tmp.iterdir():
+                    f.unlink()
     v = statistics.median(vals)
-    metric = ("decompressed GB/s (byte-RLE + RLE v2 columns)" if args.workload == "brle_rlev2"
-              else f"encoded GB/s ({args.workload.split('_')[0]} device encoder, column bytes in)"
-              if args.workload.endswith("_encode") else f"decompressed GB/s ({args.workload})")
-    return {"impl": "reference", "metric": metric,
-            "value": round(v, 3), "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": None, "higher_is_better": True, "config": cfg,
+    return {"impl": "reference", "metric": HEADLINE_METRIC if w == "all" else f"decompressed GB/s ({w})",
+            "value": round(v, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "config": run_config(head, world),
             "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": kind,
                              "sample": sample},
-            "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "kernels": kern,
+            "inputs": "seeded generators (the oracle's copy), reference encoders (brle::encode, "
+                      "rlev2::block_encode, lzss::compress_func), Python zlib; RLE v1 by the oracle's input builder",
+            "prep_s": round(prep, 1), "native_libs": native_libs()}
+
+
+def native_libs():
+    """Shared objects of this repository mapped into this process."""
+    try:
+        with open("/proc/self/maps") as f:
+            return sorted({ln.split()[-1].replace(str(ROOT) + "/", "") for ln in f
+                           if ln.rstrip().endswith(".so") and str(ROOT) in ln})
+    except OSError:
+        return None
 
 
 def main():
@@ -906,12 +1152,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="brle_rlev2", choices=["brle_rlev2", "rlev1", "lzss", "deflate", "mixed",
-                                                                 "brle_encode", "lzss_encode", "rlev1_encode",
-                                                                 "rlev2_encode"])
+    ap.add_argument("--workload", default="all", choices=["all", "brle_rlev2", "rlev1", "lzss", "deflate", "mixed",
+                                                          "brle_encode", "lzss_encode", "rlev1_encode",
+                                                          "rlev2_encode"])
     ap.add_argument("--scale", type=float, default=1.0, help="workload size factor (1.0 = full size)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="default workload without config 5")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -921,7 +1168,7 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            print(json.dumps(run_reference(args)), flush=True)
+            print(json.dumps(run_reference(args, world)), flush=True)
         return 0
 
     if world > 1:
@@ -929,7 +1176,9 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    if args.workload == "mixed":
+    if args.workload == "all":
+        line = run_all(args, rank, world, local_rank)
+    elif args.workload == "mixed":
         line = run_mixed(args, rank, world, local_rank)
     elif args.workload.endswith("_encode"):
         line = run_encode(args, rank, world, local_rank)

@@ -78,13 +78,19 @@ def make_mixed_batch(seed: int, n_items: int, total_bytes: int, lo: int = 4096, 
     counts[-1] = n_items - counts[:-1].sum()
     codecs = np.concatenate([[order[i]] * counts[i] for i in range(5)])
     rng.shuffle(codecs)
-    items = []
-    for i, (codec, sz) in enumerate(zip(codecs, sizes)):
+    def one(i):
+        codec, sz = codecs[i], sizes[i]
         g = GRANULE[codec]
         n = max(g, int(sz) // g * g)
         raw = _gen(codec, seed * 100003 + i, n)
-        items.append(Item(codec, raw, encode_item(codec, raw, seed * 7 + i)))
-    return items
+        return Item(codec, raw, encode_item(codec, raw, seed * 7 + i))
+
+    # items are independent: built on all host threads (the C ABI calls
+    # release the interpreter lock); the result does not depend on the order
+    import concurrent.futures as cf
+    import os
+    with cf.ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        return list(ex.map(one, range(n_items)))
 
 
 @dataclass

@@ -72,7 +72,8 @@ __global__ void __launch_bounds__(NW * 32) inflate_kernel(Chunks ch, uint32_t n_
 template <class Chunks, uint32_t WIN, int NP, uint32_t RB = IRING, uint32_t DB = LBITS, uint32_t NL = NLIT,
           uint32_t NC = NCMD>
 __global__ void __launch_bounds__(NP * 64) inflate_pair_kernel(Chunks ch, uint32_t n_chunks, int zlib_hdr,
-                                                              const uint32_t* __restrict__ order) {
+                                                              const uint32_t* __restrict__ order,
+                                                              uint32_t spin_limit, uint32_t writer_stop) {
     using SmemT = WarpSmemT<WIN, 2, RB, DB, NL, NC>;
     extern __shared__ __align__(16) uint8_t smem_raw[];
     const uint32_t wid = threadIdx.x >> 5, pair = wid >> 1;
@@ -97,12 +98,13 @@ __global__ void __launch_bounds__(NP * 64) inflate_pair_kernel(Chunks ch, uint32
     // the pair's 64 threads, reached unconditionally by both warps
     asm volatile("bar.sync %0, 64;" ::"r"(1u + pair) : "memory");
     if (wid & 1u) {
-        const uint32_t werr = stream_pair_writer<WIN, RB, DB, NL, NC>(S, src, dst);
+        const uint32_t werr = stream_pair_writer<WIN, RB, DB, NL, NC>(S, src, dst, spin_limit, writer_stop);
         if (werr != ST_OK && lane_id() == 0) ch.put(chunk, werr, 0);
         return;
     }
     uint32_t fin = 0;
-    err = stream_warp_impl<WIN, 2, RB, DB, NL, NC>(src, (uint32_t)clen64, dst, (uint32_t)olen64, zlib_hdr, S, &fin);
+    err = stream_warp_impl<WIN, 2, RB, DB, NL, NC>(src, (uint32_t)clen64, dst, (uint32_t)olen64, zlib_hdr, S, &fin,
+                                                   spin_limit);
     if (err == ST_OK && Chunks::exact && fin != (uint32_t)olen64) err = ST_CORRUPT;
     if (lane_id() == 0) ch.put(chunk, err, err == ST_OK ? fin : 0);
 }
@@ -149,7 +151,10 @@ gd_status_t launch_pair(const Chunks& ch, uint32_t n, int zlib_hdr, const uint32
         attr_set = true;
     }
     const uint32_t grid = (n + NP - 1) / NP;
-    kern<<<grid, NP * 64, smem, s>>>(ch, n, zlib_hdr, order);
+    const int spin = gd_tune_get(GD_TUNE_INFLATE_PAIR_SPIN);
+    const int stop = gd_tune_get(GD_TUNE_INFLATE_WRITER_STOP);
+    kern<<<grid, NP * 64, smem, s>>>(ch, n, zlib_hdr, order, spin > 0 ? (uint32_t)spin : PAIR_SPIN_LIMIT,
+                                     stop > 0 ? (uint32_t)stop : 0u);
     return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
 }
 

@@ -312,17 +312,19 @@ static __device__ __forceinline__ void execute_batch(const BatchType& B, uint32_
 
 // Hand-off between the two warps of a pair: counters in shared memory.
 // produced = batches the decoder has filled, consumed = batches the writer
-// has executed.  Every wait is bounded (about a second): on expiry the waiter
-// reports GD_ERR_TIMEOUT and both warps still leave.
+// has executed.  Every wait is bounded (by default 2^25 polls, about a
+// second; GD_TUNE_INFLATE_PAIR_SPIN sets it): on expiry the waiter reports
+// GD_ERR_TIMEOUT and both warps still leave.
 constexpr uint32_t PAIR_SPIN_LIMIT = 1u << 25;
 
-// Wait (lane 0 spins, the warp follows) until *ctr >= target; false on expiry.
-__device__ __forceinline__ bool pair_wait(const uint32_t* ctr, uint32_t target) {
+// Wait (lane 0 spins, the warp follows) until *ctr >= target, polling at
+// most `limit` times; false on expiry.
+__device__ __forceinline__ bool pair_wait(const uint32_t* ctr, uint32_t target, uint32_t limit) {
     uint32_t ok = 1;
     if (lane_id() == 0) {
         uint32_t it = 0;
         while (*reinterpret_cast<const volatile uint32_t*>(ctr) < target) {
-            if (++it > PAIR_SPIN_LIMIT) {
+            if (++it > limit) {
                 ok = 0;
                 break;
             }
@@ -453,7 +455,8 @@ static __device__ bool build_huff(HuffT<BITS>* h, const uint8_t* lens, uint32_t 
 template <uint32_t WIN, int NB = 1, uint32_t RB = IRING, uint32_t DB = LBITS, uint32_t NL = NLIT, uint32_t NC = NCMD>
 static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __restrict__ src, uint32_t clen,
                                                             uint8_t* __restrict__ dst, uint32_t olen, int zlib_hdr,
-                                                            WarpSmemT<WIN, NB, RB, DB, NL, NC>& S, uint32_t* written) {
+                                                            WarpSmemT<WIN, NB, RB, DB, NL, NC>& S, uint32_t* written,
+                                                            uint32_t spin_limit = PAIR_SPIN_LIMIT) {
     static_assert(RB >= 1024 && (RB & (RB - 1)) == 0, "input ring: a power of two >= 1 KiB");
     // a window below the Deflate window's 32 KiB serves the nearer copies;
     // the executor reads farther ones from the output
@@ -625,7 +628,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
         auto& BT = S.bt[NB == 2 ? (kb & 1u) : 0u];
         // pairs: the buffer's previous batch (kb - 2) must have been executed
         if constexpr (NB == 2) {
-            if (kb >= 2 && !pair_wait(&S.consumed, kb - 1)) {
+            if (kb >= 2 && !pair_wait(&S.consumed, kb - 1, spin_limit)) {
                 err = ST_TIMEOUT;
                 break;
             }
@@ -984,7 +987,7 @@ static __device__ __forceinline__ uint32_t stream_warp_impl(const uint8_t* __res
         }
     }
     if constexpr (NB == 2) {  // the final (empty) hand-off
-        if (err != ST_TIMEOUT && kb >= 2 && !pair_wait(&S.consumed, kb - 1)) err = ST_TIMEOUT;
+        if (err != ST_TIMEOUT && kb >= 2 && !pair_wait(&S.consumed, kb - 1, spin_limit)) err = ST_TIMEOUT;
         auto& BT = S.bt[kb & 1u];
         if (lane == 0) {
             BT.n_cmd = 0;
@@ -1007,13 +1010,17 @@ static __device__ __noinline__ uint32_t stream_warp(const uint8_t* __restrict__ 
 // Writer warp of a pair: executes batch k while the decoder warp (running
 // stream_warp_impl<WIN, 2> on the same S) decodes batch k+1.  The decoder's
 // last hand-off is an empty batch marked last (also after an error).
-// Returns GD_ERR_TIMEOUT if a wait expired, else OK.
+// Returns GD_ERR_TIMEOUT if a wait expired, else OK.  stop_after > 0 (a test
+// setting) makes the writer leave after that many batches without posting
+// more, so that the decoder's bounded wait is exercised.
 template <uint32_t WIN, uint32_t RB = IRING, uint32_t DB = LBITS, uint32_t NL = NLIT, uint32_t NC = NCMD>
 static __device__ __forceinline__ uint32_t stream_pair_writer(WarpSmemT<WIN, 2, RB, DB, NL, NC>& S,
                                                               const uint8_t* __restrict__ src,
-                                                              uint8_t* __restrict__ dst) {
+                                                              uint8_t* __restrict__ dst, uint32_t spin_limit,
+                                                              uint32_t stop_after) {
     for (uint32_t kb = 0;; ++kb) {
-        if (!pair_wait(&S.produced, kb + 1)) return ST_TIMEOUT;
+        if (stop_after && kb >= stop_after) return ST_OK;  // the decoder's wait will run out
+        if (!pair_wait(&S.produced, kb + 1, spin_limit)) return ST_TIMEOUT;
         auto& BT = S.bt[kb & 1u];
         if (BT.last) return ST_OK;
         execute_batch<WIN>(BT, BT.pos0, S.win, src, dst);

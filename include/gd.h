@@ -288,7 +288,13 @@ typedef enum gd_tune_key {
                                           2 / 4 / 8: that many chunks (warps) per block, output
                                           written as decoded (also the path for chunks too large to
                                           stage, > 200 KiB) */
-    GD_TUNE_COUNT = 5
+    GD_TUNE_INFLATE_PAIR_SPIN = 5,     /* polls of a decoder/writer hand-off wait before the stream
+                                          gives up with GD_ERR_TIMEOUT (0: 2^25, about a second) */
+    GD_TUNE_INFLATE_WRITER_STOP = 6,   /* test knob for the bounded hand-off wait: k > 0 makes each
+                                          pair's writer warp leave after executing k batches, so the
+                                          decoder warp's wait runs out and the stream reports
+                                          GD_ERR_TIMEOUT (0: off) */
+    GD_TUNE_COUNT = 7
 } gd_tune_key_t;
 
 /* Set a knob; returns its previous value, or -1 for an unknown key or a

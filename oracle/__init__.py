@@ -44,6 +44,17 @@ def lib():
         L.gdo_export_lanes.argtypes = [vp, u64, vp, vp, u32, vp, vp]
         L.gdo_export_lanes.restype = i32
         L.gdo_version.restype = C.c_char_p
+        L.gdo_rlev1_encode.argtypes = [vp, u64, u64, u32, u32, vp, vp, vp]
+        L.gdo_rlev1_encode.restype = u64
+        L.gdo_rlev1_max_encoded_bytes.argtypes = [u64, u64]
+        L.gdo_rlev1_max_encoded_bytes.restype = u64
+        for f in ("gd_gen_rlev1_ints", "gd_gen_brle_bytes", "gd_gen_rlev2_ints"):
+            getattr(L, f).argtypes = [u64, u64, vp]
+            getattr(L, f).restype = None
+        L.gd_gen_markov_copy.argtypes = [u64, u64, u32, vp]
+        L.gd_gen_markov_copy.restype = None
+        L.gd_gen_loguniform_sizes.argtypes = [u64, u32, u64, u64, u64, u64, vp]
+        L.gd_gen_loguniform_sizes.restype = i32
         _L = L
     return _L
 
@@ -112,3 +123,71 @@ def export_lanes(enc) -> tuple[np.ndarray, np.ndarray]:
     if rc:
         raise RuntimeError(f"export_lanes: status {rc}")
     return out[: int(off[-1])], off
+
+
+# --------------------------------------------------------------------------
+# input builders for the CPU baselines (the reference arm of bench.py builds
+# its inputs without the product library)
+# --------------------------------------------------------------------------
+
+class Container:
+    """A compressed column in the shape decode() reads: codec, payload, meta
+    arrays, parameters (the fields of compression_b200.codecs.Encoded)."""
+
+    def __init__(self, codec, data, n_out, n_chunks, chunk_size=0, meta=None, params=None):
+        self.codec, self.data, self.n_out, self.n_chunks = codec, data, int(n_out), int(n_chunks)
+        self.chunk_size, self.meta, self.params = int(chunk_size), meta or {}, params or {}
+
+    @property
+    def comp_bytes(self) -> int:
+        return int(self.data.nbytes)
+
+    @property
+    def meta_bytes(self) -> int:
+        return int(sum(v.nbytes for v in self.meta.values()))
+
+
+def gen_rlev1_ints(seed: int, n: int) -> np.ndarray:
+    a = np.empty(n, dtype=np.int32)
+    lib().gd_gen_rlev1_ints(seed, n, _p(a))
+    return a
+
+
+def gen_brle_bytes(seed: int, n: int) -> np.ndarray:
+    a = np.empty(n, dtype=np.uint8)
+    lib().gd_gen_brle_bytes(seed, n, _p(a))
+    return a
+
+
+def gen_rlev2_ints(seed: int, n: int) -> np.ndarray:
+    a = np.empty(n, dtype=np.int64)
+    lib().gd_gen_rlev2_ints(seed, n, _p(a))
+    return a
+
+
+def gen_markov_copy(seed: int, n: int, max_dist: int) -> np.ndarray:
+    a = np.empty(n, dtype=np.uint8)
+    lib().gd_gen_markov_copy(seed, n, max_dist, _p(a))
+    return a
+
+
+def loguniform_sizes(seed: int, n: int, lo: int, hi: int, total: int, granule: int = 1) -> np.ndarray:
+    a = np.empty(n, dtype=np.uint64)
+    if lib().gd_gen_loguniform_sizes(seed, n, lo, hi, total, granule, _p(a)) != 0:
+        raise ValueError("loguniform_sizes")
+    return a
+
+
+def rlev1_encode(raw, chunk_size: int = 128 * 1024, comp_col_len: int = 128, elem_bytes: int = 4) -> Container:
+    """The RLE v1 container of `raw` (gd_inputs.cpp)."""
+    b = np.ascontiguousarray(raw).view(np.uint8).reshape(-1)
+    L = lib()
+    nc = (b.size + chunk_size - 1) // chunk_size
+    data = np.empty(L.gdo_rlev1_max_encoded_bytes(b.size, chunk_size), dtype=np.uint8)
+    blk = np.empty(nc + 1, dtype=np.uint64)
+    col = np.empty(32 * nc, dtype=np.uint64)
+    n = L.gdo_rlev1_encode(_p(b), b.size, chunk_size, comp_col_len, elem_bytes, _p(data), _p(blk), _p(col))
+    if n == 0:
+        raise ValueError("rlev1 encode failed")
+    return Container("rlev1", data[:n].copy(), b.size, nc, chunk_size, {"blk_off": blk, "col_len": col},
+                     {"comp_col_len": comp_col_len, "elem_bytes": elem_bytes})

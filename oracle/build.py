@@ -17,13 +17,28 @@ HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 
 
+# liboracle.so: the C restatement of the decoders (gd_oracle.c), the input
+# builders of the CPU baselines (gd_inputs.cpp, with the lane encoder header
+# it includes) and the seeded column generators, compiled from the product's
+# generator source so that a seed gives the same column in both libraries.
+GEN = HERE.parent / "compression_b200" / "csrc" / "host" / "gd_gen.cpp"
+DEPS = [HERE / "gd_oracle.c", HERE / "gd_inputs.cpp", GEN, HERE.parent / "compression_b200" / "csrc" / "lane_enc.h"]
+
+
 def build_oracle() -> Path:
-    src = HERE / "gd_oracle.c"
-    if LIB.exists() and LIB.stat().st_mtime >= src.stat().st_mtime:
+    if LIB.exists() and all(LIB.stat().st_mtime >= d.stat().st_mtime for d in DEPS):
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    subprocess.run(["gcc", "-O2", "-fPIC", "-shared", "-std=c11", "-Wall", str(src), "-lz", "-o", str(tmp)],
-                   check=True)
+    obj = HERE / "_ref" / "obj"
+    obj.mkdir(parents=True, exist_ok=True)
+    inc = str(HERE.parent / "include")
+    subprocess.run(["gcc", "-O2", "-fPIC", "-std=c11", "-Wall", "-c", str(HERE / "gd_oracle.c"), "-o",
+                    str(obj / "gd_oracle.o")], check=True)
+    for src in (HERE / "gd_inputs.cpp", GEN):
+        subprocess.run(["g++", "-O2", "-fPIC", "-std=c++17", "-Wall", "-I", inc, "-I", "/usr/local/cuda/include",
+                        "-c", str(src), "-o", str(obj / (src.stem + ".o"))], check=True)
+    subprocess.run(["g++", "-shared", "-o", str(tmp), str(obj / "gd_oracle.o"), str(obj / "gd_inputs.o"),
+                    str(obj / "gd_gen.o"), "-lz", "-pthread"], check=True)
     tmp.replace(LIB)
     return LIB
 

@@ -773,8 +773,9 @@ int gdo_brle_trans4_decode(const uint8_t* data, uint64_t data_len, const uint64_
  * Deflate container is produced with: zlib.compress in
  * orig_compressor.py:87, consumed by deflate::decompress_gpu,
  * include/zlib/zlib.h:966-1082, which skips the 2-byte zlib header,
- * zlib.h:580).  zlib_header != 0: each stream is a zlib stream (RFC 1950);
- * 0: raw deflate (RFC 1951).  Chunk i: compressed bytes
+ * zlib.h:580).  zlib_header 1: each stream is a zlib stream (RFC 1950);
+ * 2: a gzip member (RFC 1952; the header cudf::io::gpuinflate parses with
+ * parse_hdr, cudf_deflate.cuh:1180-1216); 0: raw deflate (RFC 1951).  Chunk i: compressed bytes
  * data[comp_off[i] .. comp_off[i]+comp_len[i]), output
  * out[out_off[i] .. out_off[i+1]).
  */
@@ -783,7 +784,9 @@ int gdo_inflate(const uint8_t* data, const uint64_t* comp_off, const uint64_t* c
     for (uint32_t c = 0; c < n_chunks; ++c) {
         z_stream zs;
         memset(&zs, 0, sizeof(zs));
-        if (inflateInit2(&zs, zlib_header ? 15 : -15) != Z_OK) return GDO_INVALID;
+        /* 0 raw deflate, 1 zlib (RFC 1950), 2 gzip member (RFC 1952) */
+        const int wbits = zlib_header == 2 ? 15 + 16 : (zlib_header ? 15 : -15);
+        if (inflateInit2(&zs, wbits) != Z_OK) return GDO_INVALID;
         zs.next_in = (Bytef*)(data + comp_off[c]);
         zs.avail_in = (uInt)comp_len[c];
         uint64_t want = out_off[c + 1] - out_off[c];

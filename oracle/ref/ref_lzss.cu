@@ -4,6 +4,9 @@
 // (lzss_gpu2.h:330-707), so one column = one call here.  Oracle tooling only.
 //   ref_lzss encode <raw> <stream>           lzss::compress_func, one chunk
 //   ref_lzss decode <stream> <n_out> <raw>    lzss::decompress_func
+//   ref_lzss encode_lanes <raw> <bytes per stream> <threads> <streams>
+//       lzss::compress_func of every consecutive <bytes per stream> bytes on
+//       <threads> host threads, written in the bench format below
 //   ref_lzss bench <streams> <threads> <seconds>   lzss::decompress_func on every
 //       stream of a [u64 n][u64 bytes per stream][u64 offsets[n+1]][bytes] file
 //       on <threads> host threads, repeated for about <seconds>; prints
@@ -15,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <thread>
 #include <vector>
 
@@ -67,6 +71,37 @@ int main(int argc, char** argv) {
     if (argc < 4) return 1;
     std::vector<uint8_t> in = slurp(argv[2]);
     if (!strcmp(argv[1], "bench")) return bench(in, atoi(argv[3]), argc > 4 ? atof(argv[4]) : 5.0);
+    if (!strcmp(argv[1], "encode_lanes")) {
+        if (argc < 6) return 1;
+        const uint64_t nb = strtoull(argv[3], nullptr, 10);
+        const int threads = atoi(argv[4]);
+        if (nb == 0 || in.size() % nb) return 4;
+        const uint64_t n = in.size() / nb;
+        const uint64_t oc = nb + OVERHEAD_PER_CHUNK_((uint32_t)nb) + 16;
+        std::vector<std::vector<uint8_t>> enc(n);
+        std::atomic<uint64_t> next{0};
+        std::vector<std::thread> th;
+        for (int t = 0; t < threads; ++t)
+            th.emplace_back([&]() {
+                std::vector<uint8_t> buf(oc);
+                for (uint64_t i; (i = next.fetch_add(1)) < n;) {
+                    uint64_t len = 0;
+                    std::fill(buf.begin(), buf.end(), 0);  // the trailing reserved flag byte stays 0
+                    lzss::compress_func(in.data() + i * nb, buf.data(), nb, oc, nb, oc, 1, &len, 0);
+                    enc[i].assign(buf.begin(), buf.begin() + len);
+                }
+            });
+        for (auto& x : th) x.join();
+        std::vector<uint64_t> head(2 + n + 1);
+        head[0] = n;
+        head[1] = nb;
+        for (uint64_t i = 0; i < n; ++i) head[3 + i] = head[2 + i] + enc[i].size();
+        std::vector<uint8_t> out(8 * head.size() + head[2 + n] + 64, 0);
+        memcpy(out.data(), head.data(), 8 * head.size());
+        for (uint64_t i = 0; i < n; ++i) memcpy(out.data() + 8 * head.size() + head[2 + i], enc[i].data(), enc[i].size());
+        spit(argv[5], out.data(), out.size());
+        return 0;
+    }
     if (!strcmp(argv[1], "encode")) {
         const uint64_t n = in.size();
         const uint64_t oc = n + OVERHEAD_PER_CHUNK_((uint32_t)n) + 16;

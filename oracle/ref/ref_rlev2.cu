@@ -6,6 +6,9 @@
 // values (encoder_trans.h:9-289).  Oracle tooling only.
 //   ref_rlev2 encode <int64 raw> <stream>           block_encode, one chunk (<= 4096 values)
 //   ref_rlev2 decode <stream> <n_values> <int64 raw> block_decode
+//   ref_rlev2 encode_lanes <int64 raw> <values per stream> <threads> <streams>
+//       block_encode of every consecutive group of <values per stream> values
+//       on <threads> host threads, written in the bench format below
 //   ref_rlev2 bench <streams> <threads> <seconds>   block_decode of every stream
 //       of a [u64 n][u64 values per stream][u64 offsets[n+1]][bytes] file on
 //       <threads> host threads, repeated for about <seconds>; prints
@@ -19,6 +22,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <thread>
 #include <vector>
 
@@ -69,6 +73,36 @@ int main(int argc, char** argv) {
     if (argc < 4) return 1;
     std::vector<uint8_t> in = slurp(argv[2]);
     if (!strcmp(argv[1], "bench")) return bench(in, atoi(argv[3]), argc > 4 ? atof(argv[4]) : 5.0);
+    if (!strcmp(argv[1], "encode_lanes")) {
+        if (argc < 6) return 1;
+        const uint64_t nv = strtoull(argv[3], nullptr, 10);
+        const int threads = atoi(argv[4]);
+        if (nv == 0 || nv * 8 > CHUNK_SIZE || in.size() % (nv * 8)) return 4;
+        const uint64_t n = in.size() / (nv * 8);
+        std::vector<std::vector<uint8_t>> enc(n);
+        std::atomic<uint64_t> next{0};
+        std::vector<std::thread> th;
+        for (int t = 0; t < threads; ++t)
+            th.emplace_back([&]() {
+                std::vector<uint8_t> buf(OUTPUT_CHUNK_SIZE * 2);
+                for (uint64_t i; (i = next.fetch_add(1)) < n;) {
+                    uint64_t len = 0;
+                    std::fill(buf.begin(), buf.end(), 0);
+                    rlev2::block_encode(0, reinterpret_cast<int64_t*>(in.data() + i * nv * 8), nv * 8, buf.data(), &len);
+                    enc[i].assign(buf.begin(), buf.begin() + len);
+                }
+            });
+        for (auto& x : th) x.join();
+        std::vector<uint64_t> head(2 + n + 1);
+        head[0] = n;
+        head[1] = nv;
+        for (uint64_t i = 0; i < n; ++i) head[3 + i] = head[2 + i] + enc[i].size();
+        std::vector<uint8_t> out(8 * head.size() + head[2 + n] + 64, 0);
+        memcpy(out.data(), head.data(), 8 * head.size());
+        for (uint64_t i = 0; i < n; ++i) memcpy(out.data() + 8 * head.size() + head[2 + i], enc[i].data(), enc[i].size());
+        spit(argv[5], out.data(), out.size());
+        return 0;
+    }
     if (!strcmp(argv[1], "encode")) {
         if (in.size() > CHUNK_SIZE) return 4;
         std::vector<uint8_t> out(OUTPUT_CHUNK_SIZE * 2, 0);
