@@ -104,13 +104,14 @@ int main(int argc, char**) {
 
 def test_tuning_knobs_set_and_get():
     L = _lib.lib()
-    for key in range(5):
+    n_keys = 7  # GD_TUNE_COUNT
+    for key in range(n_keys):
         old = L.gd_tune_get(key)
         assert old >= 0
         assert L.gd_tune_set(key, 4) == old
         assert L.gd_tune_get(key) == 4
         assert L.gd_tune_set(key, old) == 4
-    assert L.gd_tune_get(5) == -1 and L.gd_tune_set(5, 1) == -1 and L.gd_tune_set(0, -1) == -1
+    assert L.gd_tune_get(n_keys) == -1 and L.gd_tune_set(n_keys, 1) == -1 and L.gd_tune_set(0, -1) == -1
 
 
 def test_host_compress_argument_errors():
