@@ -1,6 +1,6 @@
 """Regenerate the golden fixtures from the reference's own codecs.
 
-    python oracle/build.py --ref          # builds oracle/_ref/ref_{brle,lzss,rlev2}
+    python oracle/build.py --ref          # builds oracle/_ref/ref_* from the reference sources
     python tests/golden/make_golden.py    # writes tests/golden/*.npz
 
 Inputs come from the seeded generators (compression_b200.codecs) and a few
@@ -9,7 +9,10 @@ the reference's own decoder output are stored, so the tests can check (a) the
 library's encoders reproduce the reference bytes exactly and (b) the oracle
 and the GPU decoders recover the input from the reference's streams.
 Deflate fixtures come from Python's zlib, the producer the reference's
-container is written with (orig_compressor.py:87).
+container is written with (orig_compressor.py:87).  The RLE v1 and byte-RLE
+flag containers have GPU-only codecs in the reference: their writers and
+readers run on host threads (oracle/ref/host_cuda.h), compiled from the
+reference's own kernels.
 """
 from __future__ import annotations
 
@@ -46,6 +49,71 @@ def negative_constant_run(tmp: Path):
     lane.tofile(tmp / "v")
     run(REF / "ref_rlev2", "encode", tmp / "v", tmp / "vs")
     np.savez_compressed(OUT / "rlev2_negconst.npz", raw=lane, enc=np.fromfile(tmp / "vs", np.uint8))
+
+
+def _interleaved(prefix: Path, with_map: bool):
+    out = {"data": np.fromfile(f"{prefix}.data", np.uint8), "col_len": np.fromfile(f"{prefix}.col_len", np.uint64),
+           "blk_off": np.fromfile(f"{prefix}.blk_off", np.uint64)}
+    if with_map:
+        out["col_map"] = np.fromfile(f"{prefix}.col_map", np.uint8)
+    return out
+
+
+def gpu_only_codecs(tmp: Path, rng):
+    """RLE v1 (rle_v1::compress_gpu / decompress_gpu: setup_deflate,
+    reduction_scan, deflate; inflate) and the byte-RLE flag containers
+    (brle_trans::compress_gpu / decompress_gpu, brle_gpu_4B.h's
+    compress_gpu / decompress_gpu): the reference writer's container and the
+    reference reader's output for each input."""
+    # ---- RLE v1: (values, element bytes, chunk size, COMP_COL_LEN) ----
+    lit_edges = np.concatenate([np.arange(127, dtype=np.int64) * 1000, np.full(5, 7), np.arange(128) * 999,
+                                np.arange(130) * 2 + 5, np.arange(131) * 3, [0xFFFFFFFF, 0, 0xFFFFFFFF]])
+    cases = [
+        (cc.gen_rlev1_ints(0xA0, 4 * 32768), 4, 128 * 1024, 128),                       # config 1's data
+        (cc.gen_rlev1_ints(0xA1, 7 * 2048 + 100), 4, 8192, 8),                          # partial last chunk
+        (cc.gen_rlev2_ints(0xA2, 5 * 2048 + 3), 8, 16384, 64),                          # 8-byte values
+        (np.resize(lit_edges, 4 * 8192).astype(np.uint32), 4, 32768, 256),            # group / run limits
+        (np.resize(np.repeat(rng.integers(0, 1 << 20, 600), rng.integers(1, 140, 600)),
+                   2 * 8192).astype(np.uint32), 4, 8192, 16),                            # constant runs
+        ((np.arange(4096, dtype=np.int64) * -5 + 1000).astype(np.uint32), 4, 16384, 32),  # negative deltas
+    ]
+    rz = {}
+    for i, (vals, eb, chunk, ccl) in enumerate(cases):
+        raw = np.ascontiguousarray(vals).view(np.uint8)
+        raw.tofile(tmp / "r1")
+        run(REF / "ref_rlev1_host", "encode", tmp / "r1", eb, chunk, ccl, tmp / "r1o")
+        run(REF / "ref_rlev1_host", "decode", tmp / "r1o", eb, chunk, ccl, raw.size, tmp / "r1d")
+        rz[f"raw{i}"] = raw
+        for k, v in _interleaved(tmp / "r1o", False).items():
+            rz[f"{k}{i}"] = v
+        rz[f"dec{i}"] = np.fromfile(tmp / "r1d", np.uint8)
+        rz[f"params{i}"] = np.array([eb, chunk, ccl], np.uint64)
+    np.savez_compressed(OUT / "rlev1_golden.npz", **rz)
+
+    # ---- byte-RLE flag containers: 1-byte symbols (4 KiB chunks, an even
+    # count: the reference reader decodes chunks in pairs) and 4-byte symbols
+    # (8 KiB chunks) ----
+    for name, exe, chunk, cases in [
+        ("brle_trans", "ref_brle_trans_host", 4096, [
+            cc.gen_brle_bytes(7, 4096 * 40), np.zeros(4096 * 2, np.uint8), rng.integers(0, 256, 4096 * 4).astype(np.uint8),
+            np.repeat(rng.integers(0, 4, 3000), rng.integers(1, 12, 3000)).astype(np.uint8)[:4096 * 6],
+            np.resize(np.array([1, 2, 3, 4, 5, 6, 7] + [9] * 121, np.uint8).repeat(1), 4096 * 2)]),
+        ("brle_trans4", "ref_brle_trans4_host", 8192, [
+            np.resize(np.repeat(rng.integers(0, 6, 20000), rng.integers(1, 20, 20000)).astype(np.uint32),
+                      8192 * 10 // 4).view(np.uint8).copy(),
+            np.zeros(8192 * 2, np.uint8), rng.integers(0, 256, 8192 * 3).astype(np.uint8),
+            cc.gen_rlev1_ints(3, 8192 * 4 // 4).view(np.uint8).copy()])]:
+        bz = {}
+        for i, raw in enumerate(cases):
+            raw = np.ascontiguousarray(raw[:raw.size // chunk * chunk])
+            raw.tofile(tmp / "b")
+            run(REF / exe, "encode", tmp / "b", tmp / "bo")
+            run(REF / exe, "decode", tmp / "bo", raw.size, tmp / "bd")
+            bz[f"raw{i}"] = raw
+            for k, v in _interleaved(tmp / "bo", True).items():
+                bz[f"{k}{i}"] = v
+            bz[f"dec{i}"] = np.fromfile(tmp / "bd", np.uint8)
+        np.savez_compressed(OUT / f"{name}_golden.npz", **bz)
 
 
 def main():
@@ -114,6 +182,8 @@ def main():
                         dec=np.fromfile(tmp / "vd", np.int64))
 
     negative_constant_run(tmp)
+
+    gpu_only_codecs(tmp, rng)
 
     # ---- Deflate chunks (Python zlib, level 6 / 9 as orig_compressor.py) ----
     dz = {}

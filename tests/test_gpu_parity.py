@@ -200,6 +200,26 @@ def test_reference_streams_on_gpu(cuda):
     assert (st == 0).all() and np.array_equal(out, vals.view(np.uint8))
 
 
+def test_reference_writer_containers_on_gpu(cuda):
+    """Containers written by the reference's own GPU-only writers (RLE v1,
+    byte-RLE flag with 1- and 4-byte symbols; tests/golden, produced by the
+    reference kernels run on host threads) decode bit-exact on the device and
+    agree with the reference's own reader."""
+    from test_golden import _interleaved_cases
+    for c in _interleaved_cases("rlev1"):
+        eb, chunk, ccl = (int(x) for x in c["params"])
+        e = cc.Encoded("rlev1", c["data"], c["raw"].size, c["blk_off"].size - 1, chunk,
+                       {"blk_off": c["blk_off"], "col_len": c["col_len"]}, {"comp_col_len": ccl, "elem_bytes": eb})
+        st, out = _gpu(e, cuda)
+        assert (st == 0).all() and np.array_equal(out, c["raw"]) and np.array_equal(out, c["dec"])
+    for name, chunk in (("brle_trans", 4096), ("brle_trans4", 8192)):
+        for c in _interleaved_cases(name):
+            e = cc.Encoded(name, c["data"], c["raw"].size, c["blk_off"].size - 1, chunk,
+                           {"blk_off": c["blk_off"], "col_len": c["col_len"], "col_map": c["col_map"]})
+            st, out = _gpu(e, cuda)
+            assert (st == 0).all() and np.array_equal(out, c["raw"]) and np.array_equal(out, c["dec"]), name
+
+
 # ---------------------------------------------------------------------------
 # LZSS contiguous container and byte-RLE flag-byte container
 # ---------------------------------------------------------------------------
