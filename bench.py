@@ -724,10 +724,13 @@ def mixed_run(args, rank, world, local_rank, clk_samples):
     corr = float(np.corrcoef(pred, y_eval)[0, 1])
     graph = CM.GraphSchedule(plan, model, X)
     out_b, in_b = task_bytes(plan)
-    orders = {"size_lpt_out": CM.lpt_order(out_b), "size_lpt_in": CM.lpt_order(in_b)}
+    # the learned order itself, computed once, so that the schedule's quality
+    # is timed apart from the cost of inference and sorting
+    orders = {"size_lpt_out": CM.lpt_order(out_b), "size_lpt_in": CM.lpt_order(in_b),
+              "learned_order_only": CM.lpt_order(pred)}
 
     flush = torch.empty(256 * MiB, dtype=torch.uint8, device=dev)
-    kinds = ("learned_lpt", "static", "queue_fifo", "size_lpt_out", "size_lpt_in")
+    kinds = ("learned_lpt", "static", "queue_fifo", "size_lpt_out", "size_lpt_in", "learned_order_only")
 
     def run(kind):
         if kind == "static":
@@ -834,6 +837,12 @@ def mixed_run(args, rank, world, local_rank, clk_samples):
         "learned_gain_vs_static": round(1.0 - ms / med["static"], 4),
         "learned_gain_vs_size_lpt_out": round(1.0 - ms / med["size_lpt_out"], 4),
         "learned_gain_vs_size_lpt_in": round(1.0 - ms / med["size_lpt_in"], 4),
+        "learned_order_gain_vs_size_lpt_out": round(1.0 - med["learned_order_only"] / med["size_lpt_out"], 4),
+        "schedules": {"static": "task i on warp i mod W", "queue_fifo": "work queue, task order",
+                      "size_lpt_out": "work queue, longest first by decompressed bytes per task",
+                      "size_lpt_in": "work queue, longest first by compressed bytes per task",
+                      "learned_lpt": "CUDA graph: MLP inference + argsort + work queue (all timed)",
+                      "learned_order_only": "work queue in the learned order computed beforehand"},
         "cost_model": {"train_batch": "separate quarter-size batch of the same mix (other seeds)",
                        "samples": int(sum(y.size for y in ys)), "epochs": 8, "final_loss": round(float(losses[-1]), 4),
                        "corr_pred_measured_eval_batch": round(corr, 4), "train_s": round(t_train, 1)},

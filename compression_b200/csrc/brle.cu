@@ -6,15 +6,15 @@
 // data[ptr[c] .. ptr[c+1]) and expand to out[c*chunk_size ..].
 //
 // The reference decodes one chunk per thread (1024 threads on the whole GPU
-// for a 256 MiB column).  Here one 256-thread block decodes a chunk, 8 KiB of
+// for a 256 MiB column).  Here one 256-thread block decodes a chunk, 9 KiB of
 // compressed bytes (a tile) at a time:
 //   1. The tile (+ a 160-byte halo for tokens that run past it) is staged in
 //      shared memory with 16-byte loads.
 //   2. Token starts form a chain (each token is 2..129 bytes).  Thread t owns
-//      a 32-byte segment and computes, by one backward pass over its bytes,
+//      a 36-byte segment and computes, by one backward pass over its bytes,
 //      where the chain leaves the segment for every entry offset (an exit
 //      table).
-//   3. Warp w owns a 1 KiB region (32 segments).  Lane l follows the chain
+//   3. Warp w owns a region of 32 segments.  Lane l follows the chain
 //      through the region from entry offset l of its first segment, one table
 //      lookup per segment, recording the entry of every segment.  All 32
 //      possible region entries are thus resolved in parallel.
@@ -42,7 +42,10 @@ namespace brle {
 
 constexpr int NT = 256;
 constexpr int NWARP = NT / 32;
-constexpr int SEG = 32;          // compressed bytes per thread segment
+// compressed bytes per thread segment: 36, not 32, so that the 32 lanes of a
+// warp, each in its own segment at the same offset, address 32 different
+// shared-memory banks (a 32-byte stride puts 8 lanes on every bank)
+constexpr int SEG = 36;
 constexpr int REG = 32 * SEG;    // bytes per warp region
 constexpr int TILE = NT * SEG;   // compressed bytes per tile
 constexpr int HALO = 160;        // a token starting in the tile reads <= 128 more bytes
@@ -126,7 +129,7 @@ __global__ void __launch_bounds__(NT, 4) decode_kernel(const uint8_t* __restrict
 
             // ---- 2. exit table of this thread's segment ----
             // s_tbl[p] = (chain exit - S) when the chain passes p in [S, lim);
-            // an exit is the first chain position >= lim (<= 31 + 129).
+            // an exit is the first chain position >= lim (<= SEG - 1 + 129).
             const uint32_t S = SEG * tid;
             const uint32_t lim = min(S + SEG, cl);
             if (S < cl) {

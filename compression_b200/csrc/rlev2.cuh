@@ -457,7 +457,62 @@ static __device__ __forceinline__ uint32_t decode_stream(const uint8_t* __restri
         uint64_t cr_acc = 0;
         // slice (rb / ru) and offset (rb % ru) of the round, kept incrementally
         uint32_t sl_k = (vbeg & ~31u) / ru, sl_j = (vbeg & ~31u) % ru;
-        for (uint32_t rb = vbeg & ~31u; rb < vend; rb += 32) {
+        for (uint32_t rb = vbeg & ~31u; rb < vend;) {
+            // ---- fast path: rounds inside one run (warp-uniform) ----
+            // The run holding value rb is rcur, or rcur + 1 when a run starts
+            // exactly at rb.  While whole rounds lie inside it, every lane
+            // decodes the same run with its fields held in registers: no run
+            // search, one kind, no divergence.
+            {
+                const int nx = rcur + 1;
+                const int r0 = (nx < (int)nr && R.vs[nx] == rb) ? nx : rcur;
+                const uint32_t rend = r0 >= 0 ? min(R.vs[r0 + 1], vend) : 0u;
+                if (r0 >= 0 && rb >= vbeg && rb + 32u <= rend) {
+                    const uint32_t meta = R.meta[r0];
+                    const uint32_t kind = meta & 3u, fbw = (meta >> 2) & 127u;
+                    const uint32_t v0 = R.vs[r0];
+                    const uint64_t base = R.base[r0], aux = R.aux[r0];
+                    const uint32_t vbit = R.vbit[r0];
+                    const bool fixed = ((meta >> 9) & 1u) != 0, sub = ((meta >> 10) & 1u) != 0;
+                    if (kind == 3u && !fixed && r0 != cr_run) cr_acc = 0;
+                    do {
+                        const uint32_t i = rb + lane - v0;  // index of this lane's value in the run
+                        uint64_t v = base;
+                        if (kind == 1u || kind == 2u) {
+                            const uint64_t x = extract_msb(sbuf, vbit + i * fbw, fbw);
+                            v = kind == 1u ? x : base + x;
+                        } else if (kind == 3u) {
+                            if (fixed) {
+                                v = base + (uint64_t)i * aux;
+                            } else {
+                                // v_0 = base, v_1 = base + delta, v_i = v_{i-1} +- d_{i-2}
+                                uint64_t sc = i >= 2 ? extract_msb(sbuf, vbit + (i - 2) * fbw, fbw) : 0ull;
+#pragma unroll
+                                for (uint32_t o = 1; o < 32; o <<= 1) {
+                                    const uint64_t n = shfl_up64(sc, o);
+                                    if (lane >= o) sc += n;
+                                }
+                                sc += cr_acc;
+                                const uint64_t b1v = base + aux;
+                                v = (i == 0) ? base : (sub ? b1v - sc : b1v + sc);
+                                cr_acc = shfl64(sc, 31);
+                            }
+                        }
+                        const uint64_t oe = ru32 ? (uint64_t)t * ru + (uint64_t)sl_k * 32u * ru + sl_j + lane
+                                                 : out_index(rb + lane);
+                        if (oe < want_vals) outv[oe] = v;
+                        sl_j += 32;
+                        if (sl_j >= ru) {
+                            sl_j -= ru;
+                            ++sl_k;
+                        }
+                        rb += 32;
+                    } while (rb + 32u <= rend);
+                    rcur = r0;
+                    cr_run = r0;
+                    continue;
+                }
+            }
             const uint32_t vi = rb + lane;
             const bool act = vi >= vbeg && vi < vend;
             // runs rcur+1 .. rcur+32 cover every run start inside this round
@@ -506,6 +561,7 @@ static __device__ __forceinline__ uint32_t decode_stream(const uint8_t* __restri
                 sl_j -= ru;
                 ++sl_k;
             }
+            rb += 32;
         }
         __syncwarp();
 
