@@ -326,6 +326,68 @@ def cpu_cols_reference(workload: str, scale: float, tmp: Path, threads: int):
     return res
 
 
+def cudf_comparator(cont, steps: int, warmup: int):
+    """The reference's vendored cuDF inflate (cudf::io::gpuinflate,
+    include/cudf_deflate.cuh:1399-1407, compiled for sm_100a into
+    oracle/_ref/libref_cudf.so) on config 4's zlib streams, passed as the
+    reference's driver passes them (base_deflate.h:66-72: past the 2-byte
+    header), in stream order; CUDA events, L2 flushed between launches.
+    Returns a dict, or None without a GPU or the library."""
+    import ctypes as C
+    lib_path = REF_BIN / "libref_cudf.so"
+    try:
+        import torch
+        if not torch.cuda.is_available() or not lib_path.exists():
+            return None
+    except ImportError:
+        return None
+    import oracle
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_in = torch.from_numpy(np.concatenate([cont.data, np.zeros(64, np.uint8)])).to(dev)
+    d_out = torch.zeros(cont.n_out + 64, dtype=torch.uint8, device=dev)
+    co, cl, oo = cont.meta["comp_off"], cont.meta["comp_len"], cont.meta["out_off"]
+    n = cont.n_chunks
+    desc = np.zeros((n, 4), np.uint64)
+    desc[:, 0] = d_in.data_ptr() + co[:-1] + 2
+    desc[:, 1] = cl - 2
+    desc[:, 2] = d_out.data_ptr() + oo[:-1]
+    desc[:, 3] = np.diff(oo)
+    d_desc = torch.from_numpy(desc.view(np.int64).reshape(-1)).to(dev)
+    d_stat = torch.zeros(2 * n, dtype=torch.int64, device=dev)
+    L = C.CDLL(str(lib_path))
+    s = torch.cuda.current_stream(dev)
+
+    def launch():
+        if L.ref_cudf_gpuinflate(C.c_void_p(d_desc.data_ptr()), C.c_void_p(d_stat.data_ptr()), n, 0,
+                                 C.c_void_p(s.cuda_stream)) != 0:
+            raise RuntimeError("cuDF gpuinflate launch failed")
+
+    launch()
+    torch.cuda.synchronize()
+    st = d_stat.cpu().numpy().reshape(-1, 2)
+    rc, ref = oracle.decode(cont)
+    exact = bool(rc == 0 and (st[:, 1] & 0xffffffff == 0).all() and (st[:, 0] == np.diff(oo)).all()
+                 and np.array_equal(d_out[:cont.n_out].cpu().numpy(), ref))
+    flush = torch.empty(256 * MiB, dtype=torch.uint8, device=dev)
+    ts = []
+    for k in range(warmup + steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        launch()
+        b.record(s)
+        torch.cuda.synchronize()
+        if k >= warmup:
+            ts.append(a.elapsed_time(b))
+    ms = statistics.median(ts)
+    alg = int(cont.data.nbytes + cont.n_out + 16 * n)
+    del d_in, d_out, d_desc, d_stat, flush
+    torch.cuda.empty_cache()
+    return {"name": "cuDF gpuinflate (the reference's vendored cudf_deflate.cuh, sm_100a)", "ms": round(ms, 4),
+            "decomp_gbs": round(cont.n_out / (ms / 1e3) / 1e9, 2), "alg_gbs": round(alg / (ms / 1e3) / 1e9, 2),
+            "exact": exact, "order": "stream order, one 128-thread block per stream, as gpuinflate launches"}
+
+
 def _sub(cont, a, b):
     """Chunks [a, b) of an oracle container as a container of their own."""
     import oracle
@@ -715,7 +777,11 @@ def mixed_run(args, rank, world, local_rank, clk_samples):
         n_samples += tplan.tasks.size
         seed += 1
     model = CM.CostModel(seed=0, device=dev)
-    losses = model.train(np.concatenate([Xt] * len(ys)), np.concatenate(ys), epochs=8, batch=256, lr=3e-3)
+    # rows weighted by their measured time: the long tasks, which set the
+    # makespan under longest-first placement, are the ones to rank right
+    yall = np.concatenate(ys)
+    losses = model.train(np.concatenate([Xt] * len(ys)), yall, epochs=8, batch=256, lr=3e-3,
+                         weights=np.exp(yall - yall.max()))
     t_train = time.perf_counter() - t0
     del tplan, titems
     X = B.task_features(plan)
@@ -1129,6 +1195,10 @@ def run_reference(args, world):
                 for c, (r, d, kind) in zip(oc, cpu_rates(oc, threads, 5.0)):
                     kern.append({"kernel": c.name, "workload": LABELS[ow], "value": round(r / 1e9, 3), "unit": "GB/s",
                                  "kind": kind, "sample": d})
+                    if c.name == "deflate" and not args.no_gpu_comparator:
+                        comp = cudf_comparator(c.cont, 5, 2)
+                        if comp is not None:
+                            kern[-1]["gpu_comparator"] = comp
                 del oc
                 for f in tmp.iterdir():
                     f.unlink()
@@ -1168,6 +1238,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="default workload without config 5")
+    ap.add_argument("--no-gpu-comparator", action="store_true",
+                    help="reference arm: skip the reference's cuDF inflate on the GPU")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -89,6 +89,7 @@ SIGNATURES = {
     "gd_brle_trans4_encode": (u64, [vp, u64, u64, vp, vp, vp, vp]),
     "gd_deflate_max_encoded_bytes": (u64, [vp, u32]),
     "gd_deflate_encode": (u64, [vp, vp, u32, i32, vp, i32, vp, vp, vp]),
+    "gd_task_features": (i32, [vp, u32, vp, vp]),
     "gd_gen_rlev1_ints": (None, [u64, u64, vp]),
     "gd_gen_brle_bytes": (None, [u64, u64, vp]),
     "gd_gen_rlev2_ints": (None, [u64, u64, vp]),

@@ -259,18 +259,33 @@ def makespan_ms(plan: Plan, order=None, dynamic=True, reps: int = 3, blocks_per_
 N_FEATURES = 16
 
 
+def header_features(plan: Plan) -> np.ndarray:
+    """gd_task_features on the device: (n, 4) float32 -- log2(1 + run
+    headers / tokens), literal share (Deflate: first block type / 2), units
+    per KiB of output (Deflate: dynamic first block's HLIT + 257 over 286),
+    malformed-header flag."""
+    import torch
+    n = plan.tasks.size
+    d = torch.empty(4 * max(n, 1), dtype=torch.float32, device=plan.d_tasks.device)
+    s = torch.cuda.current_stream(plan.d_tasks.device).cuda_stream
+    cc.check(lib().gd_task_features(C.c_void_p(plan.d_tasks.data_ptr()), n, C.c_void_p(d.data_ptr()),
+                                    C.c_void_p(s)), "gd_task_features")
+    return d.cpu().numpy().reshape(-1, 4)[:n]
+
+
 def task_features(plan: Plan) -> np.ndarray:
-    """16 features per task from container metadata only (what a scheduler
-    knows before decoding):
+    """16 features per task, from container metadata and headers only (what
+    a scheduler knows before decoding):
       0-4  codec one-hot (brle, RLE v1, RLE v2, LZSS, Deflate)
       5    log2 compressed bytes the task reads (its lane stream for RLE)
       6    log2 output bytes the task writes
       7    compressed / output bytes
-      8-9  lane-stream length skew of the chunk: max/mean, std/mean (RLE, LZSS)
-      10   this lane's length / mean lane length (RLE)
-      11   log2 chunk (or stream) size
-      12   Deflate stream stored in the clear (compressed >= half its output)
-      13   log2 of compressed bytes per 64 KiB of output
+      8    lane-stream length skew of the chunk, max / mean (RLE, LZSS)
+      9    log2(1 + run headers or tokens)           } the device header
+      10   literal share / Deflate first block type   } walk,
+      11   log2 chunk (or stream) size                  gd_task_features
+      12   units per KiB / Deflate dynamic HLIT share }
+      13   malformed-header flag                      }
       14   log2 size of the whole item
       15   constant 1"""
     T = plan.tasks
@@ -283,8 +298,6 @@ def task_features(plan: Plan) -> np.ndarray:
     src_len = T["src_len"].astype(np.float64)
     dst_len = T["dst_len"].astype(np.float64)
     skew_max = np.ones(n)
-    skew_std = np.ones(n)
-    share = np.ones(n)
     # lane-length statistics of every chunk of the RLE / LZSS items
     lane_items = [i for i, it in enumerate(plan.items) if "col_len" in it.enc.meta]
     if lane_items:
@@ -297,29 +310,25 @@ def task_features(plan: Plan) -> np.ndarray:
             pos += cl.shape[0]
         L = np.concatenate(rows)                     # (chunks, 32)
         mean = np.maximum(L.mean(1), 1.0)
-        cmax, cstd = L.max(1) / mean, L.std(1) / mean
         sel = np.isin(codec, (1, 2, 3))
         r = base[item[sel]] + chunk[sel]
-        skew_max[sel] = cmax[r]
-        skew_std[sel] = cstd[r]
+        skew_max[sel] = (L.max(1) / mean)[r]
         rle = np.isin(codec, (1, 2))
         rr = base[item[rle]] + chunk[rle]
-        lane_len = L[rr, T["lane"][rle].astype(np.int64)]
-        share[rle] = lane_len / mean[rr]
-        src_len[rle] = lane_len
+        src_len[rle] = L[rr, T["lane"][rle].astype(np.int64)]
         dst_len[rle] = dst_len[rle] / 32.0
-    comp_total = np.array([it.enc.comp_bytes for it in plan.items], np.float64)
     out_total = np.array([it.enc.n_out for it in plan.items], np.float64)
+    H = header_features(plan)
     F[:, 5] = np.log2(src_len + 1.0)
     F[:, 6] = np.log2(dst_len + 1.0)
     F[:, 7] = src_len / np.maximum(dst_len, 1.0)
     F[:, 8] = skew_max
-    F[:, 9] = skew_std
-    F[:, 10] = share
+    F[:, 9] = H[:, 0]
+    F[:, 10] = H[:, 1]
     cs = T["chunk_size"].astype(np.float64)
     F[:, 11] = np.log2(np.where(cs > 0, cs, T["dst_len"].astype(np.float64)) + 1.0)
-    F[:, 12] = ((codec == 4) & (comp_total[item] > 0.5 * out_total[item])).astype(np.float32)
-    F[:, 13] = np.log2(src_len / np.maximum(dst_len, 1.0) * 65536.0 + 1.0)
+    F[:, 12] = np.minimum(H[:, 2], 1024.0) / 64.0
+    F[:, 13] = H[:, 3]
     F[:, 14] = np.log2(out_total[item] + 1.0)
     F[:, 15] = 1.0
     return F

@@ -88,8 +88,12 @@ class CostModel:
         return g, loss
 
     def train(self, X: np.ndarray, y: np.ndarray, epochs: int = 20, batch: int = 256, lr: float = 2e-3,
-              seed: int = 0) -> list[float]:
-        """Adam on log-time targets; returns the mean loss of every epoch."""
+              seed: int = 0, weights: np.ndarray | None = None) -> list[float]:
+        """Adam on log-time targets; returns the mean loss of every epoch.
+        weights (optional, one per row): every epoch draws its n rows with
+        replacement in proportion to them (so the squared error of a row
+        counts in proportion to its weight); without them each row is seen
+        once per epoch."""
         torch = self.torch
         if self.step == 0:
             self.fit_normaliser(X, y)
@@ -102,8 +106,14 @@ class CostModel:
         L = lib()
         s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
         d_loss = torch.zeros(max(1, (n + batch - 1) // batch), dtype=torch.float32, device=self.dev)
+        d_w = None
+        if weights is not None:
+            d_w = torch.from_numpy(np.asarray(weights, np.float64) / np.sum(weights)).to(self.dev)
         for _ in range(epochs):
-            perm = torch.randperm(n, generator=gen, device=self.dev).to(torch.int32)
+            if d_w is None:
+                perm = torch.randperm(n, generator=gen, device=self.dev).to(torch.int32)
+            else:
+                perm = torch.multinomial(d_w, n, replacement=True, generator=gen).to(torch.int32)
             nsteps = (n + batch - 1) // batch
             for k in range(nsteps):
                 nb = min(batch, n - k * batch)

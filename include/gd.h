@@ -236,6 +236,23 @@ gd_status_t gd_batch_decode(const gd_task* d_tasks, uint32_t n_tasks, const uint
                             uint32_t max_lane_bytes, uint32_t blocks_per_sm, uint32_t* d_counter,
                             uint32_t* d_status, uint64_t* d_timing, gd_stream_t stream);
 
+/*
+ * No counterpart in the reference.  Header features of every task for the
+ * learned cost model, computed on the device from the containers' headers
+ * only: d_features[4n] (16-byte aligned) receives per task
+ *   [0] log2(1 + units): run headers (RLE v1 / v2 lane), tokens (byte-RLE,
+ *       LZSS chunk), 0 (Deflate);
+ *   [1] literal share: literal values / values (RLE v1), DIRECT and
+ *       PATCHED_BASE runs / runs (RLE v2), literal tokens / tokens (byte-RLE,
+ *       LZSS: 1 - match density), first block type / 2 (Deflate: 0 stored,
+ *       0.5 fixed, 1 dynamic);
+ *   [2] units per KiB of output; Deflate: HLIT + 257 of a dynamic first
+ *       block / 286;
+ *   [3] 1 if the walk found the headers malformed, else 0.
+ * Each walk is bounded by the stream's length.
+ */
+gd_status_t gd_task_features(const gd_task* d_tasks, uint32_t n_tasks, float* d_features, gd_stream_t stream);
+
 /* Number of warps gd_batch_decode runs with for these parameters. */
 uint32_t gd_batch_warps(uint32_t max_lane_bytes, uint32_t blocks_per_sm);
 

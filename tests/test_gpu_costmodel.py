@@ -87,3 +87,127 @@ def test_graph_captured_schedule(batch):
     g.replay()
     torch.cuda.synchronize()
     assert B.verify(plan)
+
+
+# ---------------------------------------------------------------------------
+# header features on the device (gd_task_features) against a host walk of the
+# same headers
+# ---------------------------------------------------------------------------
+
+_W = [1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 24, 26, 28, 30, 32, 40,
+      48, 56, 64]
+
+
+def _cfb(b):
+    for w in [1] + list(range(2, 25)) + [26, 28, 30, 32, 40, 48, 56, 64]:
+        if b <= w:
+            return w
+    return 64
+
+
+def _walk_rlev1(s):
+    pos, hdr, lit, vals = 0, 0, 0, 0
+    while pos < len(s):
+        h = s[pos] - 256 if s[pos] > 127 else s[pos]
+        pos += 1
+        hdr += 1
+        if h < 0:
+            nv, lit, vals = -h, lit - h, vals - h
+        else:
+            nv, vals = 1, vals + h + 3
+            pos += 1
+        for _ in range(nv):
+            while pos < len(s) and s[pos] & 0x80:
+                pos += 1
+            pos += 1
+    return hdr, (lit / vals if vals else 0.0)
+
+
+def _walk_rlev2(s):
+    pos, runs, unpack = 0, 0, 0
+    while pos < len(s):
+        h = s[pos]
+        k = h >> 6
+        runs += 1
+        if k == 0:
+            pos += 2 + ((h >> 3) & 7)
+            continue
+        n, fbw = (((h & 1) << 8) | s[pos + 1]) + 1, _W[(h >> 1) & 31]
+        if k == 1:
+            unpack += 1
+            pos += 2 + (n * fbw + 7) // 8
+        elif k == 2:
+            unpack += 1
+            b2, b3 = s[pos + 2], s[pos + 3]
+            pos += 4 + (b2 >> 5) + 1 + (n * fbw + 7) // 8 + ((b3 & 31) * _cfb(_W[b2 & 31] + (b3 >> 5) + 1) + 7) // 8
+        else:
+            q = pos + 2
+            for _ in range(2):
+                while s[q] & 0x80:
+                    q += 1
+                q += 1
+            pos = q + (((n - 2) * fbw + 7) // 8 if (h >> 1) & 31 else 0)
+    return runs, (unpack / runs if runs else 0.0)
+
+
+def _walk_lzss(cols):
+    toks = lits = 0
+    for s in cols:
+        pos, k, head = 0, 8, 0
+        while pos < len(s):
+            if k == 8:
+                head, k, pos = s[pos], 0, pos + 1
+                continue
+            lit = (head >> k) & 1
+            k += 1
+            toks += 1
+            lits += lit
+            pos += 1 if lit else 2
+    return toks, (lits / toks if toks else 0.0)
+
+
+def test_header_features_match_host_walk(cuda):
+    import oracle
+    items = B.make_mixed_batch(23, 60, 12 << 20, 4096, 1 << 20)
+    plan = B.build_plan(items, cuda)
+    H = B.header_features(plan)
+    T = plan.tasks
+    lanes = {}
+    for ti in range(T.size):
+        it = plan.items[plan.task_item[ti]]
+        e, k = it.enc, int(plan.extra["task_chunk"][ti])
+        units, share, dens = 0, 0.0, 0.0
+        out_b = float(T["dst_len"][ti])
+        if it.codec == "brle":
+            p = e.meta["ptr"]
+            s = e.data[int(p[k]):int(p[k + 1])].tolist()
+            pos = lit = 0
+            while pos < len(s):
+                units += 1
+                if s[pos] > 127:
+                    lit += 1
+                    pos += s[pos] - 126
+                else:
+                    pos += 2
+            share, dens = (lit / units if units else 0.0), units * 1024 / out_b
+        elif it.codec in ("rlev1", "rlev2", "lzss"):
+            if plan.task_item[ti] not in lanes:
+                lanes[plan.task_item[ti]] = oracle.export_lanes(e)
+            L, off = lanes[plan.task_item[ti]]
+            if it.codec == "lzss":
+                cols = [L[off[32 * k + r]:off[32 * k + r + 1]].tolist() for r in range(32)]
+                units, share = _walk_lzss(cols)
+                dens = units * 1024 / out_b
+            else:
+                t = int(T["lane"][ti])
+                s = L[off[32 * k + t]:off[32 * k + t + 1]].tolist()
+                units, share = (_walk_rlev1 if it.codec == "rlev1" else _walk_rlev2)(s)
+                dens = units * 1024 / max(int(out_b) // 32, 1)
+        else:
+            b = int(e.data[int(e.meta["comp_off"][0]) + 2])
+            bt = (b >> 1) & 3
+            share = bt * 0.5
+            dens = (((b >> 3) & 31) + 257) / 286 if bt == 2 else 0.0
+        want = [np.log2(1 + units), share, dens, 0.0]
+        assert np.allclose(H[ti], want, rtol=1e-5, atol=1e-5), (it.codec, ti, H[ti], want)
+    assert set(np.unique(T["codec"])) == {0, 1, 2, 3, 4}
