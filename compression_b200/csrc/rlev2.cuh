@@ -475,7 +475,30 @@ static __device__ __forceinline__ uint32_t decode_stream(const uint8_t* __restri
                     const uint32_t vbit = R.vbit[r0];
                     const bool fixed = ((meta >> 9) & 1u) != 0, sub = ((meta >> 10) & 1u) != 0;
                     if (kind == 3u && !fixed && r0 != cr_run) cr_acc = 0;
-                    do {
+                    // bit-packed kinds: two rounds per iteration, so that the
+                    // two unpack chains overlap
+                    if (ru32 && (kind == 1u || kind == 2u)) {
+                        for (; rb + 64u <= rend; rb += 64) {
+                            const uint32_t i = rb + lane - v0;
+                            const uint64_t xa = extract_msb(sbuf, vbit + i * fbw, fbw);
+                            const uint64_t xb = extract_msb(sbuf, vbit + (i + 32u) * fbw, fbw);
+                            const uint64_t oa = (uint64_t)t * ru + (uint64_t)sl_k * 32u * ru + sl_j + lane;
+                            sl_j += 32;
+                            if (sl_j >= ru) {
+                                sl_j -= ru;
+                                ++sl_k;
+                            }
+                            const uint64_t ob = (uint64_t)t * ru + (uint64_t)sl_k * 32u * ru + sl_j + lane;
+                            sl_j += 32;
+                            if (sl_j >= ru) {
+                                sl_j -= ru;
+                                ++sl_k;
+                            }
+                            if (oa < want_vals) outv[oa] = kind == 1u ? xa : base + xa;
+                            if (ob < want_vals) outv[ob] = kind == 1u ? xb : base + xb;
+                        }
+                    }
+                    while (rb + 32u <= rend) {
                         const uint32_t i = rb + lane - v0;  // index of this lane's value in the run
                         uint64_t v = base;
                         if (kind == 1u || kind == 2u) {
@@ -507,7 +530,7 @@ static __device__ __forceinline__ uint32_t decode_stream(const uint8_t* __restri
                             ++sl_k;
                         }
                         rb += 32;
-                    } while (rb + 32u <= rend);
+                    }
                     rcur = r0;
                     cr_run = r0;
                     continue;
