@@ -12,9 +12,10 @@ are compiled into libgd.so or sets a launch shape:
   brle     GD_TUNE_BRLE_BLOCKS_PER_SM     grid = value x SMs
   rlev1    GD_TUNE_RLEV1_LANES_PER_BLOCK  lane streams (warps) per block
   rlev2    GD_TUNE_RLEV2_LANES_PER_BLOCK  lane streams (warps) per block
-  lzss     GD_TUNE_LZSS_WARPS_PER_BLOCK   0 / 512: 16 lanes per column, 256: 8, 1: one lane per
-                                          column (all stage the chunk in shared memory); 2 / 4 / 8:
-                                          chunks (warps) per block, output written as decoded
+  lzss     GD_TUNE_LZSS_WARPS_PER_BLOCK   0: a warp per chunk, a lane per column, output in rounds
+                                          (1 chunk per block), 4: the same, 4 per block; 512 / 256:
+                                          16 / 8 lanes per column, 1: a lane per column (these stage
+                                          the whole chunk in shared memory)
 
 For the batched decoder the tuned quantity is its blocks per SM (4 warps each),
 which sets how many tasks run at once against how much shared memory each
@@ -51,7 +52,7 @@ KNOBS = {
     "brle": (TUNE_BRLE_BLOCKS_PER_SM, [8, 4, 16]),
     "rlev1": (TUNE_RLEV1_LANES_PER_BLOCK, [8, 4]),
     "rlev2": (TUNE_RLEV2_LANES_PER_BLOCK, [4, 8]),
-    "lzss": (TUNE_LZSS_WARPS_PER_BLOCK, [0, 256, 1, 4]),
+    "lzss": (TUNE_LZSS_WARPS_PER_BLOCK, [0, 4, 512, 256]),
 }
 
 

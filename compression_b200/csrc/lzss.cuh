@@ -1,5 +1,5 @@
-// lzss.cuh -- warp-level LZSS chunk decoder (shared by the plain kernel in
-// lzss.cu and the batched decoder in batch.cu).
+// lzss.cuh -- LZSS chunk decoders (the plain kernels in lzss.cu; chunk_warp
+// serves the batched decoder in batch.cu).
 //
 // Grammar (restated from lzss::decompress_func, include/lzss/lzss_gpu2.h:
 // 112-325): per column stream, a flag byte then 8 tokens LSB-first; flag 1 =
@@ -9,23 +9,38 @@
 // length (col_len sorted, col_map = rank -> column) and 4-byte interleaved.
 //
 // The reference runs one thread per column with a 2 KiB history array in
-// local memory and byte-wise 4-byte-strided stores.  Here a warp decodes a
-// chunk (lane = rank) with the shared interleave reader; each round every
-// lane produces 64 bytes (16 output rows) of its column into shared memory,
-// then the warp writes those 16 rows (2 KiB contiguous) with coalesced
-// stores.  Match sources inside the current round come from shared memory,
-// older ones from the already-written output (same SM, ordered by
-// __syncwarp).  A match never overlaps its source (length <= offset,
-// lzss_gpu2.h:79), but the byte loop is correct either way.
+// local memory and byte-wise 4-byte-strided stores.  Four decoders here:
+//   * chunk_warp (the batch decoder's): a warp per chunk, a lane per column,
+//     one output byte per lane and step;
+//   * chunk_warp_groups (the default): a warp per chunk, a lane per column,
+//     a flag group of tokens per lane and step, output staged per lane in
+//     rounds and written as whole rows;
+//   * chunk_block_cols: a block per chunk, 8 or 16 lanes per column, the
+//     whole chunk staged in shared memory;
+//   * chunk_warp_staged: a warp per chunk, a lane per column, the whole chunk
+//     staged (3 chunks per SM).
+// A match never overlaps its source in the reference encoder's output
+// (length <= offset, lzss_gpu2.h:79), but every decoder copies self-
+// overlapping matches byte-exactly, as the reference's byte loop does.
 #pragma once
 #include "interleave.cuh"
 
 namespace gd {
 namespace lzss {
 
-constexpr uint32_t RB = 64;        // column bytes per lane per round (16 rows)
-constexpr uint32_t SSTR = RB + 4;  // 17 words: row reads across columns are conflict-free
-constexpr uint32_t WARP_SMEM = (uint32_t)sizeof(SegTable) + 32u * RING_STRIDE + 32u * SSTR;
+// Byte-loop warp decoder (the batch decoder's LZSS path): a warp per chunk,
+// a lane per column, one output byte per lane and step.  Each round every
+// lane produces 64 bytes (16 output rows) of its column into shared memory,
+// then the warp writes those 16 rows (2 KiB contiguous) with coalesced
+// stores.  Match sources inside the current round come from shared memory,
+// older ones from the already-written output (same SM, ordered by
+// __syncwarp).  Inside the batch kernel it measured faster than the group
+// decoder below (mixed batch 20.6 against 23.2 ms, longest-first order):
+// with the group decoder the other codecs' tasks ran slower beside it too
+// (the cause was not isolated).
+constexpr uint32_t WARP_RB = 64;             // column bytes per lane per round (16 rows)
+constexpr uint32_t WARP_SSTR = WARP_RB + 4;  // 17 words: row reads across columns are conflict-free
+constexpr uint32_t WARP_SMEM = (uint32_t)sizeof(SegTable) + 32u * RING_STRIDE + 32u * WARP_SSTR;
 
 // Decode one LZSS chunk with the calling warp.  `block` = the chunk's
 // interleaved block (b_len bytes, 4-byte aligned), col_len/col_map = its 32
@@ -66,8 +81,8 @@ static __device__ __noinline__ uint32_t chunk_warp(const uint8_t* __restrict__ b
     LaneRing r{ring + lane * RING_STRIDE, 0, 0, len};
 
     const uint32_t col_bytes = (uint32_t)(chunk_size / 32);
-    const uint32_t rounds = (col_bytes + RB - 1) / RB;
-    uint8_t* my_stage = stage + q * SSTR;
+    const uint32_t rounds = (col_bytes + WARP_RB - 1) / WARP_RB;
+    uint8_t* my_stage = stage + q * WARP_SSTR;
     uint32_t o = 0;            // column bytes produced
     uint32_t flags = 0, ntok = 0;
     uint32_t mrem = 0, msrc = 0;  // pending match: bytes left, source position
@@ -80,8 +95,8 @@ static __device__ __noinline__ uint32_t chunk_warp(const uint8_t* __restrict__ b
     };
 
     for (uint32_t rnd = 0; rnd < rounds; ++rnd) {
-        const uint32_t r0 = rnd * RB;
-        const uint32_t rend = min(r0 + RB, col_bytes);
+        const uint32_t r0 = rnd * WARP_RB;
+        const uint32_t rend = min(r0 + WARP_RB, col_bytes);
         for (;;) {
             const bool act = (o < rend) && (err == ST_OK);
             const bool need = act && (r.fl - r.rd < (uint32_t)RING_LOW) && (lw.k < lw.nw);
@@ -142,12 +157,228 @@ static __device__ __noinline__ uint32_t chunk_warp(const uint8_t* __restrict__ b
         // rows [r0/4, rend/4): lane l writes column l's word of every row
         const uint32_t rows = (rend - r0) >> 2;
         for (uint32_t i = 0; i < rows; ++i) {
-            const uint32_t w = *reinterpret_cast<const uint32_t*>(stage + lane * SSTR + 4 * i);
+            const uint32_t w = *reinterpret_cast<const uint32_t*>(stage + lane * WARP_SSTR + 4 * i);
             reinterpret_cast<uint32_t*>(cout)[(size_t)(r0 / 4 + i) * 32u + lane] = w;
         }
         __syncwarp();
         if (__any_sync(GD_FULL_MASK, err != ST_OK)) break;
     }
+    if (err == ST_OK && o != col_bytes) err = ST_CORRUPT;
+    return __reduce_max_sync(GD_FULL_MASK, err);
+}
+
+// ---------------------------------------------------------------------------
+// Group decoder: one warp per chunk, one lane per column, up to one flag
+// group (8 tokens) per lane and step.
+//
+// The token positions of a group follow from its flag byte alone, so a lane
+// loads the group's token bytes together, derives every token's length and
+// source with a running sum, loads all match sources before writing
+// anything, and appends the tokens through a register holding the column's
+// partial word.  The output is produced in rounds of RB column bytes per
+// lane: a round's bytes are staged in the lane's own shared-memory slice and
+// written out as whole 128-byte rows (the 32 lanes store row k of the chunk
+// together: coalesced).  A token may end up to 33 bytes past the round; those
+// bytes move to the front of the slice for the next round.  Match sources
+// before the round are read back from the output, which this same lane wrote
+// (a column's words are stored only by its own lane), so program order makes
+// them visible; sources inside the round come from the slice.  With 320-byte
+// rounds and a 64-byte input ring a warp holds 14.5 KiB of shared memory, so
+// 15 chunks run per SM (3 when the whole 64 KiB output of a chunk is
+// staged).  More chunks in flight measured slower: their recent output, which
+// the history reads go back to, no longer fits in L2.
+// Long (> 8 byte) and self-overlapping (offset < length) matches take a 4-
+// or 1-byte loop (byte-exact for every offset >= 1, as the reference's
+// byte-wise copy).  The statuses are those of the other decoders: a column
+// stops at its first bad token (CORRUPT: stream exhausted, offset 0 or
+// before the column start; OVERRUN: past the column end), the chunk reports
+// the largest code over its columns.
+// ---------------------------------------------------------------------------
+constexpr uint32_t GSLACK = 48;  // a round's last token and the 12-byte store window run past RB
+__host__ __device__ constexpr uint32_t group_sstr(uint32_t rb) { return rb + GSLACK + 4u; }  // odd word count
+// input ring of GR bytes per lane, padded to an odd word count (lanes at
+// equal offsets hit distinct banks)
+__host__ __device__ constexpr uint32_t group_rstr(uint32_t gr) { return gr + 4u; }
+__host__ __device__ constexpr uint32_t group_warp_smem(uint32_t rb, uint32_t gr) {
+    return (uint32_t)sizeof(SegTable) + 32u * group_rstr(gr) + 32u * group_sstr(rb);
+}
+
+template <uint32_t RB, uint32_t GRING>
+static __device__ __forceinline__ uint32_t chunk_warp_groups(const uint8_t* __restrict__ block, uint64_t b_len,
+                                                            const uint64_t* __restrict__ col_len,
+                                                            const uint8_t* __restrict__ col_map, uint64_t chunk_size,
+                                                            uint8_t* cout, uint8_t* wsmem) {
+    static_assert(RB % 4 == 0 && (group_sstr(RB) / 4) % 2 == 1, "round bytes");
+    static_assert(GRING >= 64 && (GRING & (GRING - 1)) == 0, "ring bytes");
+    const uint32_t lane = lane_id();
+    SegTable* T_ = reinterpret_cast<SegTable*>(wsmem);
+    uint8_t* rbuf = wsmem + sizeof(SegTable) + lane * group_rstr(GRING);
+    uint32_t* st =
+        reinterpret_cast<uint32_t*>(wsmem + sizeof(SegTable) + 32u * group_rstr(GRING) + lane * group_sstr(RB));
+
+    uint32_t err = ST_OK;
+    const uint64_t len64 = col_len[lane];
+    const uint32_t len = len64 > 0x3fffffffull ? 0u : (uint32_t)len64;
+    if (len64 > 0x3fffffffull) err = ST_CORRUPT;
+    const uint32_t q = col_map[lane];
+    if (q >= 32) err = ST_CORRUPT;
+    {  // col_map must be a permutation of the 32 columns
+        uint32_t bits = 0;
+#pragma unroll
+        for (int o = 0; o < 32; ++o) bits |= 1u << (__shfl_sync(GD_FULL_MASK, q, o) & 31u);
+        if (bits != 0xffffffffu) err = ST_CORRUPT;
+    }
+    const uint32_t nw = (len + 3) >> 2;
+    uint32_t tot = warp_incl_scan(nw);
+    tot = __shfl_sync(GD_FULL_MASK, tot, 31);
+    if ((uint64_t)tot * 4 > b_len) err = ST_CORRUPT;
+    if ((reinterpret_cast<uintptr_t>(block) & 3u) != 0) err = ST_CORRUPT;  // words are 4-byte copies
+    if ((reinterpret_cast<uintptr_t>(cout) & 3u) != 0) err = ST_INVALID;    // rows are 4-byte stores
+    if (chunk_size == 0 || chunk_size % 128 || chunk_size > (1ull << 31)) err = ST_INVALID;
+    if (__any_sync(GD_FULL_MASK, err != ST_OK)) return __reduce_max_sync(GD_FULL_MASK, err);
+    seg_build(T_, nw);
+    const uint32_t ltmask = (1u << lane) - 1u;
+    LaneWords lw;
+    lw_init(lw, T_, nw);
+
+    const uint32_t col_bytes = (uint32_t)(chunk_size / 32);
+    uint32_t* gcol = reinterpret_cast<uint32_t*>(cout) + q;  // column q's word k is gcol[32k]
+    uint32_t rd = 0, fl = 0, arrived = 0;  // ring: bytes [rd, arrived) readable, [arrived, fl) in flight
+    uint32_t o = 0, acc = 0;               // column bytes produced; the bytes of the partial word o >> 2
+    uint32_t flags = 0, ntok = 0;          // the current group's remaining flag bits and tokens
+    uint32_t r0 = 0, kr0 = 0;              // the round's first column byte and word
+
+    auto prefetch = [&]() {  // top the ring up (asynchronous 4-byte copies)
+        uint32_t n = 0;
+        while (lw.k < lw.nw && fl - rd <= GRING - 4u) {
+            const uint32_t off = lw_addr(lw, T_, ltmask, lw.k);
+            const uint32_t sa = (uint32_t)__cvta_generic_to_shared(rbuf + (fl & (GRING - 1u)));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(block + off) : "memory");
+            fl += 4;
+            ++lw.k;
+            ++n;
+        }
+        if (n) asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    auto rb = [&](uint32_t p) -> uint32_t { return rbuf[p & (GRING - 1u)]; };
+    // word k of the column: the slice from the round start on, else the output
+    auto word = [&](uint32_t k) -> uint32_t { return k >= kr0 ? st[k - kr0] : gcol[(size_t)k * 32u]; };
+    auto rd8 = [&](uint32_t sp) -> uint64_t {  // column bytes sp .. sp+7
+        const uint32_t k = sp >> 2, sh = (sp & 3u) * 8u;
+        const uint32_t w0 = word(k), w1 = word(k + 1u), w2 = word(k + 2u);
+        return ((uint64_t)__funnelshift_r(w1, w2, sh) << 32) | __funnelshift_r(w0, w1, sh);
+    };
+    // append the n (1..8) low bytes of x (zero above them): the partial word
+    // and the two words after it are stored (bytes past o are rewritten
+    // before anything reads them)
+    auto put = [&](uint64_t x, uint32_t n) {
+        const uint32_t s = o - r0, sh = (s & 3u) * 8u;
+        uint32_t* w = st + (s >> 2);
+        const uint64_t v = (uint64_t)acc | (x << sh);
+        const uint32_t hi = sh ? (uint32_t)(x >> (64u - sh)) : 0u;
+        w[0] = (uint32_t)v;
+        w[1] = (uint32_t)(v >> 32);
+        w[2] = hi;
+        const uint32_t e = (s & 3u) + n;
+        acc = e < 4u ? (uint32_t)v : (e < 8u ? (uint32_t)(v >> 32) : hi);
+        o += n;
+    };
+    auto mask = [](uint32_t n) -> uint64_t { return n >= 8u ? ~0ull : ((1ull << (8u * n)) - 1ull); };
+
+    prefetch();
+    for (; r0 < col_bytes; r0 += RB, kr0 += RB / 4u) {
+        const uint32_t rend = min(r0 + RB, col_bytes);
+        for (;;) {
+            const bool act = o < rend && err == ST_OK;
+            if (!__any_sync(GD_FULL_MASK, act)) break;
+            // rings are topped up together once any active lane's is half empty
+            if (__any_sync(GD_FULL_MASK, act && fl - rd <= GRING / 2u && lw.k < lw.nw)) prefetch();
+            if (!act) continue;
+            // a step reads bytes rd .. rd+16 (a flag byte and 8 two-byte tokens)
+            if (arrived < fl && arrived < rd + 17u) {
+                asm volatile("cp.async.wait_all;\n" ::: "memory");
+                arrived = fl;
+            }
+            if (ntok == 0) {
+                if (rd >= len) {
+                    err = ST_CORRUPT;
+                    continue;
+                }
+                flags = rb(rd);
+                ++rd;
+                ntok = 8;
+            }
+            // the tokens' bytes: token t starts t + (matches before it) bytes after rd
+            uint32_t v[8];
+#pragma unroll
+            for (uint32_t t = 0; t < 8; ++t) {
+                const uint32_t p = rd + t + __popc(~flags & ((1u << t) - 1u));
+                v[t] = rb(p) | (rb(p + 1u) << 8);
+            }
+            // lengths and sources of the tokens that start inside the round;
+            // a bad token ends the column
+            uint32_t L[8], src[8];
+            uint32_t p = rd, oo = o, nc = 0;
+            bool stop = false;
+#pragma unroll
+            for (uint32_t t = 0; t < 8; ++t) {
+                const bool lit = (flags >> t) & 1u;
+                const uint32_t ml = lit ? 1u : (v[t] & 31u) + 3u, off = lit ? 0u : v[t] >> 5;
+                const bool live = !stop && t < ntok && oo < rend;
+                const bool nobytes = p + (lit ? 0u : 1u) >= len;
+                const bool badoff = !lit && (off == 0 || off > oo);
+                const bool over = oo + ml > col_bytes;
+                if (live && (nobytes || badoff || over)) {
+                    err = (nobytes || badoff) ? ST_CORRUPT : ST_OVERRUN;
+                    stop = true;
+                }
+                const bool ok = live && !stop;
+                L[t] = ok ? ml : 0u;
+                src[t] = oo - off;
+                oo += ok ? ml : 0u;
+                p += ok ? (lit ? 1u : 2u) : 0u;
+                nc += ok ? 1u : 0u;
+            }
+            // match sources as they are before this group writes anything
+            uint64_t x[8];
+#pragma unroll
+            for (uint32_t t = 0; t < 8; ++t)
+                x[t] = (L[t] && !((flags >> t) & 1u)) ? rd8(src[t]) : (uint64_t)(v[t] & 0xffu);
+            const uint32_t o0 = o;
+#pragma unroll
+            for (uint32_t t = 0; t < 8; ++t) {
+                const uint32_t n = L[t];
+                if (n == 0) continue;
+                const uint32_t sp = src[t], off = o - sp;
+                const bool lit = (flags >> t) & 1u;
+                if (lit || (n <= 8u && off >= n)) {
+                    // a source reaching into this group's output is re-read now
+                    const uint64_t y = (!lit && sp + n > o0) ? rd8(sp) : x[t];
+                    put(y & mask(n), n);
+                } else {
+                    // long or self-overlapping match: each piece is read after
+                    // the bytes before it are written
+                    const uint32_t step = off >= 8u ? 8u : (off >= 4u ? 4u : 1u);
+                    for (uint32_t j = 0; j < n; j += step) {
+                        const uint32_t m = min(step, n - j);
+                        put(rd8(sp + j) & mask(m), m);
+                    }
+                }
+            }
+            rd = p;
+            flags >>= nc;
+            ntok -= nc;
+        }
+        // the round's rows, then the bytes past it to the front of the slice
+        __syncwarp();
+        const uint32_t rows = (rend - r0) >> 2;
+        for (uint32_t i = 0; i < rows; ++i) gcol[(size_t)(kr0 + i) * 32u] = st[i];
+        if (o > rend) {
+            const uint32_t cw = (o - rend + 3u) >> 2;
+            for (uint32_t i = 0; i < cw; ++i) st[i] = st[rows + i];
+        }
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     if (err == ST_OK && o != col_bytes) err = ST_CORRUPT;
     return __reduce_max_sync(GD_FULL_MASK, err);
 }

@@ -298,13 +298,13 @@ typedef enum gd_tune_key {
     GD_TUNE_BRLE_BLOCKS_PER_SM = 1,   /* byte-RLE grid = value x SMs blocks (default 8) */
     GD_TUNE_RLEV1_LANES_PER_BLOCK = 2, /* 0/8: 8 lane streams per block; 4: 4 */
     GD_TUNE_RLEV2_LANES_PER_BLOCK = 3, /* 0/4: 4 lane streams per block; 8: 8 */
-    GD_TUNE_LZSS_WARPS_PER_BLOCK = 4,  /* 0 / 512: one chunk per 512-thread block, 16 lanes per
-                                          column (two flag groups per step), output staged in shared
-                                          memory; 256: 8 lanes per column (one group per step);
-                                          1: one chunk per warp, one lane per column, output staged;
-                                          2 / 4 / 8: that many chunks (warps) per block, output
-                                          written as decoded (also the path for chunks too large to
-                                          stage, > 200 KiB) */
+    GD_TUNE_LZSS_WARPS_PER_BLOCK = 4,  /* 0: one chunk per 32-thread block, one lane per column, a
+                                          flag group per lane and step, output in 320-byte rounds
+                                          per column (any chunk size); 4: the same with four chunks
+                                          per block and 256-byte rounds (the batch decoder's shape);
+                                          512 / 256: one chunk per block of 512 / 256 threads, 16 / 8
+                                          lanes per column, output staged in shared memory; 1: one
+                                          chunk per warp, one lane per column, output staged */
     GD_TUNE_INFLATE_PAIR_SPIN = 5,     /* polls of a decoder/writer hand-off wait before the stream
                                           gives up with GD_ERR_TIMEOUT (0: 2^25, about a second) */
     GD_TUNE_INFLATE_WRITER_STOP = 6,   /* test knob for the bounded hand-off wait: k > 0 makes each

@@ -341,7 +341,7 @@ def _lzss_token_column(rng, col_bytes):
     return np.frombuffer(bytes(out), np.uint8)
 
 
-@pytest.mark.parametrize("knob", [0, 256, 1, 4])
+@pytest.mark.parametrize("knob", [0, 4, 512, 256, 1])
 @pytest.mark.parametrize("chunk", [4096, 65536])
 def test_lzss_token_shapes(cuda, knob, chunk):
     from test_golden import interleave_streams
