@@ -1240,8 +1240,15 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="default workload without config 5")
     ap.add_argument("--no-gpu-comparator", action="store_true",
                     help="reference arm: skip the reference's cuDF inflate on the GPU")
+    ap.add_argument("--tune", action="append", default=[], metavar="CODEC=VALUE",
+                    help="pin a decoder knob (autotune.KNOBS), e.g. lzss=512; repeatable")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.tune and args.impl == "ours":
+        from compression_b200 import autotune as AT
+        for kv in args.tune:
+            codec, val = kv.split("=", 1)
+            AT.set_knob(AT.KNOBS[codec][0], int(val))
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -1265,6 +1272,8 @@ def main():
         line = run_encode(args, rank, world, local_rank)
     else:
         line = run_ours(args, rank, world, local_rank)
+    if args.tune and isinstance(line, dict) and isinstance(line.get("config"), dict):
+        line["config"]["tune"] = args.tune
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
