@@ -447,3 +447,91 @@ def test_rlev2_decoder_shapes(cuda, knob):
         assert (st != 0).any()
     finally:
         at.set_knob(at.TUNE_RLEV2_LANES_PER_BLOCK, prev)
+
+
+def _lzss_pack(toks):
+    """Token list (("l", byte) or ("m", offset, length)) -> LZSS column stream."""
+    out = bytearray()
+    for g in range(0, len(toks), 8):
+        grp = toks[g:g + 8]
+        out.append(sum(1 << i for i, t in enumerate(grp) if t[0] == "l"))
+        for t in grp:
+            if t[0] == "l":
+                out.append(t[1])
+            else:
+                v = (t[1] << 5) | (t[2] - 3)
+                out += bytes([v & 0xFF, v >> 8])
+    return np.frombuffer(bytes(out), np.uint8)
+
+
+def _lzss_tokens_ending_in_match(rng, col_bytes):
+    toks, o = [], 0
+    while o < col_bytes - 8:
+        if o < 4 or col_bytes - 8 - o < 3 or rng.random() < 0.6:
+            toks.append(("l", int(rng.integers(0, 256))))
+            o += 1
+        else:
+            ln = int(rng.integers(3, min(35, col_bytes - 8 - o + 1)))
+            toks.append(("m", int(rng.integers(1, min(o, 2047) + 1)), ln))
+            o += ln
+    while o < col_bytes - 5:
+        toks.append(("l", int(rng.integers(0, 256))))
+        o += 1
+    toks.append(("m", int(rng.integers(1, o + 1)), col_bytes - o))  # the last token: a match up to the end
+    return toks
+
+
+def test_lzss_corrupt_statuses_agree(cuda):
+    """One planted defect per chunk (truncated column, offset past the column
+    start, offset 0, a last match running past the column end): every LZSS
+    kernel choice reports the oracle's status for every chunk, and the clean
+    chunk decodes as the oracle does."""
+    from test_golden import interleave_streams
+    import compression_b200.autotune as at
+    rng = np.random.default_rng(77)
+    chunk = 65536
+    cb = chunk // 32
+    blocks, cls, maps = [], [], []
+    for c in range(5):
+        cols = []
+        for q in range(32):
+            toks = _lzss_tokens_ending_in_match(rng, cb)
+            if c == 2 and q == 7:    # first match reaches before the column start
+                i = next(k for k, t in enumerate(toks) if t[0] == "m")
+                o = sum(1 if t[0] == "l" else t[2] for t in toks[:i])
+                toks[i] = ("m", o + 1, toks[i][2])
+            if c == 3 and q == 9:    # the last match runs 3 bytes past the column end
+                toks[-1] = ("m", toks[-1][1], toks[-1][2] + 3)
+            if c == 4 and q == 20:   # a match with offset 0
+                i = next(k for k, t in enumerate(toks) if t[0] == "m")
+                toks[i] = ("m", 0, toks[i][2])
+            s = _lzss_pack(toks)
+            if c == 1 and q == 5:    # truncated: the stream ends inside its last match
+                s = s[:-1]
+            cols.append(s)
+        order = sorted(range(32), key=lambda q: -cols[q].size)
+        blk, cl = interleave_streams([cols[q] for q in order])
+        blocks.append(blk)
+        cls.append(cl)
+        maps.append(np.array(order, np.uint8))
+    # the oracle's status of every chunk alone
+    want, ref = [], None
+    for c in range(5):
+        one = cc.Encoded("lzss", blocks[c].copy(), chunk, 1, chunk,
+                         {"blk_off": np.array([0, blocks[c].size], np.uint64), "col_len": cls[c], "col_map": maps[c]})
+        rc, out = oracle.decode(one)
+        want.append(rc)
+        if c == 0:
+            ref = out
+    assert want == [0, 2, 2, 3, 2]  # GD_OK, GD_ERR_CORRUPT x2, GD_ERR_OVERRUN, GD_ERR_CORRUPT
+    bo = np.concatenate([[0], np.cumsum([b.size for b in blocks])]).astype(np.uint64)
+    e = cc.Encoded("lzss", np.concatenate(blocks), 5 * chunk, 5, chunk,
+                   {"blk_off": bo, "col_len": np.concatenate(cls), "col_map": np.concatenate(maps)})
+    for knob in (0, 4, 512, 256, 1):
+        prev = at.set_knob(at.TUNE_LZSS_WARPS_PER_BLOCK, knob)
+        try:
+            st, out = _gpu(e, cuda)
+        finally:
+            at.set_knob(at.TUNE_LZSS_WARPS_PER_BLOCK, prev)
+        assert list(st) == want, (knob, list(st))
+        assert np.array_equal(out[:chunk], ref), knob
