@@ -716,15 +716,18 @@ def task_bytes(plan):
 def mixed_run(args, rank, world, local_rank, clk_samples):
     """Config 5, the mixed-codec batch: 16384 items (log-uniform 4 KiB - 2 MiB,
     4 GiB decompressed in all; 20% RLE v1, 20% RLE v2, 10% byte-RLE, 25% LZSS,
-    25% Deflate) decoded in one persistent launch under five schedules:
+    25% Deflate) decoded in one persistent launch under seven schedules:
 
     * static: task i on warp i mod W (the fallback);
     * queue_fifo: the dynamic work queue in task order;
     * size_lpt_out / size_lpt_in: longest-first through the queue with the
       task's decompressed / compressed bytes as its cost (the method without
       the network);
-    * learned_lpt: longest-first by the cost model's prediction, as one
-      CUDA-graph replay of [MLP inference -> order -> batch decode].
+    * learned_lpt: longest-first by the cost model's prediction (the lane
+      tasks of an RLE chunk keyed by their largest prediction, kept
+      together), as one CUDA-graph replay of [MLP inference -> group maximum
+      -> order -> batch decode]; learned_order_only is that order computed
+      beforehand, learned_per_task every task by its own prediction.
 
     The cost model is trained on a separate, quarter-size batch of the same
     mix (other seeds), on 200k+ per-task decode times that the batch decoder
@@ -792,11 +795,13 @@ def mixed_run(args, rank, world, local_rank, clk_samples):
     out_b, in_b = task_bytes(plan)
     # the learned order itself, computed once, so that the schedule's quality
     # is timed apart from the cost of inference and sorting
+    groups = CM.task_groups(plan)
     orders = {"size_lpt_out": CM.lpt_order(out_b), "size_lpt_in": CM.lpt_order(in_b),
-              "learned_order_only": CM.lpt_order(pred)}
+              "learned_order_only": CM.lpt_order(pred, groups), "learned_per_task": CM.lpt_order(pred)}
 
     flush = torch.empty(256 * MiB, dtype=torch.uint8, device=dev)
-    kinds = ("learned_lpt", "static", "queue_fifo", "size_lpt_out", "size_lpt_in", "learned_order_only")
+    kinds = ("learned_lpt", "static", "queue_fifo", "size_lpt_out", "size_lpt_in", "learned_order_only",
+             "learned_per_task")
 
     def run(kind):
         if kind == "static":
@@ -907,8 +912,11 @@ def mixed_run(args, rank, world, local_rank, clk_samples):
         "schedules": {"static": "task i on warp i mod W", "queue_fifo": "work queue, task order",
                       "size_lpt_out": "work queue, longest first by decompressed bytes per task",
                       "size_lpt_in": "work queue, longest first by compressed bytes per task",
-                      "learned_lpt": "CUDA graph: MLP inference + argsort + work queue (all timed)",
-                      "learned_order_only": "work queue in the learned order computed beforehand"},
+                      "learned_lpt": "CUDA graph: MLP inference + group maximum + argsort + work queue (all "
+                                     "timed); the 32 lane tasks of an RLE chunk share their largest prediction "
+                                     "and stay adjacent",
+                      "learned_order_only": "work queue in the learned (grouped) order computed beforehand",
+                      "learned_per_task": "work queue, every task by its own prediction (no grouping)"},
         "cost_model": {"train_batch": "separate quarter-size batch of the same mix (other seeds)",
                        "samples": int(sum(y.size for y in ys)), "epochs": 8, "final_loss": round(float(losses[-1]), 4),
                        "corr_pred_measured_eval_batch": round(corr, 4), "train_s": round(t_train, 1)},

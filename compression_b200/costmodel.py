@@ -8,8 +8,14 @@ The training data are per-task times the batch decoder measures itself
 (%globaltimer stamps around every task).
 
 Scheduling: tasks are sorted by predicted cost, longest first, and fed to the
-persistent decoder's work queue -- LPT list scheduling.  The static mapping
-(task i -> warp i mod W) remains the fallback.
+persistent decoder's work queue -- LPT list scheduling.  The lane tasks of one
+RLE chunk (the 32 tasks that read the same interleaved block) are ordered as
+one group, keyed by their largest prediction, so that they stay adjacent in
+the queue and run side by side: each of them reads 4 bytes of every 128-byte
+row of the block, and when they run apart every one of them fetches the rows
+again (ordering every task by its own measured time was slower than ordering
+by output bytes for that reason).  The static mapping (task i -> warp i mod W)
+remains the fallback.
 """
 from __future__ import annotations
 
@@ -144,10 +150,36 @@ class CostModel:
 # scheduling
 # --------------------------------------------------------------------------
 
-def lpt_order(cost: np.ndarray):
-    """Task order, longest predicted first (device int32 tensor)."""
+def task_groups(plan: B.Plan) -> np.ndarray:
+    """Group id of every task: a run of consecutive tasks that read the same
+    source block (the lane tasks of one RLE chunk, which the plan lists
+    together) is one group; every other task is a group alone.  Ids count up
+    in task order, so a group's tasks are contiguous."""
+    src = plan.tasks["src"]
+    new = np.ones(src.size, bool)
+    new[1:] = src[1:] != src[:-1]
+    return (np.cumsum(new) - 1).astype(np.int64)
+
+
+def group_max(cost: np.ndarray, groups: np.ndarray) -> np.ndarray:
+    """Every task's cost replaced by the largest cost in its group."""
+    cost = np.asarray(cost, np.float64)
+    k = np.full(int(groups.max()) + 1 if groups.size else 0, -np.inf)
+    np.maximum.at(k, groups, cost)
+    return k[groups]
+
+
+def lpt_order_host(cost: np.ndarray, groups: np.ndarray | None = None) -> np.ndarray:
+    """Task order, longest predicted first; with groups, a group's tasks share
+    its largest cost and stay together, in task order (ties keep task order)."""
+    key = np.asarray(cost, np.float64) if groups is None else group_max(cost, groups)
+    return np.argsort(-key, kind="stable").astype(np.int32)
+
+
+def lpt_order(cost: np.ndarray, groups: np.ndarray | None = None):
+    """lpt_order_host as a device int32 tensor (the batch decoder's order)."""
     import torch
-    return torch.from_numpy(np.argsort(-np.asarray(cost), kind="stable").astype(np.int32)).cuda()
+    return torch.from_numpy(lpt_order_host(cost, groups)).cuda()
 
 
 def measure_tasks(plan: B.Plan, seed: int = 0, reps: int = 1) -> np.ndarray:
@@ -166,27 +198,54 @@ def measure_tasks(plan: B.Plan, seed: int = 0, reps: int = 1) -> np.ndarray:
 
 
 class GraphSchedule:
-    """[MLP inference -> longest-first sort -> persistent decode] captured in
-    one CUDA graph over device-resident features; replay() decodes the batch."""
+    """[MLP inference -> group maximum -> longest-first sort -> persistent
+    decode] captured in one CUDA graph over device-resident features;
+    replay() decodes the batch.  groups: task_groups(plan) (default; groups
+    must be contiguous runs of tasks), or None to order every task by its own
+    prediction."""
 
-    def __init__(self, plan: B.Plan, model: CostModel, X: np.ndarray):
+    _AUTO = object()
+
+    def __init__(self, plan: B.Plan, model: CostModel, X: np.ndarray, groups=_AUTO):
         import torch
         self.torch = torch
         self.plan = plan
         n = plan.tasks.size
+        if groups is GraphSchedule._AUTO:
+            groups = task_groups(plan)
         self.d_x = torch.from_numpy(model._norm(X)).cuda()
-        self.d_pred = torch.empty(n, dtype=torch.float32, device="cuda")
+        # the group maximum as a padded gather (no atomics, no host syncs, so
+        # it can be captured): row g of d_gidx lists group g's tasks, padded
+        # with n, which points at a -inf after the predictions
+        self.d_pred = torch.full((n + 1,), float("-inf"), dtype=torch.float32, device="cuda")
+        self.d_grp = self.d_gidx = None
+        if groups is not None:
+            groups = np.asarray(groups, np.int64)
+            ng = int(groups.max()) + 1 if n else 0
+            cnt = np.bincount(groups, minlength=ng)
+            first = np.concatenate([[0], np.cumsum(cnt)[:-1]])
+            order = np.argsort(groups, kind="stable")  # tasks grouped, in task order
+            gidx = np.full((ng, int(cnt.max()) if ng else 1), n, np.int64)
+            gidx[groups[order], np.arange(n) - first[groups[order]]] = order
+            self.d_grp = torch.from_numpy(groups).cuda()
+            self.d_gidx = torch.from_numpy(gidx).cuda()
+
+        def order_of():
+            key = self.d_pred[:n]
+            if self.d_grp is not None:
+                key = self.d_pred[self.d_gidx].amax(dim=1)[self.d_grp]
+            return torch.argsort(key, descending=True, stable=True).to(torch.int32)
+
         s = torch.cuda.Stream()
         # warm-up outside capture (first launches set kernel attributes)
         with torch.cuda.stream(s):
             model.predict_device(self.d_x, n, self.d_pred, s)
-            order = torch.argsort(self.d_pred, descending=True).to(torch.int32)
-            B.launch(plan, order, dynamic=True, timing=False, stream=s)
+            B.launch(plan, order_of(), dynamic=True, timing=False, stream=s)
         torch.cuda.synchronize()
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph, stream=s):
             model.predict_device(self.d_x, n, self.d_pred, s)
-            self.order = torch.argsort(self.d_pred, descending=True).to(torch.int32)
+            self.order = order_of()
             B.launch(plan, self.order, dynamic=True, timing=False, stream=s)
         torch.cuda.synchronize()
 

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import compression_b200.batch as B
-from compression_b200.costmodel import CostModel, GraphSchedule, lpt_order, measure_tasks
+from compression_b200.costmodel import CostModel, GraphSchedule, lpt_order, measure_tasks, task_groups
 from oracle import mlp_ref
 
 pytestmark = pytest.mark.gpu
@@ -65,13 +65,14 @@ def test_learned_lpt_beats_static_mapping(batch):
     r = np.corrcoef(pred, ys[0])[0, 1]
     static = B.makespan_ms(plan, None, dynamic=False, reps=5)
     queue = B.makespan_ms(plan, None, dynamic=True, reps=5)
-    learned = B.makespan_ms(plan, lpt_order(pred), dynamic=True, reps=5)
+    groups = task_groups(plan)
+    learned = B.makespan_ms(plan, lpt_order(pred, groups), dynamic=True, reps=5)
     print(f"\ncorr(pred, measured)={r:.3f}  static={static:.3f} ms  queue={queue:.3f} ms  "
           f"learned-LPT={learned:.3f} ms  gain vs static={(1 - learned / static) * 100:.1f}%")
     assert r > 0.8
     assert learned < 0.8 * static  # >= 20% shorter makespan than the static mapping
     plan.d_out.zero_()
-    B.launch(plan, lpt_order(pred), dynamic=True)
+    B.launch(plan, lpt_order(pred, groups), dynamic=True)
     torch.cuda.synchronize()
     assert B.verify(plan)
 
@@ -87,6 +88,18 @@ def test_graph_captured_schedule(batch):
     g.replay()
     torch.cuda.synchronize()
     assert B.verify(plan)
+    # the graph's order (group maximum and stable sort on the device) is the
+    # host's grouped longest-first order of the same predictions
+    from compression_b200.costmodel import lpt_order_host
+    pred = g.d_pred[:plan.tasks.size].cpu().numpy()
+    groups = task_groups(plan)
+    assert np.array_equal(g.order.cpu().numpy(), lpt_order_host(pred, groups))
+    # every RLE chunk's 32 lane tasks sit together in it
+    pos = np.empty(plan.tasks.size, np.int64)
+    pos[g.order.cpu().numpy()] = np.arange(plan.tasks.size)
+    for gid in np.unique(groups[np.isin(plan.tasks["codec"], (1, 2))])[:50]:
+        p = np.sort(pos[groups == gid])
+        assert p[-1] - p[0] == p.size - 1
 
 
 # ---------------------------------------------------------------------------
