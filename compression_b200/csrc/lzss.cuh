@@ -35,9 +35,12 @@ namespace lzss {
 // stores.  Match sources inside the current round come from shared memory,
 // older ones from the already-written output (same SM, ordered by
 // __syncwarp).  Inside the batch kernel it measured faster than the group
-// decoder below (mixed batch 20.6 against 23.2 ms, longest-first order):
-// with the group decoder the other codecs' tasks ran slower beside it too
-// (the cause was not isolated).
+// decoder below on the mixed batch (19.5 against 21.9 ms, longest-first
+// order), although a batch of LZSS chunks alone decodes 1.7x faster with the
+// group decoder (5.0 against 8.6 ms): the group decoder's unrolled code added
+// to the five decoders' in one kernel overflows the instruction cache
+// (warps stalled for instructions 3.5 instead of 1.0 times per issue), which
+// slows every codec's tasks.
 constexpr uint32_t WARP_RB = 64;             // column bytes per lane per round (16 rows)
 constexpr uint32_t WARP_SSTR = WARP_RB + 4;  // 17 words: row reads across columns are conflict-free
 constexpr uint32_t WARP_SMEM = (uint32_t)sizeof(SegTable) + 32u * RING_STRIDE + 32u * WARP_SSTR;
