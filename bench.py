@@ -716,17 +716,19 @@ def task_bytes(plan):
 def mixed_run(args, rank, world, local_rank, clk_samples):
     """Config 5, the mixed-codec batch: 16384 items (log-uniform 4 KiB - 2 MiB,
     4 GiB decompressed in all; 20% RLE v1, 20% RLE v2, 10% byte-RLE, 25% LZSS,
-    25% Deflate) decoded in one persistent launch under seven schedules:
+    25% Deflate) decoded in one persistent launch under eight schedules:
 
     * static: task i on warp i mod W (the fallback);
     * queue_fifo: the dynamic work queue in task order;
     * size_lpt_out / size_lpt_in: longest-first through the queue with the
       task's decompressed / compressed bytes as its cost (the method without
-      the network);
+      the network); size_lpt_out_banded: the same with the codec runs that
+      the learned schedule uses;
     * learned_lpt: longest-first by the cost model's prediction (the lane
       tasks of an RLE chunk keyed by their largest prediction, kept
-      together), as one CUDA-graph replay of [MLP inference -> group maximum
-      -> order -> batch decode]; learned_order_only is that order computed
+      together; inside bands of a factor of 2, one codec after another), as
+      one CUDA-graph replay of [MLP inference -> group maximum -> banded
+      order -> batch decode]; learned_order_only is that order computed
       beforehand, learned_per_task every task by its own prediction.
 
     The cost model is trained on a separate, quarter-size batch of the same
@@ -795,13 +797,15 @@ def mixed_run(args, rank, world, local_rank, clk_samples):
     out_b, in_b = task_bytes(plan)
     # the learned order itself, computed once, so that the schedule's quality
     # is timed apart from the cost of inference and sorting
-    groups = CM.task_groups(plan)
+    groups, codec = CM.task_groups(plan), plan.tasks["codec"]
+    pred32 = model.predict32(X)
     orders = {"size_lpt_out": CM.lpt_order(out_b), "size_lpt_in": CM.lpt_order(in_b),
-              "learned_order_only": CM.lpt_order(pred, groups), "learned_per_task": CM.lpt_order(pred)}
+              "size_lpt_out_banded": CM.lpt_order(np.log(out_b + 1.0), None, codec),
+              "learned_order_only": CM.lpt_order(pred32, groups, codec), "learned_per_task": CM.lpt_order(pred)}
 
     flush = torch.empty(256 * MiB, dtype=torch.uint8, device=dev)
-    kinds = ("learned_lpt", "static", "queue_fifo", "size_lpt_out", "size_lpt_in", "learned_order_only",
-             "learned_per_task")
+    kinds = ("learned_lpt", "static", "queue_fifo", "size_lpt_out", "size_lpt_in", "size_lpt_out_banded",
+             "learned_order_only", "learned_per_task")
 
     def run(kind):
         if kind == "static":
@@ -909,14 +913,18 @@ def mixed_run(args, rank, world, local_rank, clk_samples):
         "learned_gain_vs_size_lpt_out": round(1.0 - ms / med["size_lpt_out"], 4),
         "learned_gain_vs_size_lpt_in": round(1.0 - ms / med["size_lpt_in"], 4),
         "learned_order_gain_vs_size_lpt_out": round(1.0 - med["learned_order_only"] / med["size_lpt_out"], 4),
+        "learned_gain_vs_size_lpt_out_banded": round(1.0 - ms / med["size_lpt_out_banded"], 4),
         "schedules": {"static": "task i on warp i mod W", "queue_fifo": "work queue, task order",
                       "size_lpt_out": "work queue, longest first by decompressed bytes per task",
                       "size_lpt_in": "work queue, longest first by compressed bytes per task",
-                      "learned_lpt": "CUDA graph: MLP inference + group maximum + argsort + work queue (all "
+                      "size_lpt_out_banded": "size_lpt_out in bands of a factor of 2, one codec after another "
+                                             "inside a band",
+                      "learned_lpt": "CUDA graph: MLP inference + group maximum + banded sort + work queue (all "
                                      "timed); the 32 lane tasks of an RLE chunk share their largest prediction "
-                                     "and stay adjacent",
-                      "learned_order_only": "work queue in the learned (grouped) order computed beforehand",
-                      "learned_per_task": "work queue, every task by its own prediction (no grouping)"},
+                                     "and stay adjacent; inside bands of a factor of 2 of predicted time, one "
+                                     "codec after another",
+                      "learned_order_only": "work queue in the learned (grouped, banded) order computed beforehand",
+                      "learned_per_task": "work queue, every task by its own prediction (no grouping, no bands)"},
         "cost_model": {"train_batch": "separate quarter-size batch of the same mix (other seeds)",
                        "samples": int(sum(y.size for y in ys)), "epochs": 8, "final_loss": round(float(losses[-1]), 4),
                        "corr_pred_measured_eval_batch": round(corr, 4), "train_s": round(t_train, 1)},

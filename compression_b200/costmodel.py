@@ -14,8 +14,11 @@ one group, keyed by their largest prediction, so that they stay adjacent in
 the queue and run side by side: each of them reads 4 bytes of every 128-byte
 row of the block, and when they run apart every one of them fetches the rows
 again (ordering every task by its own measured time was slower than ordering
-by output bytes for that reason).  The static mapping (task i -> warp i mod W)
-remains the fallback.
+by output bytes for that reason).  Inside bands of a factor of 2 of
+predicted time the order runs one codec after another, so that an SM's warps
+mostly run one decoder's code: the batch kernel holds all five decoders,
+more code than the instruction cache keeps.  The static mapping (task i ->
+warp i mod W) remains the fallback.
 """
 from __future__ import annotations
 
@@ -75,11 +78,16 @@ class CostModel:
 
     def predict(self, X: np.ndarray) -> np.ndarray:
         """Predicted log(ns) per row of raw features X."""
+        return self.predict32(X).astype(np.float64)
+
+    def predict32(self, X: np.ndarray) -> np.ndarray:
+        """Predicted log(ns) in float32, computed as the scheduling graph does
+        (network output + mean target, in float32)."""
         torch = self.torch
         d_x = torch.from_numpy(self._norm(X)).to(self.dev)
         d_o = torch.empty(X.shape[0], dtype=torch.float32, device=self.dev)
         self.predict_device(d_x, X.shape[0], d_o)
-        return d_o.cpu().numpy().astype(np.float64) + self.y_mu
+        return (d_o + np.float32(self.y_mu)).cpu().numpy()
 
     def grad(self, d_x, d_y, d_idx, nb: int):
         """Gradient of the mini-batch MSE (normalised targets), on the device."""
@@ -169,17 +177,43 @@ def group_max(cost: np.ndarray, groups: np.ndarray) -> np.ndarray:
     return k[groups]
 
 
-def lpt_order_host(cost: np.ndarray, groups: np.ndarray | None = None) -> np.ndarray:
+BAND = float(np.log(2.0))  # width of a cost band (natural-log units): a factor of 2
+
+
+def band_sort_key(cost: np.ndarray, codec: np.ndarray, band: float = BAND) -> np.ndarray:
+    """Ascending int32 sort key of the banded longest-first order of log
+    costs (float32): bands of `band` (a cost factor of e^band), the costliest
+    band first; inside a band one codec after another; inside that, the
+    costliest first (the cost's place in its band in 21 bits).  Runs of one
+    codec keep the warps of an SM on one decoder's code (the batch kernel
+    holds all five, more than the instruction cache)."""
+    c = np.asarray(cost, np.float32)
+    t = c / np.float32(band)
+    fl = np.floor(t)
+    k1 = 127 - np.clip(fl, 0, 127).astype(np.int32)
+    q = np.clip(np.floor((np.float32(1.0) - (t - fl)) * np.float32(1 << 21)), 0, (1 << 21) - 1).astype(np.int32)
+    return (k1 << 24) | (np.asarray(codec, np.int32) << 21) | q
+
+
+def lpt_order_host(cost: np.ndarray, groups: np.ndarray | None = None, codec: np.ndarray | None = None,
+                   band: float = BAND) -> np.ndarray:
     """Task order, longest predicted first; with groups, a group's tasks share
-    its largest cost and stay together, in task order (ties keep task order)."""
+    its largest cost and stay together, in task order (ties keep task order);
+    with codec (and log costs), the banded order of band_sort_key."""
+    if codec is not None:
+        c = np.asarray(cost, np.float32)
+        if groups is not None:
+            c = group_max(c, groups).astype(np.float32)
+        return np.argsort(band_sort_key(c, codec, band), kind="stable").astype(np.int32)
     key = np.asarray(cost, np.float64) if groups is None else group_max(cost, groups)
     return np.argsort(-key, kind="stable").astype(np.int32)
 
 
-def lpt_order(cost: np.ndarray, groups: np.ndarray | None = None):
+def lpt_order(cost: np.ndarray, groups: np.ndarray | None = None, codec: np.ndarray | None = None,
+              band: float = BAND):
     """lpt_order_host as a device int32 tensor (the batch decoder's order)."""
     import torch
-    return torch.from_numpy(lpt_order_host(cost, groups)).cuda()
+    return torch.from_numpy(lpt_order_host(cost, groups, codec, band)).cuda()
 
 
 def measure_tasks(plan: B.Plan, seed: int = 0, reps: int = 1) -> np.ndarray:
@@ -202,11 +236,13 @@ class GraphSchedule:
     decode] captured in one CUDA graph over device-resident features;
     replay() decodes the batch.  groups: task_groups(plan) (default; groups
     must be contiguous runs of tasks), or None to order every task by its own
-    prediction."""
+    prediction; banded: the order of band_sort_key (codec runs inside cost
+    bands of a factor of 2), else plain longest first."""
 
     _AUTO = object()
 
-    def __init__(self, plan: B.Plan, model: CostModel, X: np.ndarray, groups=_AUTO):
+    def __init__(self, plan: B.Plan, model: CostModel, X: np.ndarray, groups=_AUTO, banded: bool = True,
+                 band: float = BAND):
         import torch
         self.torch = torch
         self.plan = plan
@@ -230,11 +266,22 @@ class GraphSchedule:
             self.d_grp = torch.from_numpy(groups).cuda()
             self.d_gidx = torch.from_numpy(gidx).cuda()
 
+        self.d_codec = (torch.from_numpy(plan.tasks["codec"].astype(np.int32) << 21).cuda() if banded else None)
+        y_mu = float(np.float32(model.y_mu))
+
         def order_of():
             key = self.d_pred[:n]
             if self.d_grp is not None:
                 key = self.d_pred[self.d_gidx].amax(dim=1)[self.d_grp]
-            return torch.argsort(key, descending=True, stable=True).to(torch.int32)
+            if self.d_codec is None:
+                return torch.argsort(key, descending=True, stable=True).to(torch.int32)
+            # band_sort_key on the device (the same float32 operations)
+            t = (key + y_mu) / band
+            fl = torch.floor(t)
+            k1 = 127 - fl.clamp(0, 127).to(torch.int32)
+            q = torch.floor((1.0 - (t - fl)) * float(1 << 21)).clamp(0, (1 << 21) - 1).to(torch.int32)
+            skey = (k1 << 24) | self.d_codec | q
+            return torch.argsort(skey, stable=True).to(torch.int32)
 
         s = torch.cuda.Stream()
         # warm-up outside capture (first launches set kernel attributes)

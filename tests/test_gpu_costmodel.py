@@ -65,14 +65,15 @@ def test_learned_lpt_beats_static_mapping(batch):
     r = np.corrcoef(pred, ys[0])[0, 1]
     static = B.makespan_ms(plan, None, dynamic=False, reps=5)
     queue = B.makespan_ms(plan, None, dynamic=True, reps=5)
-    groups = task_groups(plan)
-    learned = B.makespan_ms(plan, lpt_order(pred, groups), dynamic=True, reps=5)
+    groups, codec = task_groups(plan), plan.tasks["codec"]
+    order = lpt_order(m.predict32(X), groups, codec)  # the scheduler's order: grouped, banded
+    learned = B.makespan_ms(plan, order, dynamic=True, reps=5)
     print(f"\ncorr(pred, measured)={r:.3f}  static={static:.3f} ms  queue={queue:.3f} ms  "
           f"learned-LPT={learned:.3f} ms  gain vs static={(1 - learned / static) * 100:.1f}%")
     assert r > 0.8
     assert learned < 0.8 * static  # >= 20% shorter makespan than the static mapping
     plan.d_out.zero_()
-    B.launch(plan, lpt_order(pred, groups), dynamic=True)
+    B.launch(plan, order, dynamic=True)
     torch.cuda.synchronize()
     assert B.verify(plan)
 
@@ -91,9 +92,13 @@ def test_graph_captured_schedule(batch):
     # the graph's order (group maximum and stable sort on the device) is the
     # host's grouped longest-first order of the same predictions
     from compression_b200.costmodel import lpt_order_host
-    pred = g.d_pred[:plan.tasks.size].cpu().numpy()
+    pred = g.d_pred[:plan.tasks.size].cpu().numpy() + np.float32(m.y_mu)
     groups = task_groups(plan)
-    assert np.array_equal(g.order.cpu().numpy(), lpt_order_host(pred, groups))
+    assert np.array_equal(g.order.cpu().numpy(), lpt_order_host(pred, groups, plan.tasks["codec"]))
+    g2 = GraphSchedule(plan, m, X, banded=False)
+    g2.replay()  # the captured order is written when the graph runs
+    torch.cuda.synchronize()
+    assert np.array_equal(g2.order.cpu().numpy(), lpt_order_host(pred, groups))
     # every RLE chunk's 32 lane tasks sit together in it
     pos = np.empty(plan.tasks.size, np.int64)
     pos[g.order.cpu().numpy()] = np.arange(plan.tasks.size)

@@ -36,3 +36,29 @@ def test_grouped_longest_first_order():
     for k in range(200):
         p = pos[g == k]
         assert p.max() - p.min() == p.size - 1 and np.all(np.diff(p) == 1)  # together, in task order
+
+
+def test_banded_order():
+    """Bands of a factor of 2 of cost, costliest band first; inside a band
+    one codec after another; inside that, costliest first; groups stay
+    together."""
+    from compression_b200.costmodel import BAND, group_max, lpt_order_host
+    rng = np.random.default_rng(4)
+    g = np.repeat(np.arange(300), rng.integers(1, 33, 300))
+    codec = rng.integers(0, 5, 300)[g]
+    cost = rng.uniform(-3.0, 20.0, g.size).astype(np.float32)
+    o = lpt_order_host(cost, g, codec)
+    assert sorted(o) == list(range(g.size))
+    c = group_max(cost, g).astype(np.float32)[o]
+    band = np.clip(np.floor(c / np.float32(BAND)), 0, 255)
+    assert np.all(np.diff(band) <= 0)
+    for b in np.unique(band):
+        m = band == b
+        cb, cc = c[m], codec[o][m]
+        assert np.all(np.diff(cc) >= 0)
+        for k in np.unique(cc):
+            assert np.all(np.diff(cb[cc == k]) <= 0)
+    pos = np.empty(g.size, np.int64)
+    pos[o] = np.arange(g.size)
+    for k in range(300):
+        assert np.all(np.diff(pos[g == k]) == 1)
