@@ -206,13 +206,14 @@ __host__ __device__ constexpr uint32_t group_warp_smem(uint32_t rb, uint32_t gr)
     return (uint32_t)sizeof(SegTable) + 32u * group_rstr(gr) + 32u * group_sstr(rb);
 }
 
-template <uint32_t RB, uint32_t GRING>
+template <uint32_t RB, uint32_t GRING, uint32_t NT = 8>
 static __device__ __forceinline__ uint32_t chunk_warp_groups(const uint8_t* __restrict__ block, uint64_t b_len,
                                                             const uint64_t* __restrict__ col_len,
                                                             const uint8_t* __restrict__ col_map, uint64_t chunk_size,
                                                             uint8_t* cout, uint8_t* wsmem) {
     static_assert(RB % 4 == 0 && (group_sstr(RB) / 4) % 2 == 1, "round bytes");
     static_assert(GRING >= 64 && (GRING & (GRING - 1)) == 0, "ring bytes");
+    static_assert(NT == 8 || NT == 4, "tokens per step");
     const uint32_t lane = lane_id();
     SegTable* T_ = reinterpret_cast<SegTable*>(wsmem);
     uint8_t* rbuf = wsmem + sizeof(SegTable) + lane * group_rstr(GRING);
@@ -312,19 +313,19 @@ static __device__ __forceinline__ uint32_t chunk_warp_groups(const uint8_t* __re
                 ntok = 8;
             }
             // the tokens' bytes: token t starts t + (matches before it) bytes after rd
-            uint32_t v[8];
+            uint32_t v[NT];
 #pragma unroll
-            for (uint32_t t = 0; t < 8; ++t) {
+            for (uint32_t t = 0; t < NT; ++t) {
                 const uint32_t p = rd + t + __popc(~flags & ((1u << t) - 1u));
                 v[t] = rb(p) | (rb(p + 1u) << 8);
             }
             // lengths and sources of the tokens that start inside the round;
             // a bad token ends the column
-            uint32_t L[8], src[8];
+            uint32_t L[NT], src[NT];
             uint32_t p = rd, oo = o, nc = 0;
             bool stop = false;
 #pragma unroll
-            for (uint32_t t = 0; t < 8; ++t) {
+            for (uint32_t t = 0; t < NT; ++t) {
                 const bool lit = (flags >> t) & 1u;
                 const uint32_t ml = lit ? 1u : (v[t] & 31u) + 3u, off = lit ? 0u : v[t] >> 5;
                 const bool live = !stop && t < ntok && oo < rend;
@@ -343,13 +344,13 @@ static __device__ __forceinline__ uint32_t chunk_warp_groups(const uint8_t* __re
                 nc += ok ? 1u : 0u;
             }
             // match sources as they are before this group writes anything
-            uint64_t x[8];
+            uint64_t x[NT];
 #pragma unroll
-            for (uint32_t t = 0; t < 8; ++t)
+            for (uint32_t t = 0; t < NT; ++t)
                 x[t] = (L[t] && !((flags >> t) & 1u)) ? rd8(src[t]) : (uint64_t)(v[t] & 0xffu);
             const uint32_t o0 = o;
 #pragma unroll
-            for (uint32_t t = 0; t < 8; ++t) {
+            for (uint32_t t = 0; t < NT; ++t) {
                 const uint32_t n = L[t];
                 if (n == 0) continue;
                 const uint32_t sp = src[t], off = o - sp;
