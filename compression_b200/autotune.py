@@ -51,7 +51,7 @@ KNOBS = {
     "deflate": (TUNE_INFLATE_VARIANT, [0, 6, 12, 10, 4]),
     "brle": (TUNE_BRLE_BLOCKS_PER_SM, [8, 4, 16]),
     "rlev1": (TUNE_RLEV1_LANES_PER_BLOCK, [8, 4]),
-    "rlev2": (TUNE_RLEV2_LANES_PER_BLOCK, [4, 8]),
+    "rlev2": (TUNE_RLEV2_LANES_PER_BLOCK, [8, 4]),
     "lzss": (TUNE_LZSS_WARPS_PER_BLOCK, [0, 4, 512, 256]),
 }
 

@@ -297,7 +297,8 @@ typedef enum gd_tune_key {
                                     0 (default): 12 for >= 4 streams per SM, else 6 */
     GD_TUNE_BRLE_BLOCKS_PER_SM = 1,   /* byte-RLE grid = value x SMs blocks (default 8) */
     GD_TUNE_RLEV1_LANES_PER_BLOCK = 2, /* 0/8: 8 lane streams per block; 4: 4 */
-    GD_TUNE_RLEV2_LANES_PER_BLOCK = 3, /* 0/4: 4 lane streams per block; 8: 8 */
+    GD_TUNE_RLEV2_LANES_PER_BLOCK = 3, /* 0: 8 lane streams per block (4 if 8 do not fit in shared
+                                          memory); 8: 8; 4: 4 */
     GD_TUNE_LZSS_WARPS_PER_BLOCK = 4,  /* 0: one chunk per 32-thread block, one lane per column, a
                                           flag group per lane and step, output in 320-byte rounds
                                           per column (any chunk size); 4: the same with four chunks
