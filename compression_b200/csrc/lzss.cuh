@@ -171,8 +171,8 @@ static __device__ __noinline__ uint32_t chunk_warp(const uint8_t* __restrict__ b
 }
 
 // ---------------------------------------------------------------------------
-// Group decoder: one warp per chunk, one lane per column, up to one flag
-// group (8 tokens) per lane and step.
+// Group decoder: one warp per chunk, one lane per column, up to NT tokens
+// per lane and step (a flag group of 8, or half of one).
 //
 // The token positions of a group follow from its flag byte alone, so a lane
 // loads the group's token bytes together, derives every token's length and
