@@ -60,6 +60,17 @@ def test_rlev2(cuda, ru):
     _parity(cc.rlev2_encode(v, 256 * ru * 4, ru), v.view(np.uint8), cuda)
 
 
+def test_rlev2_wide_lanes_use_four_streams_per_block(cuda):
+    """Lane streams too long for 8 per block in shared memory (1 MiB chunks of
+    wide random values, about 30 KB per lane stream): the default launch
+    falls back to 4 streams per block and still decodes as the oracle."""
+    rng = np.random.default_rng(12)
+    v = rng.integers(-2**59, 2**59, 3 * (1 << 17)).astype(np.int64)  # 3 chunks of 1 MiB
+    enc = cc.rlev2_encode(v, 1 << 20, 32)
+    assert 8 * (int(enc.meta["col_len"].max()) + 48) > 200 * 1024  # 8 streams would not fit
+    _parity(enc, v.view(np.uint8), cuda)
+
+
 def test_rlev2_negative_and_wide(cuda):
     rng = np.random.default_rng(1)
     v = np.concatenate([rng.integers(-2**62, 2**62, 3000), -np.arange(3000), np.full(500, -7),
